@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 gradient-domain Poisson solver.
+
+Default workload (one GPU): tone-mapping-style Neumann integration of a
+4096 x 4096 x 3 radiance map (16.8 MP per channel, three channels solved as
+one batched plan), mixed precision (FP32 V-cycle, FP64 residual refresh and
+accumulator) to a true relative residual of 1e-8.  One step = one batched
+solve of the three channels from x0 = 0.  ``value`` is whole-job Mpix/s
+(channels x pixels / step time, device-timed, inputs resident in HBM);
+``e2e`` repeats the measurement through the public API with pinned host
+buffers, including both copies; the FP64 MGPCG on the same plan shape is
+timed for the mixed-vs-FP64 ratio.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank solves its own replica (no collective on the data
+path; ``scaling`` = weak) and rank 0 prints one JSON line with the max over
+ranks of the device time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mpix/s to 1e-8 rel. residual, mixed vs FP64 MGPCG; served p50/p99 latency"
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per grid cell of each kernel kind (FP32 vectors of the
+# mixed plan; the FP64 plan doubles the FP32 terms).  Level kernels count the
+# cells of the level they work on; coarse arrays are a quarter of that.
+BYTES_PER_CELL_MIXED = {
+    "down0": 4 + 1, "down": 4 + 1,          # read b, write coarse b
+    "up0": 4 + 1 + 4, "up": 4 + 1 + 4,      # read b and coarse e, write u
+    "pupdate": 4 + 4 + 4,                   # read z, p; write p
+    "cgupdate": 12 + 8,                     # read p, d, r; write d, r
+    "resid": 8 + 8 + 4,                     # read x, f; write r (refresh iterations)
+    "fold": 8 + 4 + 8 + 4,                  # read x, d; write x, d (refresh iterations)
+    "init": 8 + 8 + 8 + 16,                 # read f twice, x; write r, d, p, z
+    "mean": 8 + 16,                         # read x; read+write x
+}
+
+
+def bytes_per_cell(kind: str, fp64: bool) -> float:
+    b = BYTES_PER_CELL_MIXED.get(kind, 0.0)
+    if not fp64:
+        return b
+    fp32_part = {"down0": 5, "down": 5, "up0": 9, "up": 9, "pupdate": 12, "cgupdate": 20,
+                 "resid": 4, "fold": 8, "init": 16, "mean": 0}.get(kind, 0)
+    return b + fp32_part
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            data = json.load(fh)
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_tonemap(rhs: np.ndarray, budget_s: float = 20.0) -> dict:
+    """Time the oracle's DCT Neumann solve (the reference's CPU path) on host cores."""
+    from oracle import solvers as osolvers
+    cores = os.cpu_count() or 1
+    n_ch, h, w = rhs.shape
+    t0 = time.perf_counter()
+    done = 0
+    while done < n_ch and (time.perf_counter() - t0) < budget_s:
+        osolvers.solve_neumann(rhs[done], workers=cores)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done * h * w / dt / 1e6, "unit": "Mpix/s", "cores": cores, "kind": "port",
+            "sample": f"{done} of {n_ch} channels of {h}x{w}, scipy DCT solve_neumann "
+                      f"restatement, {cores} fft workers, {dt:.2f} s"}
+
+
+def reference_arm(args) -> None:
+    """`--impl reference`: the reference's CPU algorithm for this path on host cores."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from gradient_domain_b200 import workloads
+    from oracle import solvers as osolvers
+    rhs = workloads.tonemap_rhs(args.size, seed=1)
+    cores = os.cpu_count() or 1
+    n_ch, h, w = rhs.shape
+    for _ in range(args.warmup):
+        osolvers.solve_neumann(rhs[0], workers=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for c in range(n_ch):
+            osolvers.solve_neumann(rhs[c], workers=cores)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = n_ch * h * w / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpix/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"tonemap-neumann {args.size}x{args.size}x3", "tolerance": "exact"},
+        "cpu_baseline": {"value": value, "unit": "Mpix/s", "cores": cores, "kind": "port",
+                         "sample": f"full workload per step ({n_ch} channels), scipy DCT "
+                                   f"restatement of solve_neumann, {cores} fft workers"},
+        "e2e": {"value": value, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from gradient_domain_b200 import workloads
+    from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
+    from gradient_domain_b200.solvers import solve_neumann_batch
+
+    dev = torch.device("cuda", local)
+    size = args.size
+    rhs_np = workloads.tonemap_rhs(size, seed=1 + rank)
+    n_ch = rhs_np.shape[0]
+    cells = n_ch * size * size
+    f = torch.as_tensor(rhs_np).to(dev)
+    x = torch.zeros_like(f)
+    insts = [Instance(size, size, "neumann", zero_mean=True) for _ in range(n_ch)]
+    plan = PoissonPlan(insts, SolveParams(precision="mixed", tolerance=args.tol,
+                                          sweeps=args.sweeps))
+    stream = torch.cuda.current_stream()
+
+    def step(p):
+        x.zero_()
+        return p.solve(list(f), list(x), scale=-1.0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        results = step(plan)
+    plan.set_profiling(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        results = step(plan)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    ktimes = plan.kernel_times()
+    plan.set_profiling(False)
+    value = cells * world / (ms / 1e3) / 1e6
+    its = [r.iterations for r in results]
+    resid = max(r.relative_residual for r in results)
+    converged = all(r.converged for r in results)
+
+    # accuracy against the FP64 oracle (DCT) and CPU baseline, rank 0 only
+    extra = {}
+    sol = (x.cpu().numpy())
+    if rank == 0 and not args.no_cpu:
+        from oracle import solvers as osolvers
+        t0 = time.perf_counter()
+        errs = []
+        for c in range(n_ch):
+            ref = osolvers.solve_neumann(rhs_np[c], workers=os.cpu_count())
+            errs.append(float(np.linalg.norm(sol[c] - ref) / np.linalg.norm(ref)))
+        extra["rel_l2_err_vs_fp64_oracle"] = errs
+        extra["oracle_seconds"] = time.perf_counter() - t0
+
+    # FP64 MGPCG on the same workload (the precision baseline)
+    plan64 = PoissonPlan(insts, SolveParams(precision="fp64", tolerance=args.tol,
+                                            sweeps=args.sweeps))
+    step(plan64)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    k64 = max(1, args.steps // 2)
+    for _ in range(k64):
+        r64 = step(plan64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms64 = max_over_ranks(e0.elapsed_time(e1) / k64)
+    value64 = cells * world / (ms64 / 1e3) / 1e6
+    del plan64
+
+    # end to end through the public API, pinned host buffers, copies timed
+    host_in = torch.as_tensor(rhs_np).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    solve_neumann_batch(host_in, tolerance=args.tol, out=host_out)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        solve_neumann_batch(host_in, tolerance=args.tol, out=host_out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps
+    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall * 1e3))
+    e2e_value = cells * world / (ms_e2e / 1e3) / 1e6
+
+    # roofline of the dominant kernel (live CUDA-event durations)
+    hbm, peak_kind = peaks()
+    kinds = {k: v for k, v in ktimes.items() if v["launches"] > 0}
+    dom = max(kinds, key=lambda k: kinds[k]["ms"])
+    d = kinds[dom]
+    per_launch_ms = d["ms"] / d["launches"]
+    per_launch_cells = d["cells"] / d["launches"]
+    algo_bytes = bytes_per_cell(dom, False) * per_launch_cells
+    achieved = algo_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            tpc = json.load(fh).get(dom)
+        if tpc:
+            traffic = tpc * per_launch_cells
+    total_ms = sum(v["ms"] for v in kinds.values())
+    launches = sum(v["launches"] for v in kinds.values())
+    launches += kinds.get("init", {}).get("launches", 0) + kinds.get("mean", {}).get("launches", 0)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32/fp64-mixed", "data": "synthetic",
+        "config": {"workload": f"tonemap-neumann {size}x{size}x3", "tolerance": args.tol,
+                   "sweeps": args.sweeps, "instances_per_gpu": n_ch,
+                   "l2": "inputs larger than L2 (3 x 134 MB rhs + solution + hierarchy)",
+                   "parallelism": f"replicas x{world}"},
+        "clocks": clock,
+        "e2e": {"value": e2e_value, "unit": "Mpix/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(host_in.numel() * 8),
+                "d2h_bytes_per_step": int(host_out.numel() * 8)},
+        "gpu_launches": int(launches),
+        "iterations": its, "relative_residual": resid, "converged": converged,
+        "fp64_mgpcg": {"value": value64, "ms_per_step": ms64,
+                       "iterations": [r.iterations for r in r64],
+                       "mixed_over_fp64": value / value64},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": algo_bytes,
+                     "avg_launch_ms": per_launch_ms},
+        "kernel_share": {k: round(v["ms"] / total_ms, 4) for k, v in kinds.items()},
+        "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in kinds.items()},
+    }
+    line.update(extra)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_tonemap(rhs_np)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--sweeps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the oracle and CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

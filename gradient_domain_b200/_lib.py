@@ -1,0 +1,138 @@
+"""ctypes binding of ``libgd_poisson.so`` (the C ABI of ``include/gd_poisson.h``).
+
+There is no CPU fallback: importing the solvers works anywhere, but the first
+call that needs the library raises if the shared object is missing, and the
+first call that needs a GPU raises if CUDA is unavailable.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgd_poisson.so")
+
+GD_DIRICHLET, GD_NEUMANN, GD_MASKED = 0, 1, 2
+GD_MIXED, GD_FP64 = 0, 1
+GD_CONVERGED, GD_MAX_ITERATIONS, GD_BREAKDOWN, GD_ACTIVE = 0, 1, 2, 3
+STATUS_NAMES = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "active"}
+
+EXPORTS = (
+    "gd_last_error", "gd_version", "gd_plan_create", "gd_plan_destroy",
+    "gd_plan_workspace_bytes", "gd_plan_bind", "gd_plan_set_mask", "gd_plan_prepare",
+    "gd_solve", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
+    "gd_ref_workspace_bytes", "gd_ref_vcycle",
+    "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
+    "gd_masked_rhs",
+)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("height", C.c_int32), ("width", C.c_int32), ("boundary", C.c_int32),
+                ("flags", C.c_int32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("pre_sweeps", C.c_int32),
+                ("post_sweeps", C.c_int32), ("max_iterations", C.c_int32),
+                ("tolerance", C.c_double), ("reliable_delta", C.c_double),
+                ("check_every", C.c_int32), ("use_graph", C.c_int32)]
+
+
+class Report(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("status", C.c_int32),
+                ("relative_residual", C.c_double), ("initial_norm", C.c_double)]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("launches", C.c_longlong), ("milliseconds", C.c_double), ("cells", C.c_double)]
+
+
+KERNEL_KINDS = ("down0", "down", "bottom", "up", "up0", "pupdate", "cgupdate", "fold", "resid",
+                "init", "mean")
+
+
+class GDError(RuntimeError):
+    """A call into libgd_poisson failed."""
+
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+_vp, _dp, _i32, _i64, _f64, _sz = C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_size_t
+
+
+def _declare(lib: C.CDLL) -> None:
+    sig = {
+        "gd_last_error": (C.c_char_p, []),
+        "gd_version": (C.c_char_p, []),
+        "gd_plan_create": (C.c_int, [C.POINTER(GridDesc), _i32, C.POINTER(Params),
+                                     C.POINTER(C.c_void_p)]),
+        "gd_plan_destroy": (None, [_vp]),
+        "gd_plan_workspace_bytes": (_sz, [_vp]),
+        "gd_plan_bind": (C.c_int, [_vp, _vp, _sz, _vp]),
+        "gd_plan_set_mask": (C.c_int, [_vp, _i32, _vp, _i32, _vp]),
+        "gd_plan_prepare": (C.c_int, [_vp, _vp]),
+        "gd_solve": (C.c_int, [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                               C.POINTER(C.c_int32), C.POINTER(C.c_double), _vp,
+                               C.POINTER(Report)]),
+        "gd_plan_apply_vcycle": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
+        "gd_plan_set_profiling": (C.c_int, [_vp, _i32]),
+        "gd_plan_kernel_times": (C.c_int, [_vp, C.POINTER(KernelTime), _i32]),
+        "gd_ref_workspace_bytes": (_sz, [_i32, _i32, _i32]),
+        "gd_ref_vcycle": (C.c_int, [_vp, _vp, _i32, _i32, _f64, _i32, _i32, _i32, _i32, _vp,
+                                    _sz, _vp]),
+        "gd_ref_residual": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+        "gd_ref_dot": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _sz, _vp]),
+        "gd_ref_axpby": (C.c_int, [_vp, _vp, _f64, _f64, _i64, _vp]),
+        "gd_gradient": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+        "gd_divergence": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+        "gd_fold_dirichlet": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+        "gd_masked_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises if ``libgd_poisson.so`` has not been built."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise GDError(
+                        f"{LIB_PATH} is missing: build it with "
+                        "`python -m gradient_domain_b200.build` (there is no CPU fallback)")
+                handle = C.CDLL(LIB_PATH)
+                _declare(handle)
+                _lib = handle
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib().gd_last_error().decode(errors="replace")
+        raise GDError(f"{what} failed ({rc}): {msg}")
+
+
+def device() -> torch.device:
+    """The CUDA device used by the solvers; raises when no GPU is visible."""
+    if not torch.cuda.is_available():
+        raise GDError("gradient_domain_b200 needs a CUDA device (B200); none is visible")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def ptr(t: torch.Tensor) -> int:
+    return int(t.data_ptr())

@@ -1,0 +1,652 @@
+// Batched cell-centred MGPCG: hierarchy planning, launch sequencing and the
+// C ABI of gd_poisson.h.
+//
+// One plan holds any number of instances (images x channels) of any sizes and
+// boundary types.  Every kernel launch covers one step of the V-cycle or of
+// the Krylov loop for all instances at once through a tile list, so a batch
+// of uneven solves costs the same number of launches as one solve
+// (poisson.py:137-145 and :216-242 loop over channels one at a time).
+// Levels are aligned at the top: launch `down[l]` / `up[l]` holds level l of
+// every instance whose hierarchy reaches below l, and one `bottom` launch
+// finishes every instance's small levels.  One Krylov iteration is
+//   down[0..D-1], bottom, up[D-1..0], pupdate, cgupdate, fold, resid
+// with all scalars on the device, so the host only polls a counter of active
+// instances every `check_every` iterations and the iteration can be captured
+// once as a CUDA graph.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gd_mg_kernels.cuh"
+
+using namespace gd;
+
+struct gd_plan_s {
+  int n = 0;
+  gd_params prm{};
+  bool fp64 = false;
+  std::vector<InstInfo> inst;
+  std::vector<LevelInfo> lv;
+  std::vector<Tile> tiles;
+  int fine_base = 0, fine_count = 0, depth = 0;
+  std::vector<int> down_base, down_count, up_base, up_count;
+  size_t arena_elems = 0, code_bytes = 0, dense_elems = 0;
+  int max_partials = 1;
+  size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
+         o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, total = 0;
+  size_t bottom_smem = 0;
+  char *ws = nullptr;
+  bool prepared = false;
+  std::vector<char> mask_set;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t cap = nullptr;
+  int *h_nact = nullptr;
+  InstState *h_st = nullptr;
+  // profiling: events around every launch (graphs are bypassed while enabled)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_kind;
+  std::vector<double> ev_cells;
+  size_t ev_used = 0;
+  double prof_ms[GD_KERNEL_KINDS] = {0};
+  double prof_cells[GD_KERNEL_KINDS] = {0};
+  long long prof_launches[GD_KERNEL_KINDS] = {0};
+  std::vector<double> launch_cells;  // fine cells covered by each launch map
+  double fine_cells = 0;
+};
+
+namespace {
+
+constexpr int kPitchAlign = 4;       // elements; rows start on 16-byte boundaries for FP32
+constexpr size_t kArrayAlign = 256;  // bytes
+
+// Record an event before a launch of `kind` covering `cells` grid cells.
+void prof_begin(gd_plan p, int kind, double cells, cudaStream_t st) {
+  if (!p->profiling) return;
+  while (p->ev_pool.size() < p->ev_used + 2) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    p->ev_pool.push_back(e);
+  }
+  if (p->ev_kind.size() < p->ev_used + 2) {
+    p->ev_kind.resize(p->ev_used + 2);
+    p->ev_cells.resize(p->ev_used + 2);
+  }
+  p->ev_kind[p->ev_used] = kind;
+  p->ev_cells[p->ev_used] = cells;
+  cudaEventRecord(p->ev_pool[p->ev_used], st);
+  p->ev_used += 1;
+}
+
+void prof_end(gd_plan p, cudaStream_t st) {
+  if (!p->profiling) return;
+  p->ev_kind[p->ev_used] = -1;
+  cudaEventRecord(p->ev_pool[p->ev_used], st);
+  p->ev_used += 1;
+}
+
+// After a synchronize: fold the recorded pairs into the per-kind totals.
+void prof_collect(gd_plan p) {
+  for (size_t k = 0; k + 1 < p->ev_used; k += 2) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p->ev_pool[k], p->ev_pool[k + 1]);
+    const int kind = p->ev_kind[k];
+    p->prof_ms[kind] += ms;
+    p->prof_cells[kind] += p->ev_cells[k];
+    p->prof_launches[kind] += 1;
+  }
+  p->ev_used = 0;
+}
+
+template <typename T>
+struct Runner {
+  using Cfg1 = VCfg<T, 1, 1>;
+
+  template <int S>
+  static void set_attrs() {
+    using C = VCfg<T, S, S>;
+    cudaFuncSetAttribute(k_down<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::down_smem());
+    cudaFuncSetAttribute(k_up<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::up_smem());
+    cudaFuncSetAttribute(k_up<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)C::up_smem());
+    cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+  }
+
+  static Args<T> args(gd_plan p) {
+    Args<T> a;
+    a.lv = reinterpret_cast<const LevelInfo *>(p->ws + p->o_lv);
+    a.inst = reinterpret_cast<const InstInfo *>(p->ws + p->o_inst);
+    a.st = reinterpret_cast<InstState *>(p->ws + p->o_st);
+    a.arena = reinterpret_cast<T *>(p->ws + p->o_arena);
+    a.codes = reinterpret_cast<const unsigned char *>(p->ws + p->o_codes);
+    a.dense = reinterpret_cast<const double *>(p->ws + p->o_dense);
+    a.part0 = reinterpret_cast<double *>(p->ws + p->o_p0);
+    a.part1 = reinterpret_cast<double *>(p->ws + p->o_p1);
+    a.counter = reinterpret_cast<unsigned *>(p->ws + p->o_cnt);
+    a.n_active = reinterpret_cast<int *>(p->ws + p->o_nact);
+    a.tiles = reinterpret_cast<const Tile *>(p->ws + p->o_tiles);
+    a.ninst = p->n;
+    a.tol2 = p->prm.tolerance * p->prm.tolerance;
+    a.delta2 = p->fp64 ? 0.0 : p->prm.reliable_delta * p->prm.reliable_delta;
+    a.max_iter = p->prm.max_iterations;
+    return a;
+  }
+
+  static Args<T> at_tiles(Args<T> a, int base) {
+    a.tiles += base;
+    return a;
+  }
+
+  template <int S>
+  static void vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    using C = VCfg<T, S, S>;
+    for (int l = 0; l < p->depth; ++l) {
+      if (p->down_count[l] <= 0) continue;
+      prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
+      k_down<T, S><<<p->down_count[l], kVThreads, C::down_smem(), st>>>(
+          at_tiles(a, p->down_base[l]), 0);
+      prof_end(p, st);
+    }
+    prof_begin(p, GD_K_BOTTOM, 0.0, st);
+    k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
+    prof_end(p, st);
+    for (int l = p->depth - 1; l >= 0; --l) {
+      if (p->up_count[l] <= 0) continue;
+      prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
+      if (l == 0)
+        k_up<T, S, S, true><<<p->up_count[l], kVThreads, C::up_smem(), st>>>(
+            at_tiles(a, p->up_base[l]), 0);
+      else
+        k_up<T, S, S, false><<<p->up_count[l], kVThreads, C::up_smem(), st>>>(
+            at_tiles(a, p->up_base[l]), 0);
+      prof_end(p, st);
+    }
+  }
+
+  template <int S>
+  static void iteration(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    vcycle<S>(p, a, st);
+    const Args<T> f = at_tiles(a, p->fine_base);
+    const double c = p->fine_cells;
+    prof_begin(p, GD_K_PUPDATE, c, st);
+    k_pupdate<T><<<p->fine_count, kFThreads, 0, st>>>(f);
+    prof_end(p, st);
+    prof_begin(p, GD_K_CGUPDATE, c, st);
+    k_cgupdate<T><<<p->fine_count, kFThreads, 0, st>>>(f);
+    prof_end(p, st);
+    prof_begin(p, GD_K_FOLD, c, st);
+    k_fold<T><<<p->fine_count, kFThreads, 0, st>>>(f);
+    prof_end(p, st);
+    prof_begin(p, GD_K_RESID, c, st);
+    k_resid<T, false><<<p->fine_count, kFThreads, 0, st>>>(f);
+    prof_end(p, st);
+  }
+
+  static void dispatch_attrs(int s) {
+    if (s == 1) set_attrs<1>();
+    else if (s == 2) set_attrs<2>();
+    else set_attrs<3>();
+  }
+  static void dispatch_iteration(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    const int s = p->prm.pre_sweeps;
+    if (s == 1) iteration<1>(p, a, st);
+    else if (s == 2) iteration<2>(p, a, st);
+    else iteration<3>(p, a, st);
+  }
+  static void dispatch_vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    const int s = p->prm.pre_sweeps;
+    if (s == 1) vcycle<1>(p, a, st);
+    else if (s == 2) vcycle<2>(p, a, st);
+    else vcycle<3>(p, a, st);
+  }
+};
+
+template <typename T>
+__global__ void k_load_r(T *r, int pitch, const double *src, int spitch, int ny, int nx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ny * nx) return;
+  const int y = k / nx, x = k - y * nx;
+  r[(long long)y * pitch + x] = (T)src[(long long)y * spitch + x];
+}
+
+template <typename T>
+__global__ void k_store_z(double *dst, int dpitch, const T *z, int pitch, int ny, int nx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ny * nx) return;
+  const int y = k / nx, x = k - y * nx;
+  dst[(long long)y * dpitch + x] = (double)z[(long long)y * pitch + x];
+}
+
+size_t elem_size(const gd_plan p) { return p->fp64 ? sizeof(double) : sizeof(float); }
+
+// Lay out hierarchy, arena, tile lists and workspace for the plan.
+int build_plan(gd_plan p, const gd_grid_desc *grids) {
+  const size_t es = elem_size(p);
+  const size_t align_el = kArrayAlign / es;
+  auto take = [&](size_t &cursor, size_t elems) {
+    const size_t off = cursor;
+    cursor = align_up(cursor + elems, align_el);
+    return (long long)off;
+  };
+  size_t arena = 0, codes = 0, dense = 0;
+  std::vector<int> bottoms(p->n);
+  for (int i = 0; i < p->n; ++i) {
+    const gd_grid_desc &g = grids[i];
+    InstInfo I{};
+    I.ny = g.height;
+    I.nx = g.width;
+    I.bc = g.boundary;
+    I.zero_mean = (g.boundary == GD_NEUMANN && (g.flags & 1)) ? 1 : 0;
+    I.pitch = (int)align_up((size_t)g.width, kPitchAlign);
+    const size_t cells0 = (size_t)I.ny * I.pitch;
+    I.r_off = take(arena, cells0);
+    I.p_off = take(arena, cells0);
+    I.d_off = take(arena, cells0);
+    I.z_off = take(arena, cells0);
+    I.level0 = (int)p->lv.size();
+    int ny = I.ny, nx = I.nx, level = 0;
+    int bottom = -1;
+    while (true) {
+      LevelInfo L{};
+      L.ny = ny;
+      L.nx = nx;
+      L.pitch = level == 0 ? I.pitch : (int)align_up((size_t)nx, kPitchAlign);
+      L.inst = i;
+      L.bc = g.boundary;
+      L.level = level;
+      L.wall = g.boundary == GD_NEUMANN ? 0.0f : (level == 0 ? 1.0f : 2.0f);
+      if (level == 0) {
+        L.b_off = I.r_off;
+        L.u_off = I.z_off;
+      } else {
+        L.b_off = take(arena, (size_t)ny * L.pitch);
+        L.u_off = take(arena, (size_t)ny * L.pitch);
+      }
+      L.code_off = -1;
+      if (g.boundary == GD_MASKED) {
+        L.code_off = (long long)codes;
+        codes = align_up(codes + (size_t)ny * L.pitch, kArrayAlign);
+      }
+      L.inv_off = -1;
+      const long long cells = (long long)ny * nx;
+      if (bottom < 0 && cells <= kBottomCells) bottom = level;
+      L.is_bottom = (bottom == level);
+      const bool coarsest = cells <= kCoarsestCells;
+      L.coarse = coarsest ? -1 : (int)p->lv.size() + 1;
+      if (coarsest) {
+        L.inv_off = (long long)dense;
+        dense += align_up((size_t)cells * cells, 32);
+      }
+      p->lv.push_back(L);
+      if (coarsest) break;
+      ny = (ny + 1) / 2;
+      nx = (nx + 1) / 2;
+      ++level;
+    }
+    I.nlevels = level + 1;
+    I.bottom = I.level0 + bottom;
+    I.coarsest = I.level0 + level;
+    bottoms[i] = bottom;
+    p->depth = std::max(p->depth, bottom);
+    p->inst.push_back(I);
+  }
+  // tile lists
+  const bool f64 = p->fp64;
+  const int CY = f64 ? VCfg<double, 1, 1>::CY : VCfg<float, 1, 1>::CY;
+  const int CX = f64 ? VCfg<double, 1, 1>::CX : VCfg<float, 1, 1>::CX;
+  const int UTY = 2 * CY, UTX = 2 * CX;
+  p->fine_base = (int)p->tiles.size();
+  for (int i = 0; i < p->n; ++i) {
+    InstInfo &I = p->inst[i];
+    I.fine_begin = (int)p->tiles.size() - p->fine_base;
+    for (int ty = 0; ty < ceil_div(I.ny, kFTY); ++ty)
+      for (int tx = 0; tx < ceil_div(I.nx, kFTX); ++tx)
+        p->tiles.push_back(Tile{I.level0, i, ty, tx});
+    I.fine_end = (int)p->tiles.size() - p->fine_base;
+  }
+  p->fine_count = (int)p->tiles.size() - p->fine_base;
+  p->down_base.assign(p->depth, 0);
+  p->down_count.assign(p->depth, 0);
+  p->up_base.assign(p->depth, 0);
+  p->up_count.assign(p->depth, 0);
+  for (int l = 0; l < p->depth; ++l) {
+    p->down_base[l] = (int)p->tiles.size();
+    for (int i = 0; i < p->n; ++i) {
+      if (bottoms[i] <= l) continue;
+      const LevelInfo &C = p->lv[p->inst[i].level0 + l + 1];
+      for (int ty = 0; ty < ceil_div(C.ny, CY); ++ty)
+        for (int tx = 0; tx < ceil_div(C.nx, CX); ++tx)
+          p->tiles.push_back(Tile{p->inst[i].level0 + l, i, ty, tx});
+    }
+    p->down_count[l] = (int)p->tiles.size() - p->down_base[l];
+  }
+  for (int l = 0; l < p->depth; ++l) {
+    p->up_base[l] = (int)p->tiles.size();
+    for (int i = 0; i < p->n; ++i) {
+      InstInfo &I = p->inst[i];
+      if (bottoms[i] <= l) continue;
+      const LevelInfo &F = p->lv[I.level0 + l];
+      if (l == 0) I.up0_begin = (int)p->tiles.size() - p->up_base[0];
+      for (int ty = 0; ty < ceil_div(F.ny, UTY); ++ty)
+        for (int tx = 0; tx < ceil_div(F.nx, UTX); ++tx)
+          p->tiles.push_back(Tile{I.level0 + l, i, ty, tx});
+      if (l == 0) I.up0_end = (int)p->tiles.size() - p->up_base[0];
+    }
+    p->up_count[l] = (int)p->tiles.size() - p->up_base[l];
+  }
+  p->max_partials = std::max(1, std::max(p->fine_count, p->depth > 0 ? p->up_count[0] : 0));
+  p->launch_cells.assign(2 * std::max(p->depth, 1), 0.0);
+  p->fine_cells = 0;
+  for (int i = 0; i < p->n; ++i) {
+    const InstInfo &I = p->inst[i];
+    p->fine_cells += (double)I.ny * I.nx;
+    for (int l = 0; l < bottoms[i]; ++l) {
+      const LevelInfo &F = p->lv[I.level0 + l];
+      p->launch_cells[2 * l] += (double)F.ny * F.nx;
+      p->launch_cells[2 * l + 1] += (double)F.ny * F.nx;
+    }
+  }
+  // bottom shared memory
+  size_t bsm = 0;
+  for (int i = 0; i < p->n; ++i) {
+    const InstInfo &I = p->inst[i];
+    size_t telems = 0, cbytes = 0;
+    for (int l = I.bottom; l <= I.coarsest; ++l) {
+      const size_t c = (size_t)p->lv[l].ny * p->lv[l].nx;
+      telems += 2 * c;
+      cbytes += c;
+    }
+    telems += (size_t)p->lv[I.bottom].ny * p->lv[I.bottom].nx;
+    telems = (telems * es + 7) / 8 * 8 / es;
+    telems += 2 * kCoarsestCells * (sizeof(double) / es);
+    bsm = std::max(bsm, telems * es + cbytes + 64);
+  }
+  p->bottom_smem = bsm;
+  p->arena_elems = arena;
+  p->code_bytes = std::max<size_t>(codes, kArrayAlign);
+  p->dense_elems = std::max<size_t>(dense, 32);
+  // workspace
+  size_t o = 0;
+  auto sect = [&](size_t bytes) {
+    const size_t at = o;
+    o = align_up(o + bytes, kArrayAlign);
+    return at;
+  };
+  p->o_lv = sect(p->lv.size() * sizeof(LevelInfo));
+  p->o_inst = sect(p->inst.size() * sizeof(InstInfo));
+  p->o_st = sect(p->n * sizeof(InstState));
+  p->o_tiles = sect(p->tiles.size() * sizeof(Tile));
+  p->o_arena = sect(p->arena_elems * es);
+  p->o_codes = sect(p->code_bytes);
+  p->o_dense = sect(p->dense_elems * sizeof(double));
+  p->o_p0 = sect(p->max_partials * sizeof(double));
+  p->o_p1 = sect(p->max_partials * sizeof(double));
+  p->o_cnt = sect(16 * sizeof(unsigned));
+  p->o_nact = sect(sizeof(int));
+  p->total = o;
+  return GD_OK;
+}
+
+}  // namespace
+
+extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_params *params,
+                              gd_plan *out) {
+  GD_REQUIRE(grids && params && out && n > 0, GD_ERR_ARG, "gd_plan_create: bad arguments");
+  *out = nullptr;
+  GD_REQUIRE(params->pre_sweeps == params->post_sweeps && params->pre_sweeps >= 1 &&
+                 params->pre_sweeps <= 3,
+             GD_ERR_UNSUPPORTED, "gd_plan_create: pre_sweeps == post_sweeps in 1..3 required");
+  GD_REQUIRE(params->precision == GD_MIXED || params->precision == GD_FP64, GD_ERR_ARG,
+             "gd_plan_create: unknown precision %d", params->precision);
+  GD_REQUIRE(params->max_iterations >= 0 && params->tolerance >= 0.0, GD_ERR_ARG,
+             "gd_plan_create: bad tolerance / iteration budget");
+  for (int i = 0; i < n; ++i) {
+    GD_REQUIRE(grids[i].height > 0 && grids[i].width > 0, GD_ERR_ARG,
+               "gd_plan_create: instance %d has an empty grid", i);
+    GD_REQUIRE(grids[i].boundary >= 0 && grids[i].boundary <= 2, GD_ERR_ARG,
+               "gd_plan_create: instance %d has unknown boundary %d", i, grids[i].boundary);
+    GD_REQUIRE((long long)grids[i].height * grids[i].width < (1ll << 31), GD_ERR_ARG,
+               "gd_plan_create: instance %d is too large", i);
+  }
+  gd_plan p = new gd_plan_s();
+  p->n = n;
+  p->prm = *params;
+  if (p->prm.check_every <= 0) p->prm.check_every = 4;
+  if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-3;
+  p->fp64 = params->precision == GD_FP64;
+  p->mask_set.assign(n, 0);
+  build_plan(p, grids);
+  if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);
+  else Runner<float>::dispatch_attrs(p->prm.pre_sweeps);
+  if (cudaMallocHost(&p->h_nact, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&p->h_st, sizeof(InstState) * n) != cudaSuccess) {
+    set_error("gd_plan_create: pinned host allocation failed");
+    gd_plan_destroy(p);
+    return GD_ERR_CUDA;
+  }
+  if (p->bottom_smem > 200 * 1024) {
+    set_error("gd_plan_create: bottom levels need %zu bytes of shared memory", p->bottom_smem);
+    gd_plan_destroy(p);
+    return GD_ERR_UNSUPPORTED;
+  }
+  *out = p;
+  return GD_OK;
+}
+
+extern "C" void gd_plan_destroy(gd_plan p) {
+  if (!p) return;
+  for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
+  if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->cap) cudaStreamDestroy(p->cap);
+  if (p->h_nact) cudaFreeHost(p->h_nact);
+  if (p->h_st) cudaFreeHost(p->h_st);
+  delete p;
+}
+
+extern "C" size_t gd_plan_workspace_bytes(gd_plan p) { return p ? p->total : 0; }
+
+extern "C" int gd_plan_bind(gd_plan p, void *ws, size_t bytes, cudaStream_t st) {
+  GD_REQUIRE(p && ws, GD_ERR_ARG, "gd_plan_bind: bad arguments");
+  GD_REQUIRE(bytes >= p->total, GD_ERR_ARG, "gd_plan_bind: workspace %zu < %zu bytes", bytes,
+             p->total);
+  GD_REQUIRE(((uintptr_t)ws & (kArrayAlign - 1)) == 0, GD_ERR_ARG,
+             "gd_plan_bind: workspace must be 256-byte aligned");
+  if (p->gexec) {
+    cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+  }
+  p->ws = (char *)ws;
+  p->prepared = false;
+  GD_CHECK_CUDA(cudaMemsetAsync(ws, 0, p->total, st));
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_lv, p->lv.data(), p->lv.size() * sizeof(LevelInfo),
+                                cudaMemcpyHostToDevice, st));
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->inst.data(),
+                                p->inst.size() * sizeof(InstInfo), cudaMemcpyHostToDevice, st));
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_tiles, p->tiles.data(),
+                                p->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
+  GD_CHECK_CUDA(cudaStreamSynchronize(st));
+  return GD_OK;
+}
+
+extern "C" int gd_plan_set_mask(gd_plan p, int32_t i, const uint8_t *mask, int32_t mpitch,
+                                cudaStream_t st) {
+  GD_REQUIRE(p && p->ws && mask && i >= 0 && i < p->n, GD_ERR_ARG,
+             "gd_plan_set_mask: bad arguments or unbound plan");
+  const InstInfo &I = p->inst[i];
+  GD_REQUIRE(I.bc == GD_MASKED, GD_ERR_ARG, "gd_plan_set_mask: instance %d is not masked", i);
+  GD_REQUIRE(mpitch >= I.nx, GD_ERR_ARG, "gd_plan_set_mask: pitch %d < width %d", mpitch, I.nx);
+  unsigned char *codes = (unsigned char *)(p->ws + p->o_codes);
+  const LevelInfo &L0 = p->lv[I.level0];
+  k_codes_fine<<<ceil_div(L0.ny * L0.nx, 256), 256, 0, st>>>(codes + L0.code_off, L0.pitch, mask,
+                                                             mpitch, L0.ny, L0.nx);
+  for (int l = I.level0 + 1; l <= I.coarsest; ++l) {
+    const LevelInfo &F = p->lv[l - 1], &C = p->lv[l];
+    k_codes_coarse_act<<<ceil_div(C.ny * C.nx, 256), 256, 0, st>>>(
+        codes + C.code_off, C.pitch, C.ny, C.nx, codes + F.code_off, F.pitch, F.ny, F.nx);
+    k_codes_classes<<<ceil_div(C.ny * C.nx, 256), 256, 0, st>>>(codes + C.code_off, C.pitch,
+                                                                C.ny, C.nx);
+  }
+  GD_CHECK_LAUNCH();
+  p->mask_set[i] = 1;
+  p->prepared = false;
+  return GD_OK;
+}
+
+extern "C" int gd_plan_prepare(gd_plan p, cudaStream_t st) {
+  GD_REQUIRE(p && p->ws, GD_ERR_STATE, "gd_plan_prepare: plan is not bound");
+  for (int i = 0; i < p->n; ++i)
+    GD_REQUIRE(p->inst[i].bc != GD_MASKED || p->mask_set[i], GD_ERR_STATE,
+               "gd_plan_prepare: masked instance %d has no mask", i);
+  k_coarse_inverse<<<p->n, 256, 0, st>>>(
+      reinterpret_cast<const LevelInfo *>(p->ws + p->o_lv),
+      reinterpret_cast<const InstInfo *>(p->ws + p->o_inst),
+      reinterpret_cast<const unsigned char *>(p->ws + p->o_codes),
+      reinterpret_cast<double *>(p->ws + p->o_dense));
+  GD_CHECK_LAUNCH();
+  p->prepared = true;
+  return GD_OK;
+}
+
+namespace {
+
+template <typename T>
+int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
+  const Args<T> a = Runner<T>::args(p);
+  const Args<T> fine = Runner<T>::at_tiles(a, p->fine_base);
+  prof_begin(p, GD_K_INIT, p->fine_cells, st);
+  k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  k_resid<T, true><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  prof_end(p, st);
+  GD_CHECK_LAUNCH();
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+  GD_CHECK_CUDA(cudaStreamSynchronize(st));
+  const bool graph = p->prm.use_graph && !p->profiling;
+  if (graph && !p->gexec) {
+    if (!p->cap) GD_CHECK_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    GD_CHECK_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    Runner<T>::dispatch_iteration(p, a, p->cap);
+    GD_CHECK_CUDA(cudaStreamEndCapture(p->cap, &g));
+    const cudaError_t e = cudaGraphInstantiate(&p->gexec, g, 0);
+    cudaGraphDestroy(g);
+    GD_CHECK_CUDA(e);
+  }
+  const int chunk = p->prm.check_every;
+  const long long cap_iters = (long long)p->prm.max_iterations + 2ll * chunk + 8;
+  long long done = 0;
+  while (*p->h_nact > 0 && done < cap_iters) {
+    for (int c = 0; c < chunk; ++c) {
+      if (graph) GD_CHECK_CUDA(cudaGraphLaunch(p->gexec, st));
+      else Runner<T>::dispatch_iteration(p, a, st);
+    }
+    GD_CHECK_LAUNCH();
+    done += chunk;
+    GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
+                                  cudaMemcpyDeviceToHost, st));
+    GD_CHECK_CUDA(cudaStreamSynchronize(st));
+    prof_collect(p);
+  }
+  bool any_mean = false;
+  for (int i = 0; i < p->n; ++i) any_mean |= p->inst[i].zero_mean != 0;
+  if (any_mean) {
+    prof_begin(p, GD_K_MEAN, p->fine_cells, st);
+    k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+    k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+    prof_end(p, st);
+    GD_CHECK_LAUNCH();
+  }
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->h_st, p->ws + p->o_st, sizeof(InstState) * p->n,
+                                cudaMemcpyDeviceToHost, st));
+  GD_CHECK_CUDA(cudaStreamSynchronize(st));
+  prof_collect(p);
+  for (int i = 0; i < p->n; ++i) {
+    const InstState &S = p->h_st[i];
+    gd_report &R = reports[i];
+    R.iterations = S.iters;
+    R.status = S.status == GD_ACTIVE ? GD_MAX_ITERATIONS : S.status;
+    R.initial_norm = std::sqrt(S.ff);
+    R.relative_residual = S.ff > 0.0 ? std::sqrt(S.rr_true / S.ff) : 0.0;
+  }
+  return GD_OK;
+}
+
+}  // namespace
+
+extern "C" int gd_solve(gd_plan p, const double *const *f, double *const *x, const int32_t *pitch,
+                        const double *scale, cudaStream_t st, gd_report *reports) {
+  GD_REQUIRE(p && f && x && pitch && scale && reports, GD_ERR_ARG, "gd_solve: bad arguments");
+  GD_REQUIRE(p->ws && p->prepared, GD_ERR_STATE, "gd_solve: plan not bound and prepared");
+  for (int i = 0; i < p->n; ++i) {
+    GD_REQUIRE(f[i] && x[i] && pitch[i] >= p->inst[i].nx, GD_ERR_ARG,
+               "gd_solve: instance %d has a bad pointer or pitch", i);
+    p->inst[i].f = f[i];
+    p->inst[i].x = x[i];
+    p->inst[i].upitch = pitch[i];
+    p->inst[i].scale = scale[i];
+  }
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->inst.data(),
+                                p->inst.size() * sizeof(InstInfo), cudaMemcpyHostToDevice, st));
+  return p->fp64 ? run_solve<double>(p, st, reports) : run_solve<float>(p, st, reports);
+}
+
+namespace {
+template <typename T>
+int run_apply_vcycle(gd_plan p, int i, const double *r, double *z, int pitch, cudaStream_t st) {
+  const InstInfo &I = p->inst[i];
+  for (int k = 0; k < p->n; ++k) {
+    std::memset(&p->h_st[k], 0, sizeof(InstState));
+    p->h_st[k].status = (k == i) ? GD_ACTIVE : GD_CONVERGED;
+    p->h_st[k].first = 1;
+  }
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_st, p->h_st, sizeof(InstState) * p->n,
+                                cudaMemcpyHostToDevice, st));
+  T *arena = reinterpret_cast<T *>(p->ws + p->o_arena);
+  const int cells = I.ny * I.nx;
+  k_load_r<T><<<ceil_div(cells, 256), 256, 0, st>>>(arena + I.r_off, I.pitch, r, pitch, I.ny,
+                                                    I.nx);
+  Runner<T>::dispatch_vcycle(p, Runner<T>::args(p), st);
+  k_store_z<T><<<ceil_div(cells, 256), 256, 0, st>>>(z, pitch, arena + I.z_off, I.pitch, I.ny,
+                                                     I.nx);
+  GD_CHECK_LAUNCH();
+  GD_CHECK_CUDA(cudaStreamSynchronize(st));
+  return GD_OK;
+}
+}  // namespace
+
+extern "C" int gd_plan_apply_vcycle(gd_plan p, int32_t i, const double *r, double *z,
+                                    int32_t pitch, cudaStream_t st) {
+  GD_REQUIRE(p && r && z && i >= 0 && i < p->n, GD_ERR_ARG, "gd_plan_apply_vcycle: bad arguments");
+  GD_REQUIRE(p->ws && p->prepared, GD_ERR_STATE, "gd_plan_apply_vcycle: plan not prepared");
+  GD_REQUIRE(pitch >= p->inst[i].nx, GD_ERR_ARG, "gd_plan_apply_vcycle: bad pitch");
+  return p->fp64 ? run_apply_vcycle<double>(p, i, r, z, pitch, st)
+                 : run_apply_vcycle<float>(p, i, r, z, pitch, st);
+}
+
+extern "C" int gd_plan_set_profiling(gd_plan p, int32_t enable) {
+  GD_REQUIRE(p, GD_ERR_ARG, "gd_plan_set_profiling: null plan");
+  p->profiling = enable != 0;
+  for (int k = 0; k < GD_KERNEL_KINDS; ++k) {
+    p->prof_ms[k] = 0.0;
+    p->prof_cells[k] = 0.0;
+    p->prof_launches[k] = 0;
+  }
+  p->ev_used = 0;
+  return GD_OK;
+}
+
+extern "C" int gd_plan_kernel_times(gd_plan p, gd_kernel_time *out, int32_t n) {
+  GD_REQUIRE(p && out && n >= GD_KERNEL_KINDS, GD_ERR_ARG,
+             "gd_plan_kernel_times: need room for %d entries", GD_KERNEL_KINDS);
+  for (int k = 0; k < GD_KERNEL_KINDS; ++k) {
+    out[k].launches = p->prof_launches[k];
+    out[k].milliseconds = p->prof_ms[k];
+    out[k].cells = p->prof_cells[k];
+  }
+  return GD_OK;
+}

@@ -1,0 +1,117 @@
+// Data structures and kernel declarations of the batched cell-centred MGPCG.
+#pragma once
+
+#include "gd_internal.cuh"
+
+namespace gd {
+
+// Hierarchy rules.  A level is coarsened (ceil(ny/2) x ceil(nx/2)) while it has
+// more than kCoarsestCells cells; the first level with at most kBottomCells
+// cells and everything below it is handled by one CTA per instance in shared
+// memory; the coarsest level is solved with a dense FP64 inverse.
+constexpr int kCoarsestCells = 64;
+constexpr int kBottomCells = 4096;
+
+// Fine-level Krylov kernels: 16 x 64 cells per CTA, 256 threads.
+constexpr int kFTY = 16, kFTX = 64, kFThreads = 256;
+constexpr int kVThreads = 256;     // down / up kernels
+constexpr int kBThreads = 512;     // bottom kernel
+constexpr int kLastWarps = kFThreads / 32;
+
+enum : int { BC_DIR = 0, BC_NEU = 1, BC_MASK = 2 };
+enum : int { FLAG_RU = 1 };
+
+struct LevelInfo {
+  int ny, nx, pitch, inst;
+  int bc, level, coarse, is_bottom;
+  float wall, pad0;
+  int pad1, pad2;
+  long long b_off, u_off;  // element offsets into the T arena
+  long long code_off;      // byte offset into the code arena, -1 if rectangle
+  long long inv_off;       // coarsest level: element offset of its dense inverse, else -1
+};
+
+struct InstInfo {
+  int ny, nx, pitch, bc;
+  int level0, bottom, coarsest, nlevels;
+  long long r_off, p_off, d_off, z_off;
+  int fine_begin, fine_end;  // tile range in the fine map
+  int up0_begin, up0_end;    // tile range in the level-0 up map (empty if bottom is level 0)
+  int zero_mean, pad;
+  // set per solve
+  const double *f;
+  double *x;
+  long long upitch;
+  double scale;
+  double cells_active;
+};
+
+struct InstState {
+  double rz, beta, pAp, alpha, rr, rr_ref, ff, rr_true, mean, fmean;
+  int status, iters, flags, first;
+};
+
+struct Tile {
+  int level;  // LevelInfo index (fine level for down/up, level 0 for fine maps)
+  int inst;
+  int ty, tx;
+};
+
+template <typename T>
+struct Args {
+  const LevelInfo *lv;
+  const InstInfo *inst;
+  InstState *st;
+  T *arena;
+  const unsigned char *codes;
+  const double *dense;
+  double *part0;
+  double *part1;
+  unsigned *counter;
+  int *n_active;
+  const Tile *tiles;
+  int ninst;
+  double tol2, delta2;
+  int max_iter;
+};
+
+// Cell class: 0 = no unknown, else 1 + number of walls (missing neighbours).
+__host__ __device__ __forceinline__ int rect_class(int y, int x, int ny, int nx) {
+  return 1 + (y == 0) + (y == ny - 1) + (x == 0) + (x == nx - 1);
+}
+
+__device__ __forceinline__ int cell_class(const LevelInfo &L, const unsigned char *codes, int y,
+                                          int x) {
+  if (y < 0 || y >= L.ny || x < 0 || x >= L.nx) return 0;
+  if (L.code_off >= 0) return codes[L.code_off + (long long)y * L.pitch + x];
+  return rect_class(y, x, L.ny, L.nx);
+}
+
+// Diagonal of the positive operator for a cell of class c on a level with wall
+// coefficient w: interior neighbours count 1, walls count w (Neumann w = 0,
+// Dirichlet w = 1 on the finest level and 2 on coarse levels).
+__host__ __device__ __forceinline__ double class_diag(int c, float w) {
+  return 4.0 - (double)(c - 1) * (1.0 - (double)w);
+}
+
+// Shared-memory layout of the down / up kernels (host and device agree).
+template <typename T, int S1, int S2>
+struct VCfg {
+  static constexpr int CY = sizeof(T) == 4 ? 16 : 8;  // down: coarse output tile
+  static constexpr int CX = 32;
+  static constexpr int DWH = 2 * CY + 4 * S1 + 4;
+  static constexpr int DWW = 2 * CX + 4 * S1 + 4;
+  static constexpr int UTY = 2 * CY, UTX = 2 * CX;  // up: fine output tile
+  static constexpr int UH = 2 * S1 + 2 * S2;
+  static constexpr int UWH = UTY + 2 * UH;
+  static constexpr int UWW = UTX + 2 * UH;
+  static constexpr int UCH = UWH / 2 + 4, UCW = UWW / 2 + 4;
+  static constexpr size_t down_smem() {
+    return (size_t)DWH * DWW * (2 * sizeof(T) + 1) + 16;
+  }
+  static constexpr size_t up_smem() {
+    return (size_t)UWH * UWW * (2 * sizeof(T) + 1) + (size_t)UCH * UCW * sizeof(T) + 16;
+  }
+};
+
+}  // namespace gd

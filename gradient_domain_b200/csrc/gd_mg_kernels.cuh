@@ -1,0 +1,877 @@
+// Kernels of the batched cell-centred MGPCG.  Included by gd_mg.cu only.
+//
+// Operator: A u = d_p u_p - sum of neighbour values, neighbours outside the
+// grid or without an unknown contribute zero; d_p = 4 - walls * (1 - w) with
+// w the level's wall coefficient.  On the finest level this is exactly
+// -h^2 laplacian (Dirichlet, operators.py:86-107), -divergence(gradient(.))
+// (Neumann, test_operators.py:51-57) or the masked Perez matrix negated
+// (poisson.py:190-204).
+//
+// V-cycle (the B200 replacement of multigrid.py:184-215): cell-centred
+// coarsening to ceil(n/2), bilinear prolongation P (weights 3/4, 1/4 per axis,
+// Neumann ghosts mirror, Dirichlet ghosts zero), restriction R = P^T,
+// red-black Gauss-Seidel with colour 0 then 1 before restriction and colour 1
+// then 0 after prolongation, so the cycle is a symmetric operator.  Each level
+// costs two passes over HBM: `k_down` smooths from zero, forms the residual and
+// restricts it in one shared-memory tile; `k_up` recomputes that pre-smoothed
+// iterate from b instead of storing it, adds P e and post-smooths.  Small
+// levels run in `k_bottom`, one CTA per instance, down to a dense FP64 solve.
+#pragma once
+
+#include "gd_mg.cuh"
+
+namespace gd {
+
+__device__ __forceinline__ bool in_grid(const LevelInfo &L, int y, int x) {
+  return y >= 0 && y < L.ny && x >= 0 && x < L.nx;
+}
+
+// Last-CTA handshake: every CTA calls it once; returns true in the last one.
+__device__ __forceinline__ bool last_block(unsigned *counter) {
+  __shared__ bool am_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(counter, 1u);
+    am_last = (prev == gridDim.x - 1);
+    if (am_last) *counter = 0u;
+  }
+  __syncthreads();
+  if (am_last) __threadfence();
+  return am_last;
+}
+
+// Deterministic per-instance sum of partials [b, e) by one warp (L2 reads).
+__device__ __forceinline__ double warp_range_sum(const double *p, int b, int e) {
+  double s = 0.0;
+  for (int k = b + (threadIdx.x & 31); k < e; k += 32) s += __ldcg(p + k);
+  return warp_sum(s);
+}
+
+__device__ __forceinline__ void finish_rz(InstState &S, double rz) {
+  if (!(rz > 0.0) || !isfinite(rz)) {
+    S.status = GD_BREAKDOWN;
+    S.flags |= FLAG_RU;
+    return;
+  }
+  S.beta = S.first ? 0.0 : rz / S.rz;
+  S.first = 0;
+  S.rz = rz;
+}
+
+// ---------------------------------------------------------------------------
+// Red-black half sweep on a shared-memory window of H x W cells whose (0, 0)
+// sits at global (Y0, X0).  Edge rows and columns of the window are never
+// updated, so after h half sweeps the values are exact at distance >= h from
+// the window edge; callers size the window for that.
+template <typename T>
+__device__ __forceinline__ void rb_half_window(T *su, const T *sb, const unsigned char *sc,
+                                               const T *dinv, int H, int W, int Y0, int X0,
+                                               int colour) {
+  const int hw = (W - 1) >> 1;
+  const int n = (H - 2) * hw;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int r = k / hw;
+    const int wy = 1 + r;
+    const int wx = 1 + ((colour - (Y0 + wy) - X0 - 1) & 1) + 2 * (k - r * hw);
+    if (wx > W - 2) continue;
+    const int idx = wy * W + wx;
+    const int c = sc[idx];
+    if (c) su[idx] = (sb[idx] + su[idx - W] + su[idx + W] + su[idx - 1] + su[idx + 1]) * dinv[c];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void make_tables(T *diag, T *dinv, float wall) {
+  if (threadIdx.x < 8) {
+    const int c = threadIdx.x;
+    const double d = c >= 1 && c <= 5 ? class_diag(c, wall) : 1.0;
+    diag[c] = (T)d;
+    dinv[c] = (c >= 1 && c <= 5 && d > 0.0) ? (T)(1.0 / d) : (T)0;
+  }
+}
+
+// Bilinear-adjoint weights of one axis for fine offsets 2I-1 .. 2I+2.
+__device__ __forceinline__ float rweight(int a) { return (a == 0 || a == 3) ? 0.25f : 0.75f; }
+
+// Neumann restriction reads the mirrored residual at fine index -1 and, for an
+// even fine size n, at index n (the clamped ghost of P^T).
+__device__ __forceinline__ int mirror_fine(int f, int n, bool neumann) {
+  if (!neumann) return f;
+  if (f == -1) return 0;
+  if (f == n && !(n & 1)) return n - 1;
+  return f;
+}
+
+// ---------------------------------------------------------------------------
+// Down: pre-smooth S1 sweeps from zero, residual, restrict to the coarse RHS.
+template <typename T, int S1>
+__global__ void __launch_bounds__(kVThreads) k_down(Args<T> a, int tile_base) {
+  using C = VCfg<T, S1, 1>;
+  constexpr int H = C::DWH, W = C::DWW;
+  const Tile tl = a.tiles[tile_base + blockIdx.x];
+  if (a.st[tl.inst].status != GD_ACTIVE) return;
+  const LevelInfo L = a.lv[tl.level];
+  const LevelInfo Lc = a.lv[L.coarse];
+  extern __shared__ __align__(16) unsigned char smem[];
+  T *sb = reinterpret_cast<T *>(smem);
+  T *su = sb + H * W;
+  unsigned char *sc = reinterpret_cast<unsigned char *>(su + H * W);
+  __shared__ T diag[8], dinv[8];
+  make_tables(diag, dinv, L.wall);
+
+  const int I0 = tl.ty * C::CY, J0 = tl.tx * C::CX;
+  const int Y0 = 2 * I0 - 2 * S1 - 2, X0 = 2 * J0 - 2 * S1 - 2;
+  const T *B = a.arena + L.b_off;
+  for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+    const int wy = k / W, wx = k - wy * W;
+    const int gy = Y0 + wy, gx = X0 + wx;
+    const int c = cell_class(L, a.codes, gy, gx);
+    sc[k] = (unsigned char)c;
+    sb[k] = c ? B[(long long)gy * L.pitch + gx] : T(0);
+    su[k] = T(0);
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 0; s < S1; ++s) {
+    rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
+    __syncthreads();
+    rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
+    __syncthreads();
+  }
+  // residual, in place over the window interior
+  for (int k = threadIdx.x; k < (H - 2) * (W - 2); k += blockDim.x) {
+    const int r = k / (W - 2);
+    const int idx = (1 + r) * W + 1 + (k - r * (W - 2));
+    const int c = sc[idx];
+    const T nb = su[idx - W] + su[idx + W] + su[idx - 1] + su[idx + 1];
+    sb[idx] = c ? sb[idx] - (diag[c] * su[idx] - nb) : T(0);
+  }
+  __syncthreads();
+  const bool neu = L.bc == BC_NEU;
+  T *Bc = a.arena + Lc.b_off;
+  for (int k = threadIdx.x; k < C::CY * C::CX; k += blockDim.x) {
+    const int I = I0 + k / C::CX, J = J0 + k % C::CX;
+    if (I >= Lc.ny || J >= Lc.nx) continue;
+    T acc = T(0);
+    if (cell_class(Lc, a.codes, I, J)) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int wy = mirror_fine(2 * I - 1 + p, L.ny, neu) - Y0;
+        T row = T(0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int wx = mirror_fine(2 * J - 1 + q, L.nx, neu) - X0;
+          row += (T)rweight(q) * sb[wy * W + wx];
+        }
+        acc += (T)rweight(p) * row;
+      }
+    }
+    Bc[(long long)I * Lc.pitch + J] = acc;
+  }
+}
+
+// Coarse value for interpolation: Neumann ghosts mirror the edge, Dirichlet
+// ghosts are zero.
+template <typename T>
+__device__ __forceinline__ T coarse_at(const T *E, const LevelInfo &Lc, int cy, int cx, bool neu) {
+  if (neu) {
+    cy = min(max(cy, 0), Lc.ny - 1);
+    cx = min(max(cx, 0), Lc.nx - 1);
+  } else if (cy < 0 || cy >= Lc.ny || cx < 0 || cx >= Lc.nx) {
+    return T(0);
+  }
+  return E[(long long)cy * Lc.pitch + cx];
+}
+
+// ---------------------------------------------------------------------------
+// Up: recompute the pre-smoothed iterate, add P e, post-smooth S2 sweeps.
+// On level 0 it also accumulates r.z for the Krylov step.
+template <typename T, int S1, int S2, bool LEVEL0>
+__global__ void __launch_bounds__(kVThreads) k_up(Args<T> a, int tile_base) {
+  using C = VCfg<T, S1, S2>;
+  constexpr int H = C::UWH, W = C::UWW, CH = C::UCH, CW = C::UCW;
+  const Tile tl = a.tiles[tile_base + blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const LevelInfo L = a.lv[tl.level];
+    const LevelInfo Lc = a.lv[L.coarse];
+    extern __shared__ __align__(16) unsigned char smem[];
+    T *sb = reinterpret_cast<T *>(smem);
+    T *su = sb + H * W;
+    T *se = su + H * W;
+    unsigned char *sc = reinterpret_cast<unsigned char *>(se + CH * CW);
+    __shared__ T diag[8], dinv[8];
+    make_tables(diag, dinv, L.wall);
+    const int Y0 = tl.ty * C::UTY - C::UH, X0 = tl.tx * C::UTX - C::UH;
+    const int CY0 = (Y0 >> 1) - 1, CX0 = (X0 >> 1) - 1;
+    const T *B = a.arena + L.b_off;
+    const T *E = a.arena + Lc.u_off;
+    const bool neu = L.bc == BC_NEU;
+    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+      const int wy = k / W, wx = k - wy * W;
+      const int gy = Y0 + wy, gx = X0 + wx;
+      const int c = cell_class(L, a.codes, gy, gx);
+      sc[k] = (unsigned char)c;
+      sb[k] = c ? B[(long long)gy * L.pitch + gx] : T(0);
+      su[k] = T(0);
+    }
+    for (int k = threadIdx.x; k < CH * CW; k += blockDim.x) {
+      const int cy = k / CW, cx = k - cy * CW;
+      se[k] = coarse_at(E, Lc, CY0 + cy, CX0 + cx, neu);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int s = 0; s < S1; ++s) {
+      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
+      __syncthreads();
+      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
+      __syncthreads();
+    }
+    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+      if (!sc[k]) continue;
+      const int wy = k / W, wx = k - wy * W;
+      const int gy = Y0 + wy, gx = X0 + wx;
+      const int cy = (gy >> 1) - CY0, cx = (gx >> 1) - CX0;
+      const int cy2 = (gy & 1) ? cy + 1 : cy - 1;
+      const int cx2 = (gx & 1) ? cx + 1 : cx - 1;
+      const T e = (T)0.5625 * se[cy * CW + cx] +
+                  (T)0.1875 * (se[cy2 * CW + cx] + se[cy * CW + cx2]) +
+                  (T)0.0625 * se[cy2 * CW + cx2];
+      su[k] += e;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int s = 0; s < S2; ++s) {
+      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
+      __syncthreads();
+      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
+      __syncthreads();
+    }
+    T *U = a.arena + L.u_off;
+    for (int k = threadIdx.x; k < C::UTY * C::UTX; k += blockDim.x) {
+      const int oy = k / C::UTX, ox = k - oy * C::UTX;
+      const int gy = Y0 + C::UH + oy, gx = X0 + C::UH + ox;
+      if (gy >= L.ny || gx >= L.nx) continue;
+      const int idx = (C::UH + oy) * W + C::UH + ox;
+      const T v = sc[idx] ? su[idx] : T(0);
+      U[(long long)gy * L.pitch + gx] = v;
+      if (LEVEL0) part += (double)sb[idx] * (double)v;
+    }
+  }
+  if (!LEVEL0) return;
+  part = block_sum<kVThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 3)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < a.ninst; i += nw) {
+    const InstInfo &I = a.inst[i];
+    if (I.up0_end <= I.up0_begin) continue;
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const double rz = warp_range_sum(a.part0, I.up0_begin, I.up0_end);
+    if ((threadIdx.x & 31) == 0) finish_rz(S, rz);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bottom: the remaining V-cycle of one instance in shared memory.
+struct BottomLevel {
+  int ny, nx, bc;
+  float wall;
+  int off_b, off_u, off_c;  // shared-memory offsets (T elements / bytes)
+};
+
+template <typename T>
+__device__ __forceinline__ T sm_at(const T *u, int y, int x, int ny, int nx) {
+  return (y >= 0 && y < ny && x >= 0 && x < nx) ? u[y * nx + x] : T(0);
+}
+
+template <typename T>
+__device__ void bottom_smooth(T *u, const T *b, const unsigned char *c, const BottomLevel &L,
+                              const T *dinv, int colour) {
+  const int hw = (L.nx + 1) >> 1;
+  for (int k = threadIdx.x; k < L.ny * hw; k += blockDim.x) {
+    const int y = k / hw;
+    const int x = 2 * (k - y * hw) + ((colour + y) & 1);
+    if (x >= L.nx) continue;
+    const int i = y * L.nx + x;
+    const int cl = c[i];
+    if (cl)
+      u[i] = (b[i] + sm_at(u, y - 1, x, L.ny, L.nx) + sm_at(u, y + 1, x, L.ny, L.nx) +
+              sm_at(u, y, x - 1, L.ny, L.nx) + sm_at(u, y, x + 1, L.ny, L.nx)) * dinv[cl];
+  }
+  __syncthreads();
+}
+
+template <typename T, int S1, int S2>
+__global__ void __launch_bounds__(kBThreads) k_bottom(Args<T> a) {
+  const int inst = blockIdx.x;
+  InstState &S = a.st[inst];
+  if (S.status != GD_ACTIVE) return;
+  const InstInfo &I = a.inst[inst];
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ BottomLevel bl[24];
+  __shared__ T tdiag[24][8], tdinv[24][8];
+  __shared__ int nb_s, res_off_s, dense_off_s, cbytes_off_s;
+  if (threadIdx.x == 0) {
+    int nb = 0, off = 0;
+    for (int l = I.bottom;; ++l) {
+      const LevelInfo &L = a.lv[l];
+      BottomLevel &B = bl[nb++];
+      B.ny = L.ny; B.nx = L.nx; B.bc = L.bc; B.wall = L.wall;
+      B.off_b = off; off += L.ny * L.nx;
+      B.off_u = off; off += L.ny * L.nx;
+      if (l == I.coarsest || nb == 24) break;
+    }
+    nb_s = nb;
+    res_off_s = off;
+    off += bl[0].ny * bl[0].nx;
+    // double buffer for the dense solve, 8-byte aligned in T units
+    off = (off * (int)sizeof(T) + 7) / 8 * 8 / (int)sizeof(T);
+    dense_off_s = off;
+    off += 2 * kCoarsestCells * (int)(sizeof(double) / sizeof(T));
+    int cb = off * (int)sizeof(T);
+    for (int q = 0; q < nb; ++q) { bl[q].off_c = cb; cb += bl[q].ny * bl[q].nx; }
+    cbytes_off_s = cb;
+  }
+  __syncthreads();
+  const int nb = nb_s;
+  T *sm = reinterpret_cast<T *>(smem);
+  for (int q = threadIdx.x; q < nb * 8; q += blockDim.x) {
+    const int l = q >> 3, c = q & 7;
+    const double d = c >= 1 && c <= 5 ? class_diag(c, bl[l].wall) : 1.0;
+    tdiag[l][c] = (T)d;
+    tdinv[l][c] = (c >= 1 && c <= 5) ? (T)(1.0 / d) : T(0);
+  }
+  // classes of every level, and b of the bottom level
+  for (int q = 0; q < nb; ++q) {
+    const LevelInfo &L = a.lv[I.bottom + q];
+    unsigned char *c = smem + bl[q].off_c;
+    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
+      const int y = k / L.nx, x = k - y * L.nx;
+      c[k] = (unsigned char)cell_class(L, a.codes, y, x);
+    }
+  }
+  {
+    const LevelInfo &L = a.lv[I.bottom];
+    const T *B = a.arena + L.b_off;
+    T *b0 = sm + bl[0].off_b;
+    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
+      const int y = k / L.nx, x = k - y * L.nx;
+      b0[k] = B[(long long)y * L.pitch + x];
+    }
+  }
+  __syncthreads();
+  T *res = sm + res_off_s;
+  for (int q = 0; q + 1 < nb; ++q) {
+    const BottomLevel &L = bl[q];
+    T *u = sm + L.off_u;
+    const T *b = sm + L.off_b;
+    const unsigned char *c = smem + L.off_c;
+    const int n = L.ny * L.nx;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = T(0);
+    __syncthreads();
+    for (int s = 0; s < S1; ++s) {
+      bottom_smooth(u, b, c, L, tdinv[q], 0);
+      bottom_smooth(u, b, c, L, tdinv[q], 1);
+    }
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int y = k / L.nx, x = k - y * L.nx;
+      const int cl = c[k];
+      const T nbs = sm_at(u, y - 1, x, L.ny, L.nx) + sm_at(u, y + 1, x, L.ny, L.nx) +
+                    sm_at(u, y, x - 1, L.ny, L.nx) + sm_at(u, y, x + 1, L.ny, L.nx);
+      res[k] = cl ? b[k] - (tdiag[q][cl] * u[k] - nbs) : T(0);
+    }
+    __syncthreads();
+    const BottomLevel &Cl = bl[q + 1];
+    T *bc = sm + Cl.off_b;
+    const unsigned char *cc = smem + Cl.off_c;
+    const bool neu = L.bc == BC_NEU;
+    for (int k = threadIdx.x; k < Cl.ny * Cl.nx; k += blockDim.x) {
+      const int Iy = k / Cl.nx, Jx = k - Iy * Cl.nx;
+      T acc = T(0);
+      if (cc[k]) {
+        for (int p = 0; p < 4; ++p) {
+          const int fy = mirror_fine(2 * Iy - 1 + p, L.ny, neu);
+          T row = T(0);
+          for (int r = 0; r < 4; ++r) {
+            const int fx = mirror_fine(2 * Jx - 1 + r, L.nx, neu);
+            row += (T)rweight(r) * sm_at(res, fy, fx, L.ny, L.nx);
+          }
+          acc += (T)rweight(p) * row;
+        }
+      }
+      bc[k] = acc;
+    }
+    __syncthreads();
+  }
+  {  // coarsest: dense FP64 inverse
+    const BottomLevel &L = bl[nb - 1];
+    const int n = L.ny * L.nx;
+    double *bd = reinterpret_cast<double *>(sm + dense_off_s);
+    const T *b = sm + L.off_b;
+    T *u = sm + L.off_u;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) bd[k] = (double)b[k];
+    __syncthreads();
+    const double *inv = a.dense + a.lv[I.coarsest].inv_off;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      double acc = 0.0;
+      for (int j = 0; j < n; ++j) acc += inv[(long long)t * n + j] * bd[j];
+      u[t] = (T)acc;
+    }
+    __syncthreads();
+  }
+  for (int q = nb - 2; q >= 0; --q) {
+    const BottomLevel &L = bl[q];
+    const BottomLevel &Cl = bl[q + 1];
+    T *u = sm + L.off_u;
+    const T *b = sm + L.off_b;
+    const T *e = sm + Cl.off_u;
+    const unsigned char *c = smem + L.off_c;
+    const bool neu = L.bc == BC_NEU;
+    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
+      if (!c[k]) continue;
+      const int y = k / L.nx, x = k - y * L.nx;
+      const int cy = y >> 1, cx = x >> 1;
+      const int cy2 = (y & 1) ? cy + 1 : cy - 1, cx2 = (x & 1) ? cx + 1 : cx - 1;
+      auto E = [&](int yy, int xx) -> T {
+        if (neu) {
+          yy = min(max(yy, 0), Cl.ny - 1);
+          xx = min(max(xx, 0), Cl.nx - 1);
+          return e[yy * Cl.nx + xx];
+        }
+        return sm_at(e, yy, xx, Cl.ny, Cl.nx);
+      };
+      u[k] += (T)0.5625 * E(cy, cx) + (T)0.1875 * (E(cy2, cx) + E(cy, cx2)) +
+              (T)0.0625 * E(cy2, cx2);
+    }
+    __syncthreads();
+    for (int s = 0; s < S2; ++s) {
+      bottom_smooth(u, b, c, L, tdinv[q], 1);
+      bottom_smooth(u, b, c, L, tdinv[q], 0);
+    }
+  }
+  const LevelInfo &L0 = a.lv[I.bottom];
+  T *U = a.arena + L0.u_off;
+  const T *u0 = sm + bl[0].off_u;
+  const T *b0 = sm + bl[0].off_b;
+  double part = 0.0;
+  for (int k = threadIdx.x; k < L0.ny * L0.nx; k += blockDim.x) {
+    const int y = k / L0.nx, x = k - y * L0.nx;
+    U[(long long)y * L0.pitch + x] = u0[k];
+    part += (double)b0[k] * (double)u0[k];
+  }
+  if (I.bottom == I.level0) {
+    part = block_sum<kBThreads>(part);
+    if (threadIdx.x == 0) finish_rz(S, part);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fine-level Krylov kernels over 16 x 64 tiles of level 0.
+
+template <typename T, typename V>
+__device__ __forceinline__ T apply_tile(const V *s, int idx, int c, const T *diag) {
+  constexpr int W = kFTX + 2;
+  return c ? (T)(diag[c] * (T)s[idx] - (T)(s[idx - W] + s[idx + W] + s[idx - 1] + s[idx + 1]))
+           : T(0);
+}
+
+// p = z + beta p and the partial p.Ap; the last CTA forms alpha = rz / pAp.
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_pupdate(Args<T> a) {
+  constexpr int W = kFTX + 2, H = kFTY + 2;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    __shared__ T sp[H * W];
+    __shared__ T diag[8], dinv[8];
+    make_tables(diag, dinv, L.wall);
+    const T beta = (T)a.st[tl.inst].beta;
+    const T *z = a.arena + I.z_off;
+    T *p = a.arena + I.p_off;
+    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
+    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+      const int wy = k / W, wx = k - wy * W;
+      const int gy = Y0 + wy, gx = X0 + wx;
+      T v = T(0);
+      if (in_grid(L, gy, gx)) {
+        const long long g = (long long)gy * L.pitch + gx;
+        v = z[g] + beta * p[g];
+      }
+      sp[k] = v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+      const int oy = k / kFTX, ox = k - oy * kFTX;
+      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
+      if (gy >= L.ny || gx >= L.nx) continue;
+      const int idx = (1 + oy) * W + 1 + ox;
+      const int c = cell_class(L, a.codes, gy, gx);
+      const T pv = sp[idx];
+      part += (double)pv * (double)apply_tile<T, T>(sp, idx, c, diag);
+      p[(long long)gy * L.pitch + gx] = pv;
+    }
+  }
+  part = block_sum<kFThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 0)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kLastWarps) {
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const InstInfo &I = a.inst[i];
+    const double pAp = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+    if ((threadIdx.x & 31) == 0) {
+      const double alpha = S.rz / pAp;
+      S.pAp = pAp;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        S.status = GD_BREAKDOWN;
+        S.flags |= FLAG_RU;
+      } else {
+        S.alpha = alpha;
+      }
+    }
+  }
+}
+
+// d += alpha p, r -= alpha A p and the partial r.r; the last CTA counts the
+// iteration and schedules an FP64 residual refresh when due.
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_cgupdate(Args<T> a) {
+  constexpr int W = kFTX + 2, H = kFTY + 2;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    __shared__ T sp[H * W];
+    __shared__ T diag[8], dinv[8];
+    make_tables(diag, dinv, L.wall);
+    const T alpha = (T)a.st[tl.inst].alpha;
+    const T *p = a.arena + I.p_off;
+    T *d = a.arena + I.d_off;
+    T *r = a.arena + I.r_off;
+    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
+    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+      const int wy = k / W, wx = k - wy * W;
+      const int gy = Y0 + wy, gx = X0 + wx;
+      sp[k] = in_grid(L, gy, gx) ? p[(long long)gy * L.pitch + gx] : T(0);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+      const int oy = k / kFTX, ox = k - oy * kFTX;
+      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
+      if (gy >= L.ny || gx >= L.nx) continue;
+      const int idx = (1 + oy) * W + 1 + ox;
+      const int c = cell_class(L, a.codes, gy, gx);
+      const long long g = (long long)gy * L.pitch + gx;
+      const T ap = apply_tile<T, T>(sp, idx, c, diag);
+      d[g] += alpha * sp[idx];
+      const T rn = r[g] - alpha * ap;
+      r[g] = rn;
+      part += (double)rn * (double)rn;
+    }
+  }
+  part = block_sum<kFThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 1)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kLastWarps) {
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const InstInfo &I = a.inst[i];
+    const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+    if ((threadIdx.x & 31) == 0) {
+      S.rr = rr;
+      S.iters += 1;
+      if (rr <= a.delta2 * S.rr_ref || rr <= a.tol2 * S.ff || S.iters >= a.max_iter ||
+          !isfinite(rr))
+        S.flags |= FLAG_RU;
+    }
+  }
+}
+
+// x += d, d = 0 for instances with a pending FP64 refresh.
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  if (!(a.st[tl.inst].flags & FLAG_RU)) return;
+  const InstInfo &I = a.inst[tl.inst];
+  T *d = a.arena + I.d_off;
+  const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
+  for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+    const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
+    if (gy >= I.ny || gx >= I.nx) continue;
+    const long long g = (long long)gy * I.pitch + gx;
+    I.x[(long long)gy * I.upitch + gx] += (double)d[g];
+    d[g] = T(0);
+  }
+}
+
+// FP64 residual r = scale f - A x of the refreshed (or, with INIT, initial)
+// iterate, its norm, and the convergence decision.
+template <typename T, bool INIT>
+__global__ void __launch_bounds__(kFThreads) k_resid(Args<T> a) {
+  constexpr int W = kFTX + 2, H = kFTY + 2;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
+  double part = 0.0, part_f = 0.0;
+  if (work) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    __shared__ double sx[H * W];
+    __shared__ double diag[8], dinv[8];
+    make_tables(diag, dinv, L.wall);
+    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
+    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
+      const int wy = k / W, wx = k - wy * W;
+      const int gy = Y0 + wy, gx = X0 + wx;
+      const int c = cell_class(L, a.codes, gy, gx);
+      sx[k] = c ? I.x[(long long)gy * I.upitch + gx] : 0.0;
+    }
+    __syncthreads();
+    T *r = a.arena + I.r_off;
+    const double fmean = a.st[tl.inst].fmean;
+    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+      const int oy = k / kFTX, ox = k - oy * kFTX;
+      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
+      if (gy >= L.ny || gx >= L.nx) continue;
+      const int idx = (1 + oy) * W + 1 + ox;
+      const int c = cell_class(L, a.codes, gy, gx);
+      const long long g = (long long)gy * L.pitch + gx;
+      const long long gu = (long long)gy * I.upitch + gx;
+      const double f = c ? I.scale * (I.f[gu] - fmean) : 0.0;
+      const double r64 = c ? f - apply_tile<double, double>(sx, idx, c, diag) : 0.0;
+      r[g] = (T)r64;
+      part += r64 * r64;
+      if (INIT) {
+        part_f += f * f;
+        a.arena[I.d_off + g] = T(0);
+        a.arena[I.p_off + g] = T(0);
+        a.arena[I.z_off + g] = T(0);
+        if (!c) I.x[gu] = 0.0;
+      }
+    }
+  }
+  part = block_sum<kFThreads>(part);
+  if (INIT) {
+    __syncthreads();
+    part_f = block_sum<kFThreads>(part_f);
+  }
+  if (threadIdx.x == 0) {
+    a.part0[blockIdx.x] = part;
+    if (INIT) a.part1[blockIdx.x] = part_f;
+  }
+  if (!last_block(a.counter + 2)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int active = 0;
+  for (int i = warp; i < a.ninst; i += kLastWarps) {
+    InstState &S = a.st[i];
+    const InstInfo &I = a.inst[i];
+    const bool part_of = INIT || (S.flags & FLAG_RU);
+    if (part_of) {
+      const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+      double ff = 0.0;
+      if (INIT) ff = warp_range_sum(a.part1, I.fine_begin, I.fine_end);
+      if (lane == 0) {
+        if (INIT) {
+          S.ff = ff;
+          S.iters = 0;
+          S.first = 1;
+          S.rz = 0.0;
+          S.beta = 0.0;
+          S.status = GD_ACTIVE;
+        }
+        S.rr_true = rr;
+        S.rr_ref = rr;
+        S.rr = rr;
+        if (rr <= a.tol2 * S.ff) {
+          S.status = GD_CONVERGED;
+        } else if (!isfinite(rr)) {
+          S.status = GD_BREAKDOWN;
+        } else if (S.status == GD_ACTIVE && S.iters >= a.max_iter) {
+          S.status = GD_MAX_ITERATIONS;
+        }
+        S.flags = 0;
+      }
+    }
+    if (lane == 0 && S.status == GD_ACTIVE) ++active;
+  }
+  __shared__ int cnt[kLastWarps];
+  if (lane == 0) cnt[warp] = active;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kLastWarps; ++w) t += cnt[w];
+    *a.n_active = t;
+  }
+}
+
+// Mean of the right-hand side of zero-mean (Neumann) instances: the constant
+// component of f is outside the range of A and is dropped, as the DCT solver
+// drops it by zeroing the DC coefficient (solvers.py:258-261).
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_fmean(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  const InstInfo &I = a.inst[tl.inst];
+  double part = 0.0;
+  if (I.zero_mean) {
+    const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
+    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+      const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
+      if (gy < I.ny && gx < I.nx) part += I.f[(long long)gy * I.upitch + gx];
+    }
+  }
+  part = block_sum<kFThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 5)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kLastWarps) {
+    const InstInfo &J = a.inst[i];
+    const double s = J.zero_mean ? warp_range_sum(a.part0, J.fine_begin, J.fine_end) : 0.0;
+    if ((threadIdx.x & 31) == 0) a.st[i].fmean = s / ((double)J.ny * (double)J.nx);
+  }
+}
+
+// Mean removal for zero-mean (Neumann) instances: partial sums, then subtract.
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  const InstInfo &I = a.inst[tl.inst];
+  double part = 0.0;
+  if (I.zero_mean) {
+    const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
+    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+      const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
+      if (gy < I.ny && gx < I.nx) part += I.x[(long long)gy * I.upitch + gx];
+    }
+  }
+  part = block_sum<kFThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 4)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kLastWarps) {
+    const InstInfo &J = a.inst[i];
+    if (!J.zero_mean) continue;
+    const double s = warp_range_sum(a.part0, J.fine_begin, J.fine_end);
+    if ((threadIdx.x & 31) == 0) a.st[i].mean = s / ((double)J.ny * (double)J.nx);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  const InstInfo &I = a.inst[tl.inst];
+  if (!I.zero_mean) return;
+  const double m = a.st[tl.inst].mean;
+  const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
+  for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
+    const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
+    if (gy < I.ny && gx < I.nx) I.x[(long long)gy * I.upitch + gx] -= m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Setup kernels.
+
+// Level-0 classes of a masked instance from the caller's unknown mask.
+__global__ void k_codes_fine(unsigned char *code, int pitch, const unsigned char *mask,
+                             int mpitch, int ny, int nx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ny * nx) return;
+  const int y = k / nx, x = k - y * nx;
+  auto on = [&](int yy, int xx) {
+    return yy >= 0 && yy < ny && xx >= 0 && xx < nx && mask[(long long)yy * mpitch + xx] != 0;
+  };
+  unsigned char c = 0;
+  if (on(y, x)) c = (unsigned char)(1 + !on(y - 1, x) + !on(y + 1, x) + !on(y, x - 1) + !on(y, x + 1));
+  code[(long long)y * pitch + x] = c;
+}
+
+// Coarse activity: a coarse cell has an unknown when any of its children has.
+__global__ void k_codes_coarse_act(unsigned char *cc, int cpitch, int cny, int cnx,
+                                   const unsigned char *fc, int fpitch, int fny, int fnx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= cny * cnx) return;
+  const int y = k / cnx, x = k - y * cnx;
+  int any = 0;
+  for (int dy = 0; dy < 2; ++dy)
+    for (int dx = 0; dx < 2; ++dx) {
+      const int fy = 2 * y + dy, fx = 2 * x + dx;
+      if (fy < fny && fx < fnx && fc[(long long)fy * fpitch + fx]) any = 1;
+    }
+  cc[(long long)y * cpitch + x] = (unsigned char)any;
+}
+
+// Turn activity flags into classes (1 + walls); in place is safe because a
+// value is non-zero exactly when the cell is active, before and after.
+__global__ void k_codes_classes(unsigned char *cc, int pitch, int ny, int nx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ny * nx) return;
+  const int y = k / nx, x = k - y * nx;
+  auto on = [&](int yy, int xx) {
+    return yy >= 0 && yy < ny && xx >= 0 && xx < nx && cc[(long long)yy * pitch + xx] != 0;
+  };
+  if (!on(y, x)) return;
+  const int w = !on(y - 1, x) + !on(y + 1, x) + !on(y, x - 1) + !on(y, x + 1);
+  cc[(long long)y * pitch + x] = (unsigned char)(1 + w);
+}
+
+// Dense FP64 inverse of the coarsest operator of each instance by in-place
+// Gauss-Jordan (the matrix is SPD, or SPD after adding J/n for Neumann).
+__global__ void __launch_bounds__(256) k_coarse_inverse(const LevelInfo *lv, const InstInfo *inst,
+                                                        const unsigned char *codes,
+                                                        double *dense) {
+  const InstInfo &I = inst[blockIdx.x];
+  const LevelInfo L = lv[I.coarsest];
+  const int n = L.ny * L.nx;
+  __shared__ double A[kCoarsestCells * kCoarsestCells];
+  __shared__ unsigned char cls[kCoarsestCells];
+  for (int k = threadIdx.x; k < n; k += blockDim.x)
+    cls[k] = (unsigned char)cell_class(L, codes, k / L.nx, k % L.nx);
+  __syncthreads();
+  const double reg = (L.bc == BC_NEU) ? 1.0 / n : 0.0;
+  for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+    const int i = k / n, j = k - i * n;
+    const int yi = i / L.nx, xi = i - yi * L.nx, yj = j / L.nx, xj = j - yj * L.nx;
+    double v = reg;
+    if (!cls[i] || !cls[j]) {
+      v = (i == j && !cls[i]) ? 1.0 : 0.0;
+    } else if (i == j) {
+      v += class_diag(cls[i], L.wall);
+    } else if (abs(yi - yj) + abs(xi - xj) == 1) {
+      v -= 1.0;
+    }
+    A[k] = v;
+  }
+  __syncthreads();
+  __shared__ double piv_inv;
+  __shared__ double colk[kCoarsestCells];
+  for (int k = 0; k < n; ++k) {
+    if (threadIdx.x == 0) piv_inv = 1.0 / A[k * n + k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      A[k * n + j] = (j == k ? 1.0 : A[k * n + j]) * piv_inv;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) colk[i] = A[i * n + k];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      const int i = q / n, j = q - i * n;
+      if (i == k) continue;
+      const double f = colk[i];
+      A[q] = (j == k ? 0.0 : A[q]) - f * A[k * n + j];
+    }
+    __syncthreads();
+  }
+  double *out = dense + L.inv_off;
+  for (int k = threadIdx.x; k < n * n; k += blockDim.x) out[k] = A[k];
+}
+
+}  // namespace gd

@@ -1,0 +1,133 @@
+"""Reference-exact geometric multigrid on the GPU.
+
+Same interface and semantics as gradient-domain/src/gradient_domain/multigrid.py:
+``MultigridOptions`` (:47-71), ``MultigridReport`` (:75-108), ``v_cycle``
+(:184-215) and ``solve`` (:218-255).  The V-cycle runs in the library's
+vertex-centred FP64 kernels (``gd_ref_vcycle``), which evaluate every
+smoothing, residual and transfer expression in the reference's order, so one
+cycle matches the NumPy one to rounding and ``solve`` takes the same number of
+cycles.  The B200 solver proper (cell-centred, mixed precision, batched) is
+``gradient_domain_b200.solvers`` method ``"mgcg"``.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+@dataclass
+class MultigridOptions:
+    """Smoother and recursion settings (multigrid.py:47-71)."""
+
+    pre_smoothing: int = 2
+    post_smoothing: int = 2
+    coarsest_size: int = 8
+    coarsest_sweeps: int = 60
+    max_cycles: int = 60
+    tolerance: float = 1e-8
+
+
+@dataclass
+class MultigridReport:
+    """Convergence record of one solve (multigrid.py:75-108)."""
+
+    residuals: list = field(default_factory=list)
+    cycles: int = 0
+    converged: bool = False
+
+    @property
+    def convergence_factor(self) -> float:
+        if len(self.residuals) < 2 or self.residuals[0] <= 0:
+            return float("nan")
+        ratio = self.residuals[-1] / self.residuals[0]
+        return float(ratio ** (1.0 / (len(self.residuals) - 1)))
+
+    def __str__(self) -> str:
+        return (f"{self.cycles} cycles, relative residual {self.residuals[-1]:.2e}, "
+                f"convergence factor {self.convergence_factor:.3f}")
+
+
+class RefWorkspace:
+    """Device scratch of the reference-exact kernels for one grid shape."""
+
+    def __init__(self, shape: tuple[int, int], coarsest_size: int, dev: torch.device):
+        m, n = shape
+        nbytes = int(_lib.lib().gd_ref_workspace_bytes(m, n, coarsest_size))
+        if nbytes == 0:
+            raise ValueError(f"unsupported grid {shape}")
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.dot_buf = torch.empty(1024, dtype=torch.float64, device=dev)
+        self.scalar = torch.empty(1, dtype=torch.float64, device=dev)
+        self.shape, self.coarsest_size = shape, coarsest_size
+
+    def vcycle(self, u: torch.Tensor, b: torch.Tensor, spacing: float, o: MultigridOptions):
+        m, n = self.shape
+        _lib.check(_lib.lib().gd_ref_vcycle(_lib.ptr(u), _lib.ptr(b), m, n, float(spacing),
+                                            o.pre_smoothing, o.post_smoothing, o.coarsest_size,
+                                            o.coarsest_sweeps, _lib.ptr(self.buf),
+                                            self.buf.numel(), _lib.stream_handle()),
+                   "gd_ref_vcycle")
+
+    def residual(self, r: torch.Tensor, u: torch.Tensor, b: torch.Tensor, spacing: float):
+        m, n = self.shape
+        _lib.check(_lib.lib().gd_ref_residual(_lib.ptr(r), _lib.ptr(u), _lib.ptr(b), m, n,
+                                              float(spacing), _lib.stream_handle()),
+                   "gd_ref_residual")
+
+    def dot(self, a: torch.Tensor, b: torch.Tensor) -> float:
+        _lib.check(_lib.lib().gd_ref_dot(_lib.ptr(self.scalar), _lib.ptr(a), _lib.ptr(b),
+                                         a.numel(), _lib.ptr(self.dot_buf),
+                                         self.dot_buf.numel() * 8, _lib.stream_handle()),
+                   "gd_ref_dot")
+        return float(self.scalar.item())
+
+    def axpby(self, y: torch.Tensor, x: torch.Tensor, alpha: float, beta: float) -> None:
+        _lib.check(_lib.lib().gd_ref_axpby(_lib.ptr(y), _lib.ptr(x), float(alpha), float(beta),
+                                           y.numel(), _lib.stream_handle()), "gd_ref_axpby")
+
+
+def _to_dev(a, dev) -> torch.Tensor:
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev).contiguous()
+
+
+def v_cycle(u, b, spacing: float, options: MultigridOptions) -> np.ndarray:
+    """One V-cycle on ``laplacian(u) = b`` (multigrid.py:184-215); returns a new array."""
+    dev = _lib.device()
+    b_d = _to_dev(b, dev)
+    u_d = _to_dev(u, dev).clone()
+    if u_d.shape != b_d.shape or u_d.dim() != 2:
+        raise ValueError("u and b must be 2-D arrays of the same shape")
+    RefWorkspace(tuple(b_d.shape), options.coarsest_size, dev).vcycle(u_d, b_d, spacing, options)
+    return u_d.cpu().numpy()
+
+
+def solve(b, spacing: float = 1.0, options: MultigridOptions | None = None,
+          initial=None) -> tuple[np.ndarray, MultigridReport]:
+    """Repeated V-cycles until the relative residual is below tolerance (multigrid.py:218-255)."""
+    options = options or MultigridOptions()
+    b = np.asarray(b, dtype=float)
+    dev = _lib.device()
+    b_d = _to_dev(b, dev)
+    u_d = torch.zeros_like(b_d) if initial is None else _to_dev(initial, dev).clone()
+    ws = RefWorkspace(tuple(b_d.shape), options.coarsest_size, dev)
+    scale = float(np.sqrt(ws.dot(b_d, b_d)))
+    if scale == 0.0:
+        return u_d.cpu().numpy(), MultigridReport([0.0], 0, True)
+    r_d = torch.empty_like(b_d)
+
+    def rel_residual() -> float:
+        ws.residual(r_d, u_d, b_d, spacing)
+        return float(np.sqrt(ws.dot(r_d, r_d))) / scale
+
+    history = [rel_residual()]
+    for cycle in range(1, options.max_cycles + 1):
+        ws.vcycle(u_d, b_d, spacing, options)
+        history.append(rel_residual())
+        if history[-1] < options.tolerance:
+            return u_d.cpu().numpy(), MultigridReport(history, cycle, True)
+    return u_d.cpu().numpy(), MultigridReport(history, options.max_cycles, False)

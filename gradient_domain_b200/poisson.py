@@ -1,0 +1,253 @@
+"""Gradient-domain editing entry points on the GPU solver.
+
+Same interface and behaviour as gradient-domain/src/gradient_domain/poisson.py:
+``GuidanceField`` (:52-92), ``solve_dirichlet`` (:102-147), ``solve_masked``
+(:154-244), ``seamless_clone`` (:261-348), ``texture_flatten`` (:351-388) and
+``illumination_change`` (:391-431).
+
+The reference loops over colour channels and solves each one separately (a
+sparse LU for masks, one ``solve_system`` per channel for rectangles).  Here
+all channels of a call are instances of one batched plan: the right-hand
+sides are assembled on the device and every channel goes through the same
+kernel launches.  The masked system is the reference's exactly (unknowns =
+mask minus the image border, known neighbours folded into the right-hand
+side); it is solved by the masked B200 MGPCG instead of a factorisation, to a
+true relative residual of 1e-12 by default, which reproduces the factorised
+solution to rounding level.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .operators import divergence_dev, gradient
+from .plan import Instance, SolveParams, cached_plan
+from .solvers import SolverReport, solve_system
+
+__all__ = ["GuidanceField", "solve_dirichlet", "solve_masked", "seamless_clone",
+           "texture_flatten", "illumination_change"]
+
+DIRECT_TOLERANCE = 1e-12
+
+
+@dataclass
+class GuidanceField:
+    """A target gradient field ``(gx, gy)`` of shape (h, w) or (h, w, c)."""
+
+    gx: np.ndarray
+    gy: np.ndarray
+
+    @classmethod
+    def of(cls, image) -> GuidanceField:
+        """The field whose integral is ``image`` exactly."""
+        return cls(*gradient(image))
+
+    def select(self, mask, other: GuidanceField) -> GuidanceField:
+        """This field inside ``mask``, ``other`` outside."""
+        sel = mask[..., None] if np.ndim(self.gx) == 3 else mask
+        return GuidanceField(np.where(sel, self.gx, other.gx), np.where(sel, self.gy, other.gy))
+
+    def mix_by_magnitude(self, other: GuidanceField) -> GuidanceField:
+        """Per component, the field of larger magnitude (mixed gradients)."""
+        return GuidanceField(np.where(np.abs(self.gx) >= np.abs(other.gx), self.gx, other.gx),
+                             np.where(np.abs(self.gy) >= np.abs(other.gy), self.gy, other.gy))
+
+    def scaled(self, factor) -> GuidanceField:
+        """Both components times a scalar or a per-pixel factor."""
+        return GuidanceField(self.gx * factor, self.gy * factor)
+
+
+def _as_channels(image: np.ndarray):
+    return (image[..., None], True) if image.ndim == 2 else (image, False)
+
+
+def _to_chw(a: np.ndarray, dev) -> torch.Tensor:
+    a = np.asarray(a, dtype=np.float64)
+    t = torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+    return t.unsqueeze(0) if t.dim() == 2 else t.permute(2, 0, 1).contiguous()
+
+
+def _field_divergence(field: GuidanceField, channels: int, dev) -> torch.Tensor:
+    gx, gy = _to_chw(field.gx, dev), _to_chw(field.gy, dev)
+    if gx.shape[0] == 1 and channels > 1:
+        gx, gy = gx.expand(channels, -1, -1).contiguous(), gy.expand(channels, -1, -1).contiguous()
+    return divergence_dev(gx, gy)
+
+
+def _reports(results, method: str, seconds: float) -> list[SolverReport]:
+    share = seconds / max(len(results), 1)
+    return [SolverReport(method, r.iterations, r.relative_residual, share, r.converged,
+                         _lib.STATUS_NAMES.get(r.status, str(r.status))) for r in results]
+
+
+def solve_dirichlet(field: GuidanceField, boundary, method: str = "mgcg",
+                    tolerance: float = 1e-8, max_iterations: int = 2000):
+    """Integrate ``field`` on a rectangle whose one-pixel ring is fixed to ``boundary``.
+
+    Returns the image (same shape as ``boundary``, equal to it on the ring)
+    and one :class:`SolverReport` per channel.
+    """
+    bnd, gray = _as_channels(np.asarray(boundary, dtype=float))
+    h, w, c = bnd.shape
+    result = bnd.copy()
+    if h <= 2 or w <= 2:
+        return (result[..., 0] if gray else result), [
+            SolverReport(method, 0, 0.0, 0.0, True) for _ in range(c)]
+    dev = _lib.device()
+    div = _field_divergence(field, c, dev)
+    bnd_d = _to_chw(bnd, dev)
+    f = torch.empty((c, h - 2, w - 2), dtype=torch.float64, device=dev)
+    for k in range(c):
+        _lib.check(_lib.lib().gd_fold_dirichlet(_lib.ptr(f[k]), _lib.ptr(div[k]),
+                                                _lib.ptr(bnd_d[k]), h, w, 1.0,
+                                                _lib.stream_handle()), "gd_fold_dirichlet")
+    if method not in ("mgcg", "mgcg_fp64"):
+        reports = []
+        folded = f.cpu().numpy()
+        for k in range(c):
+            sol, rep = solve_system(folded[k], method=method, tolerance=tolerance,
+                                    max_iterations=max_iterations)
+            result[1:-1, 1:-1, k] = sol
+            reports.append(rep)
+        return (result[..., 0] if gray else result), reports
+    params = SolveParams(precision="fp64" if method == "mgcg_fp64" else "mixed",
+                         tolerance=tolerance, max_iterations=max_iterations)
+    plan = cached_plan(tuple(Instance(h - 2, w - 2, "dirichlet") for _ in range(c)), params)
+    x = torch.zeros_like(f)
+    started = time.perf_counter()
+    results = plan.solve(list(f), list(x), scale=-1.0)
+    elapsed = time.perf_counter() - started
+    result[1:-1, 1:-1, :] = x.permute(1, 2, 0).cpu().numpy()
+    return (result[..., 0] if gray else result), _reports(results, method, elapsed)
+
+
+def _interior(mask: np.ndarray) -> np.ndarray:
+    inner = np.zeros(mask.shape, dtype=bool)
+    inner[1:-1, 1:-1] = np.asarray(mask, dtype=bool)[1:-1, 1:-1]
+    return inner
+
+
+def solve_masked(field: GuidanceField, image, mask, tolerance: float = DIRECT_TOLERANCE,
+                 max_iterations: int = 2000, precision: str = "mixed"):
+    """Integrate ``field`` over the pixels of ``mask``; the rest of ``image`` is kept.
+
+    The unknowns are ``mask`` without the image border (poisson.py:181-182);
+    pixels outside stay bit-exact and act as Dirichlet data.
+    """
+    img = np.asarray(image, dtype=float)
+    chans, gray = _as_channels(img)
+    mask = np.asarray(mask, dtype=bool)
+    interior = _interior(mask)
+    if not interior.any():
+        return img.copy(), []
+    h, w, c = chans.shape
+    rows = np.nonzero(interior.any(axis=1))[0]
+    cols = np.nonzero(interior.any(axis=0))[0]
+    r0, r1 = rows[0] - 1, rows[-1] + 2
+    c0, c1 = cols[0] - 1, cols[-1] + 2
+    win = (slice(r0, r1), slice(c0, c1))
+    hc, wc = r1 - r0, c1 - c0
+    dev = _lib.device()
+    sub = GuidanceField(np.asarray(field.gx)[win], np.asarray(field.gy)[win])
+    div = _field_divergence(sub, c, dev)
+    img_d = _to_chw(chans[win], dev)
+    unk = torch.as_tensor(np.ascontiguousarray(interior[win]).astype(np.uint8)).to(dev)
+    f = torch.empty((c, hc, wc), dtype=torch.float64, device=dev)
+    for k in range(c):
+        _lib.check(_lib.lib().gd_masked_rhs(_lib.ptr(f[k]), _lib.ptr(div[k]), _lib.ptr(img_d[k]),
+                                            _lib.ptr(unk), hc, wc, -1.0, _lib.stream_handle()),
+                   "gd_masked_rhs")
+    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations)
+    plan = cached_plan(tuple(Instance(hc, wc, "masked") for _ in range(c)), params)
+    for k in range(c):
+        plan.set_mask(k, unk)
+    x = torch.zeros_like(f)
+    started = time.perf_counter()
+    results = plan.solve(list(f), list(x), scale=1.0)
+    elapsed = time.perf_counter() - started
+    sol = x.permute(1, 2, 0).cpu().numpy()
+    out = chans.copy()
+    inner_win = interior[win]
+    out_win = out[win]
+    out_win[inner_win] = sol[inner_win]
+    return (out[..., 0] if gray else out), _reports(results, "mgcg (masked)", elapsed)
+
+
+def _place(source, mask, target_shape, offset):
+    row, column = offset
+    height, width = source.shape[:2]
+    if row < 0 or column < 0 or row + height > target_shape[0] or column + width > target_shape[1]:
+        raise ValueError("the source patch does not fit the target at this offset")
+    canvas = np.zeros(target_shape, dtype=float)
+    canvas[row:row + height, column:column + width] = source
+    placed = np.zeros(target_shape[:2], dtype=bool)
+    placed[row:row + height, column:column + width] = mask
+    return canvas, placed
+
+
+def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
+                   domain: str = "mask", method: str = "mgcg", margin: int = 24):
+    """Paste ``source[mask]`` into ``target`` at ``offset`` without a visible seam.
+
+    Raises ``ValueError`` for an unknown ``mode`` or ``domain``, or a patch that
+    does not fit (poisson.py:310-335).
+    """
+    target = np.asarray(target, dtype=float)
+    source = np.asarray(source, dtype=float)
+    if source.ndim != target.ndim:
+        raise ValueError("source and target must have the same number of dimensions")
+    placed, placed_mask = _place(source, mask, target.shape, offset)
+    source_field = GuidanceField.of(placed)
+    target_field = GuidanceField.of(target)
+    if mode == "import":
+        inside = source_field
+    elif mode == "mixed":
+        inside = source_field.mix_by_magnitude(target_field)
+    elif mode == "average":
+        inside = GuidanceField(0.5 * (source_field.gx + target_field.gx),
+                               0.5 * (source_field.gy + target_field.gy))
+    else:
+        raise ValueError(f"unknown mode {mode!r}")
+    field = inside.select(placed_mask, target_field)
+    if domain == "mask":
+        return solve_masked(field, target, placed_mask)
+    if domain != "rectangle":
+        raise ValueError(f"unknown domain {domain!r}")
+    rows, columns = np.nonzero(placed_mask)
+    top = max(int(rows.min()) - margin, 0)
+    bottom = min(int(rows.max()) + margin + 1, target.shape[0])
+    left = max(int(columns.min()) - margin, 0)
+    right = min(int(columns.max()) + margin + 1, target.shape[1])
+    window = (slice(top, bottom), slice(left, right))
+    patch, reports = solve_dirichlet(GuidanceField(field.gx[window], field.gy[window]),
+                                     target[window], method=method)
+    result = target.copy()
+    result[window] = patch
+    return result, reports
+
+
+def texture_flatten(image, edges, method: str = "mgcg", mask=None):
+    """Keep gradients only on ``edges`` (weights in [0, 1]) and re-integrate."""
+    image = np.asarray(image, dtype=float)
+    weights = np.asarray(edges, dtype=float)
+    if image.ndim == 3:
+        weights = weights[..., None]
+    field = GuidanceField.of(image).scaled(weights)
+    if mask is not None:
+        return solve_masked(field, image, mask)
+    return solve_dirichlet(field, image, method=method)
+
+
+def illumination_change(image, mask, alpha: float = 0.2, beta: float = 0.2,
+                        epsilon: float = 1e-4):
+    """Compress local dynamic range inside ``mask`` (gradient remap alpha^b g^-b)."""
+    image = np.asarray(image, dtype=float)
+    field = GuidanceField.of(image)
+    magnitude = np.sqrt(field.gx ** 2 + field.gy ** 2)
+    factor = (alpha ** beta) * np.maximum(magnitude, epsilon) ** (-beta)
+    return solve_masked(field.scaled(factor), image, mask)

@@ -1,0 +1,210 @@
+/*
+ * gd_poisson.h - C ABI of the B200 gradient-domain Poisson solver.
+ *
+ * The reference (gradient-domain, pure Python) exposes the Poisson path as
+ * Python functions; this library is what those functions bind to through
+ * ctypes.  Every pointer argument named *_dev is a device pointer owned by the
+ * caller; the library never allocates device memory on a solve.  Every call is
+ * ordered on the given CUDA stream and returns GD_OK (0) or a negative error
+ * code; gd_last_error() gives the message of the calling thread's last error.
+ * A plan is not thread-safe: one host thread drives it at a time.
+ *
+ * Conventions shared by all entry points:
+ *   - grids are row-major (rows = height, cols = width) with a row pitch given
+ *     in elements; FP64 arrays are double, masks are uint8 (non-zero = unknown);
+ *   - the system solved is A x = f with A the positive five-point operator
+ *     (A u = d_p u_p - sum of neighbour values), so the reference's
+ *     laplacian(u) = b with spacing h maps to f = -h^2 b.
+ */
+#ifndef GD_POISSON_H
+#define GD_POISSON_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GD_OK 0
+#define GD_ERR_ARG (-1)
+#define GD_ERR_CUDA (-2)
+#define GD_ERR_STATE (-3)
+#define GD_ERR_UNSUPPORTED (-4)
+
+/* Boundary of one solve instance. */
+enum gd_boundary {
+  GD_DIRICHLET = 0, /* rectangle, zero values outside (solvers.py:171 system)   */
+  GD_NEUMANN = 1,   /* rectangle, edge-replicated ghosts (solvers.py:224 system) */
+  GD_MASKED = 2     /* unknowns where mask != 0, Dirichlet elsewhere (poisson.py:154) */
+};
+
+/* Arithmetic of a plan. */
+enum gd_precision {
+  GD_MIXED = 0, /* FP32 V-cycle and Krylov vectors, FP64 residual/scalars/solution */
+  GD_FP64 = 1   /* everything in FP64 */
+};
+
+/* Per-instance status words reported by a solve. */
+enum gd_status {
+  GD_CONVERGED = 0,
+  GD_MAX_ITERATIONS = 1,
+  GD_BREAKDOWN = 2,  /* p.Ap <= 0 or a non-finite scalar */
+  GD_ACTIVE = 3      /* internal: still iterating */
+};
+
+typedef struct gd_grid_desc {
+  int32_t height;   /* unknown rows    */
+  int32_t width;    /* unknown columns */
+  int32_t boundary; /* enum gd_boundary */
+  int32_t flags;    /* bit 0 (Neumann): drop the mean of f, return the zero-mean x (solvers.py:258-262) */
+} gd_grid_desc;
+
+typedef struct gd_params {
+  int32_t precision;      /* enum gd_precision                                   */
+  int32_t pre_sweeps;     /* RB-GS sweeps before restriction (1..3)               */
+  int32_t post_sweeps;    /* RB-GS sweeps after prolongation (1..3)               */
+  int32_t max_iterations; /* PCG iteration budget (solvers.py:176 default 2000)    */
+  double tolerance;       /* target ||f - A x|| / ||f|| (solvers.py:175 default 1e-8) */
+  double reliable_delta;  /* mixed precision: residual drop between FP64 refreshes */
+  int32_t check_every;    /* iterations between host-side convergence polls        */
+  int32_t use_graph;      /* capture one iteration as a CUDA graph and replay it    */
+} gd_params;
+
+typedef struct gd_report {
+  int32_t iterations;        /* PCG iterations taken                      */
+  int32_t status;            /* enum gd_status                            */
+  double relative_residual;  /* true FP64 ||f - A x|| / ||f|| at exit      */
+  double initial_norm;       /* ||f||                                      */
+} gd_report;
+
+typedef struct gd_plan_s *gd_plan;
+
+/* Thread-local message of the last failed call ("" if none). */
+const char *gd_last_error(void);
+
+/* Library build identification, e.g. "gd_poisson sm_100a". */
+const char *gd_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Batched MG-preconditioned CG (the B200 replacement of the reference's
+ * solve_system(method="mgcg") loop, solvers.py:134-160, its per-channel loops
+ * poisson.py:137-145 and :216-242, and the DCT solve_neumann, solvers.py:224-262).
+ * -------------------------------------------------------------------------*/
+
+/* Build the multigrid hierarchy and work lists for n instances. */
+int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_params *params,
+                   gd_plan *out);
+void gd_plan_destroy(gd_plan plan);
+
+/* Device workspace the caller must provide (bytes, 256-byte aligned). */
+size_t gd_plan_workspace_bytes(gd_plan plan);
+
+/* Attach the workspace and upload descriptors; zeroes the hierarchy arrays. */
+int gd_plan_bind(gd_plan plan, void *workspace_dev, size_t bytes, cudaStream_t stream);
+
+/* Masked instances only: mask_dev[r*pitch+c] != 0 marks an unknown.  Builds the
+ * per-level cell classes; call before gd_plan_prepare. */
+int gd_plan_set_mask(gd_plan plan, int32_t instance, const uint8_t *mask_dev,
+                     int32_t pitch, cudaStream_t stream);
+
+/* Factor the coarsest grid of every instance (FP64 dense inverse on device). */
+int gd_plan_prepare(gd_plan plan, cudaStream_t stream);
+
+/* Solve A x_i = scale_i * f_i for every instance.  f_dev[i], x_dev[i] point to
+ * height x width FP64 arrays with row pitch pitch[i] (elements); x_dev[i] holds
+ * the initial guess on entry (zero it for the reference's x0 = 0) and the
+ * solution on exit.  Unknown-free cells of masked instances are written 0.
+ * Blocks until every instance has converged or stopped; fills reports[n]. */
+int gd_solve(gd_plan plan, const double *const *f_dev, double *const *x_dev,
+             const int32_t *pitch, const double *scale, cudaStream_t stream,
+             gd_report *reports);
+
+/* One application of the preconditioner (a single V-cycle from zero) to the
+ * FP64 residual r of instance i: z = M r.  Test and inspection hook. */
+int gd_plan_apply_vcycle(gd_plan plan, int32_t instance, const double *r_dev,
+                         double *z_dev, int32_t pitch, cudaStream_t stream);
+
+/* Kernel kinds reported by gd_plan_kernel_times. */
+enum gd_kernel_kind {
+  GD_K_DOWN0 = 0,   /* level-0 pre-smooth + residual + restriction      */
+  GD_K_DOWN = 1,    /* same on levels >= 1                              */
+  GD_K_BOTTOM = 2,  /* small levels of every instance, one CTA each      */
+  GD_K_UP = 3,      /* prolongation + correction + post-smooth, levels >= 1 */
+  GD_K_UP0 = 4,     /* same on level 0, with the r.z reduction           */
+  GD_K_PUPDATE = 5, /* p = z + beta p and p.Ap                           */
+  GD_K_CGUPDATE = 6,/* d += alpha p, r -= alpha A p and r.r              */
+  GD_K_FOLD = 7,    /* x += d on FP64 refresh iterations                 */
+  GD_K_RESID = 8,   /* FP64 residual refresh and convergence test        */
+  GD_K_INIT = 9,    /* right-hand-side mean and initial FP64 residual    */
+  GD_K_MEAN = 10,   /* zero-mean projection of Neumann solutions         */
+  GD_KERNEL_KINDS = 11
+};
+
+typedef struct gd_kernel_time {
+  long long launches;  /* launches since profiling was enabled              */
+  double milliseconds; /* summed CUDA-event durations on the solve stream    */
+  double cells;        /* summed grid cells covered by those launches        */
+} gd_kernel_time;
+
+/* Record CUDA events around every launch of subsequent solves (graphs are
+ * bypassed while enabled); resets the totals. */
+int gd_plan_set_profiling(gd_plan plan, int32_t enable);
+
+/* Per-kind totals since gd_plan_set_profiling; out has GD_KERNEL_KINDS entries. */
+int gd_plan_kernel_times(gd_plan plan, gd_kernel_time *out, int32_t n);
+
+/* ---------------------------------------------------------------------------
+ * Reference-exact vertex-centred FP64 multigrid (multigrid.py:147-215), used by
+ * v_cycle, multigrid.solve and solve_system("multigrid" | "cg" | "mgcg_fp64").
+ * Arrays are m x n FP64, contiguous (pitch = n).
+ * -------------------------------------------------------------------------*/
+
+/* Scratch bytes needed by gd_ref_vcycle for an m x n interior grid. */
+size_t gd_ref_workspace_bytes(int32_t m, int32_t n, int32_t coarsest_size);
+
+/* u <- v_cycle(u, b, spacing, options) (multigrid.py:184-215). */
+int gd_ref_vcycle(double *u_dev, const double *b_dev, int32_t m, int32_t n, double spacing,
+                  int32_t pre, int32_t post, int32_t coarsest_size, int32_t coarsest_sweeps,
+                  void *workspace_dev, size_t bytes, cudaStream_t stream);
+
+/* r <- b - laplacian(u, spacing) (multigrid.py:210, operators.py:86-107). */
+int gd_ref_residual(double *r_dev, const double *u_dev, const double *b_dev, int32_t m,
+                    int32_t n, double spacing, cudaStream_t stream);
+
+/* out[0] <- sum(a*b) over m*n elements, deterministic (solvers.py:146,151,157). */
+int gd_ref_dot(double *out_dev, const double *a_dev, const double *b_dev, int64_t count,
+               void *workspace_dev, size_t bytes, cudaStream_t stream);
+
+/* y <- alpha * x + beta * y over count elements (solvers.py:152-158). */
+int gd_ref_axpby(double *y_dev, const double *x_dev, double alpha, double beta,
+                 int64_t count, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Right-hand-side assembly (operators.py:53-83, :139-169; poisson.py:210-224).
+ * -------------------------------------------------------------------------*/
+
+/* (gx, gy) <- gradient(u) (operators.py:30-50); all arrays h x w contiguous FP64. */
+int gd_gradient(double *gx_dev, double *gy_dev, const double *u_dev, int32_t h, int32_t w,
+                cudaStream_t stream);
+
+/* div_dev (h x w) <- divergence(gx, gy); all arrays contiguous FP64. */
+int gd_divergence(double *div_dev, const double *gx_dev, const double *gy_dev, int32_t h,
+                  int32_t w, cudaStream_t stream);
+
+/* f_dev ((h-2) x (w-2)) <- scale * fold_boundary(div[1:-1,1:-1], boundary, 1)
+ * (solve_dirichlet's per-channel system, poisson.py:131-143). */
+int gd_fold_dirichlet(double *f_dev, const double *div_dev, const double *boundary_dev,
+                      int32_t h, int32_t w, double scale, cudaStream_t stream);
+
+/* Masked system on the whole h x w image: f <- scale * (div - sum of known
+ * neighbour values) at unknowns, 0 elsewhere (poisson.py:216-224). */
+int gd_masked_rhs(double *f_dev, const double *div_dev, const double *image_dev,
+                  const uint8_t *unknown_dev, int32_t h, int32_t w, double scale,
+                  cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GD_POISSON_H */
