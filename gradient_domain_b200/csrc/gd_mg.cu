@@ -248,6 +248,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     I.p_off = take(arena, cells0);
     I.d_off = take(arena, cells0);
     I.z_off = take(arena, cells0);
+    I.q_off = take(arena, cells0);
     I.level0 = (int)p->lv.size();
     int ny = I.ny, nx = I.nx, level = 0;
     int bottom = -1;

@@ -34,7 +34,7 @@ struct LevelInfo {
 struct InstInfo {
   int ny, nx, pitch, bc;
   int level0, bottom, coarsest, nlevels;
-  long long r_off, p_off, d_off, z_off;
+  long long r_off, p_off, d_off, z_off, q_off;  // p is double-buffered: p_off / q_off
   int fine_begin, fine_end;  // tile range in the fine map
   int up0_begin, up0_end;    // tile range in the level-0 up map (empty if bottom is level 0)
   int zero_mean, pad;
@@ -49,6 +49,7 @@ struct InstInfo {
 struct InstState {
   double rz, beta, pAp, alpha, rr, rr_ref, ff, rr_true, mean, fmean;
   int status, iters, flags, first;
+  int pcur, pad;  // which of the two p buffers holds the current direction
 };
 
 struct Tile {

@@ -48,6 +48,13 @@ __device__ __forceinline__ double warp_range_sum(const double *p, int b, int e) 
   return warp_sum(s);
 }
 
+// The search direction lives in two buffers: k_pupdate reads the current one
+// (including halo cells owned by other CTAs) and writes the other, so no CTA
+// overwrites a value another CTA still has to read.
+__device__ __forceinline__ long long p_offset(const InstInfo &I, int which) {
+  return which ? I.q_off : I.p_off;
+}
+
 __device__ __forceinline__ void finish_rz(InstState &S, double rz) {
   if (!(rz > 0.0) || !isfinite(rz)) {
     S.status = GD_BREAKDOWN;
@@ -493,8 +500,10 @@ __global__ void __launch_bounds__(kFThreads) k_pupdate(Args<T> a) {
     __shared__ T diag[8], dinv[8];
     make_tables(diag, dinv, L.wall);
     const T beta = (T)a.st[tl.inst].beta;
+    const int cur = a.st[tl.inst].pcur;
     const T *z = a.arena + I.z_off;
-    T *p = a.arena + I.p_off;
+    const T *p = a.arena + p_offset(I, cur);
+    T *pn = a.arena + p_offset(I, cur ^ 1);
     const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
     for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
       const int wy = k / W, wx = k - wy * W;
@@ -515,7 +524,7 @@ __global__ void __launch_bounds__(kFThreads) k_pupdate(Args<T> a) {
       const int c = cell_class(L, a.codes, gy, gx);
       const T pv = sp[idx];
       part += (double)pv * (double)apply_tile<T, T>(sp, idx, c, diag);
-      p[(long long)gy * L.pitch + gx] = pv;
+      pn[(long long)gy * L.pitch + gx] = pv;
     }
   }
   part = block_sum<kFThreads>(part);
@@ -530,6 +539,7 @@ __global__ void __launch_bounds__(kFThreads) k_pupdate(Args<T> a) {
     if ((threadIdx.x & 31) == 0) {
       const double alpha = S.rz / pAp;
       S.pAp = pAp;
+      S.pcur ^= 1;
       if (!(pAp > 0.0) || !isfinite(alpha)) {
         S.status = GD_BREAKDOWN;
         S.flags |= FLAG_RU;
@@ -555,7 +565,7 @@ __global__ void __launch_bounds__(kFThreads) k_cgupdate(Args<T> a) {
     __shared__ T diag[8], dinv[8];
     make_tables(diag, dinv, L.wall);
     const T alpha = (T)a.st[tl.inst].alpha;
-    const T *p = a.arena + I.p_off;
+    const T *p = a.arena + p_offset(I, a.st[tl.inst].pcur);
     T *d = a.arena + I.d_off;
     T *r = a.arena + I.r_off;
     const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
@@ -655,6 +665,7 @@ __global__ void __launch_bounds__(kFThreads) k_resid(Args<T> a) {
         part_f += f * f;
         a.arena[I.d_off + g] = T(0);
         a.arena[I.p_off + g] = T(0);
+        a.arena[I.q_off + g] = T(0);
         a.arena[I.z_off + g] = T(0);
         if (!c) I.x[gu] = 0.0;
       }
@@ -687,6 +698,7 @@ __global__ void __launch_bounds__(kFThreads) k_resid(Args<T> a) {
           S.first = 1;
           S.rz = 0.0;
           S.beta = 0.0;
+          S.pcur = 0;
           S.status = GD_ACTIVE;
         }
         S.rr_true = rr;
