@@ -71,8 +71,10 @@ def test_solve_system_conventions():
 
 @pytest.mark.parametrize("key", ["neu32x40", "neu97x131", "neu64x64"])
 def test_solve_neumann_matches_golden(golden, key):
+    # relative to the solution's size: a rough right-hand side has a large smooth solution
     got = gd.solve_neumann(golden[f"{key}_b"])
-    assert np.abs(got - golden[f"{key}_u"]).max() < 1e-9
+    ref = golden[f"{key}_u"]
+    assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max()
     assert abs(float(got.mean())) < 1e-12
 
 
