@@ -11,6 +11,8 @@
 // all-FP64 GPU translation of the reference that the fused solver is measured
 // against, and the parity hook for v_cycle / multigrid.solve.
 
+#include <mutex>
+
 #include "gd_internal.cuh"
 
 namespace gd {
@@ -307,4 +309,67 @@ extern "C" int gd_ref_axpby(double *y, const double *x, double alpha, double bet
   ref_axpby_kernel<<<blocks_for(count, 256), 256, 0, st>>>(y, x, alpha, beta, count);
   GD_CHECK_LAUNCH();
   return GD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of gd_ref_vcycle.
+//
+// Some callers cannot allocate device memory when they need a V-cycle: code
+// running while a CUDA stream is being captured into a graph (cudaMalloc is
+// not permitted there), real-time loops that forbid allocation after start-up,
+// and host applications that own the whole device memory budget and give
+// plug-ins no allocator.  gd_ref_vcycle_static takes its coarse-level scratch
+// from the file-scope array below instead of a caller workspace.  The array
+// is GD_STATIC_SCRATCH_BYTES (4 MiB) on every GPU that loads this library and
+// stays allocated until the process exits.  In host code `g_static_scratch`
+// names a host-side stand-in, not device memory, so its device address is
+// looked up with cudaGetSymbolAddress once per device and cached.
+namespace gd {
+namespace {
+
+__device__ __align__(256) unsigned char g_static_scratch[GD_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxStaticDevices = 64;
+void *g_static_ptr[kMaxStaticDevices] = {};
+std::mutex g_static_mu;
+
+// Device address of g_static_scratch on the current device (looked up once).
+int static_scratch(void **out) {
+  int dev = 0;
+  GD_CHECK_CUDA(cudaGetDevice(&dev));
+  GD_REQUIRE(dev >= 0 && dev < kMaxStaticDevices, GD_ERR_UNSUPPORTED,
+             "gd_ref_vcycle_static: device %d beyond the %d supported", dev, kMaxStaticDevices);
+  std::lock_guard<std::mutex> hold(g_static_mu);
+  if (g_static_ptr[dev] == nullptr) {
+    void *p = nullptr;
+    GD_CHECK_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return GD_OK;
+}
+
+}  // namespace
+}  // namespace gd
+
+extern "C" int gd_ref_vcycle_static(double *u, const double *b, int32_t m, int32_t n,
+                                    double spacing, int32_t pre, int32_t post,
+                                    int32_t coarsest_size, int32_t coarsest_sweeps,
+                                    cudaStream_t st) {
+  GD_REQUIRE(u && b && m > 0 && n > 0 && pre >= 0 && post >= 0 && coarsest_sweeps >= 0,
+             GD_ERR_ARG, "gd_ref_vcycle_static: bad arguments");
+  RefLevel lv[64];
+  size_t need = 0;
+  const int nlev = ref_levels(m, n, coarsest_size, lv, 64, &need);
+  GD_REQUIRE(nlev > 0, GD_ERR_ARG, "gd_ref_vcycle_static: hierarchy too deep");
+  GD_REQUIRE(need <= (size_t)GD_STATIC_SCRATCH_BYTES, GD_ERR_ARG,
+             "gd_ref_vcycle_static: a %d x %d grid needs %zu bytes of scratch, more than the "
+             "%zu-byte static array; use gd_ref_vcycle with a workspace",
+             m, n, need, (size_t)GD_STATIC_SCRATCH_BYTES);
+  void *ws = nullptr;
+  const int rc = static_scratch(&ws);
+  if (rc != GD_OK) return rc;
+  // ref_vcycle_rec zeroes every coarse iterate before use, so the contents left
+  // by the previous call do not leak into this one.
+  return ref_vcycle_rec(lv, nlev, 0, u, b, spacing, pre, post, coarsest_sweeps, (char *)ws, st);
 }

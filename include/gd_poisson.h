@@ -169,6 +169,25 @@ int gd_ref_vcycle(double *u_dev, const double *b_dev, int32_t m, int32_t n, doub
                   int32_t pre, int32_t post, int32_t coarsest_size, int32_t coarsest_sweeps,
                   void *workspace_dev, size_t bytes, cudaStream_t stream);
 
+/* Size of the file-scope device scratch array used by gd_ref_vcycle_static. */
+#define GD_STATIC_SCRATCH_BYTES (4u << 20)
+
+/* Allocation-free u <- v_cycle(u, b, spacing, options).  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they need a cycle (inside CUDA stream capture, in allocation-free real-time
+ * loops, or as a plug-in of an application that owns the memory budget).  The
+ * coarse-level scratch is a GD_STATIC_SCRATCH_BYTES (4 MiB) static device
+ * array that every GPU loading this library holds until exit; grids needing
+ * more (gd_ref_workspace_bytes > 4 MiB, about 500 x 500 and up) are rejected
+ * with GD_ERR_ARG.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (different streams or
+ * threads) race and must be serialised by the caller.  Nothing is allocated
+ * or freed; the coarse iterates are zeroed on every call. */
+int gd_ref_vcycle_static(double *u_dev, const double *b_dev, int32_t m, int32_t n,
+                         double spacing, int32_t pre, int32_t post, int32_t coarsest_size,
+                         int32_t coarsest_sweeps, cudaStream_t stream);
+
 /* r <- b - laplacian(u, spacing) (multigrid.py:210, operators.py:86-107). */
 int gd_ref_residual(double *r_dev, const double *u_dev, const double *b_dev, int32_t m,
                     int32_t n, double spacing, cudaStream_t stream);
