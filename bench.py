@@ -195,7 +195,7 @@ def ours(args) -> None:
 
     dev = torch.device("cuda", local)
     size = args.size
-    rhs_np = workloads.tonemap_rhs(size, seed=1 + rank)
+    rhs_np = workloads.tonemap_rhs(size, seed=1 + rank, channels=args.channels)
     n_ch = rhs_np.shape[0]
     cells = n_ch * size * size
     f = torch.as_tensor(rhs_np).to(dev)
@@ -222,6 +222,15 @@ def ours(args) -> None:
 
     for _ in range(args.warmup):
         results = step(plan)
+    if args.solve_only:
+        for _ in range(args.steps):
+            results = step(plan)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"solve_only": True, "iterations": [r.iterations for r in results],
+                              "relative_residual": max(r.relative_residual for r in results)}))
+        plan.close()
+        return
     plan.set_profiling(True)
     clocks = ClockSampler(local)
     clocks.start()
@@ -313,7 +322,7 @@ def ours(args) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32/fp64-mixed", "data": "synthetic",
-        "config": {"workload": f"tonemap-neumann {size}x{size}x3", "tolerance": args.tol,
+        "config": {"workload": f"tonemap-neumann {size}x{size}x{n_ch}", "tolerance": args.tol,
                    "sweeps": args.sweeps, "instances_per_gpu": n_ch,
                    "l2": "inputs larger than L2 (3 x 134 MB rhs + solution + hierarchy)",
                    "parallelism": f"replicas x{world}"},
@@ -353,6 +362,10 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the oracle and CPU baseline")
+    ap.add_argument("--channels", type=int, default=3)
+    ap.add_argument("--solve-only", action="store_true",
+                    help="only the mixed-precision solves (small profiling runs): no FP64 plan, "
+                         "no end-to-end leg, no oracle")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

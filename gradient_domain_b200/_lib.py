@@ -18,8 +18,9 @@ LIB_PATH = os.path.join(HERE, "libgd_poisson.so")
 
 GD_DIRICHLET, GD_NEUMANN, GD_MASKED = 0, 1, 2
 GD_MIXED, GD_FP64 = 0, 1
-GD_CONVERGED, GD_MAX_ITERATIONS, GD_BREAKDOWN, GD_ACTIVE = 0, 1, 2, 3
-STATUS_NAMES = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "active"}
+GD_CONVERGED, GD_MAX_ITERATIONS, GD_BREAKDOWN, GD_ACTIVE, GD_STAGNATED = 0, 1, 2, 3, 4
+STATUS_NAMES = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "active",
+                4: "stagnated"}
 
 EXPORTS = (
     "gd_last_error", "gd_version", "gd_plan_create", "gd_plan_destroy",
@@ -40,7 +41,8 @@ class Params(C.Structure):
     _fields_ = [("precision", C.c_int32), ("pre_sweeps", C.c_int32),
                 ("post_sweeps", C.c_int32), ("max_iterations", C.c_int32),
                 ("tolerance", C.c_double), ("reliable_delta", C.c_double),
-                ("check_every", C.c_int32), ("use_graph", C.c_int32)]
+                ("check_every", C.c_int32), ("use_graph", C.c_int32),
+                ("strip_target_warps", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Report(C.Structure):

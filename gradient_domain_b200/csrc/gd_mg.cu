@@ -19,7 +19,7 @@
 #include <cstring>
 #include <vector>
 
-#include "gd_mg_kernels.cuh"
+#include "gd_stream.cuh"
 
 using namespace gd;
 
@@ -100,21 +100,29 @@ void prof_collect(gd_plan p) {
   p->ev_used = 0;
 }
 
+// Strip geometry of the down / up kernels for a plan's precision and sweeps.
+template <typename T, int S>
+struct StripCfg {
+  static constexpr int down_ow = st::DownGeom<T, S>::H::OW;
+  static constexpr int up_ow = st::UpGeom<T, S, S>::H::OW;
+};
+
 template <typename T>
 struct Runner {
-  using Cfg1 = VCfg<T, 1, 1>;
-
   template <int S>
   static void set_attrs() {
-    using C = VCfg<T, S, S>;
-    cudaFuncSetAttribute(k_down<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::down_smem());
-    cudaFuncSetAttribute(k_up<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::up_smem());
-    cudaFuncSetAttribute(k_up<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)C::up_smem());
     cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          200 * 1024);
+    const int lvl = (int)st::level_smem<T>();
+    cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, lvl);
+    cudaFuncSetAttribute(st::k_up_s<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         lvl);
+    cudaFuncSetAttribute(st::k_up_s<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         lvl);
+    cudaFuncSetAttribute(st::k_pupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)st::pupdate_smem<T>());
+    cudaFuncSetAttribute(st::k_cgupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)st::cgupdate_smem<T>());
   }
 
   static Args<T> args(gd_plan p) {
@@ -144,12 +152,11 @@ struct Runner {
 
   template <int S>
   static void vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
-    using C = VCfg<T, S, S>;
     for (int l = 0; l < p->depth; ++l) {
       if (p->down_count[l] <= 0) continue;
       prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
-      k_down<T, S><<<p->down_count[l], kVThreads, C::down_smem(), st>>>(
-          at_tiles(a, p->down_base[l]), 0);
+      st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+          at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     prof_begin(p, GD_K_BOTTOM, 0.0, st);
@@ -159,11 +166,11 @@ struct Runner {
       if (p->up_count[l] <= 0) continue;
       prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
       if (l == 0)
-        k_up<T, S, S, true><<<p->up_count[l], kVThreads, C::up_smem(), st>>>(
-            at_tiles(a, p->up_base[l]), 0);
+        st::k_up_s<T, S, S, true><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+            at_tiles(a, p->up_base[l]));
       else
-        k_up<T, S, S, false><<<p->up_count[l], kVThreads, C::up_smem(), st>>>(
-            at_tiles(a, p->up_base[l]), 0);
+        st::k_up_s<T, S, S, false><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+            at_tiles(a, p->up_base[l]));
       prof_end(p, st);
     }
   }
@@ -174,16 +181,16 @@ struct Runner {
     const Args<T> f = at_tiles(a, p->fine_base);
     const double c = p->fine_cells;
     prof_begin(p, GD_K_PUPDATE, c, st);
-    k_pupdate<T><<<p->fine_count, kFThreads, 0, st>>>(f);
+    st::k_pupdate_s<T><<<p->fine_count, st::kThreads, st::pupdate_smem<T>(), st>>>(f);
     prof_end(p, st);
     prof_begin(p, GD_K_CGUPDATE, c, st);
-    k_cgupdate<T><<<p->fine_count, kFThreads, 0, st>>>(f);
+    st::k_cgupdate_s<T><<<p->fine_count, st::kThreads, st::cgupdate_smem<T>(), st>>>(f);
     prof_end(p, st);
     prof_begin(p, GD_K_FOLD, c, st);
     k_fold<T><<<p->fine_count, kFThreads, 0, st>>>(f);
     prof_end(p, st);
     prof_begin(p, GD_K_RESID, c, st);
-    k_resid<T, false><<<p->fine_count, kFThreads, 0, st>>>(f);
+    st::k_resid_s<T, false><<<p->fine_count, st::kThreads, 0, st>>>(f);
     prof_end(p, st);
   }
 
@@ -205,6 +212,30 @@ struct Runner {
     else vcycle<3>(p, a, st);
   }
 };
+
+void strip_widths(gd_plan p, int *down_ow, int *up_ow) {
+  const int s = p->prm.pre_sweeps;
+  if (p->fp64) {
+    if (s == 1) { *down_ow = StripCfg<double, 1>::down_ow; *up_ow = StripCfg<double, 1>::up_ow; }
+    else if (s == 2) { *down_ow = StripCfg<double, 2>::down_ow; *up_ow = StripCfg<double, 2>::up_ow; }
+    else { *down_ow = StripCfg<double, 3>::down_ow; *up_ow = StripCfg<double, 3>::up_ow; }
+  } else {
+    if (s == 1) { *down_ow = StripCfg<float, 1>::down_ow; *up_ow = StripCfg<float, 1>::up_ow; }
+    else if (s == 2) { *down_ow = StripCfg<float, 2>::down_ow; *up_ow = StripCfg<float, 2>::up_ow; }
+    else { *down_ow = StripCfg<float, 3>::down_ow; *up_ow = StripCfg<float, 3>::up_ow; }
+  }
+}
+
+// Strip height for one level: the tallest of 64, 32, 16, 8 rows that still
+// gives `target` warps for this level, else 8 (taller strips amortise the
+// warm-up rows, shorter ones give small levels enough parallelism).
+int strip_rows(int ny, int nx, int ow, int target) {
+  for (int rb = 64; rb >= 8; rb >>= 1) {
+    const long long warps = (long long)ceil_div(nx, ow) * ceil_div(ny, rb);
+    if (warps >= target) return rb;
+  }
+  return 8;
+}
 
 template <typename T>
 __global__ void k_load_r(T *r, int pitch, const double *src, int spitch, int ny, int nx) {
@@ -268,6 +299,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
         L.b_off = take(arena, (size_t)ny * L.pitch);
         L.u_off = take(arena, (size_t)ny * L.pitch);
       }
+      L.w_off = -1;
       L.code_off = -1;
       if (g.boundary == GD_MASKED) {
         L.code_off = (long long)codes;
@@ -297,10 +329,23 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     p->inst.push_back(I);
   }
   // tile lists
-  const bool f64 = p->fp64;
-  const int CY = f64 ? VCfg<double, 1, 1>::CY : VCfg<float, 1, 1>::CY;
-  const int CX = f64 ? VCfg<double, 1, 1>::CX : VCfg<float, 1, 1>::CX;
-  const int UTY = 2 * CY, UTX = 2 * CX;
+  for (int i = 0; i < p->n; ++i) {
+    const InstInfo &I = p->inst[i];
+    for (int l = 0; l < bottoms[i]; ++l) {
+      LevelInfo &L = p->lv[I.level0 + l];
+      L.w_off = take(arena, (size_t)L.ny * L.pitch);
+    }
+  }
+  int down_ow = 0, up_ow = 0;
+  strip_widths(p, &down_ow, &up_ow);
+  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 1200;
+  for (int i = 0; i < p->n; ++i) {
+    const InstInfo &I = p->inst[i];
+    for (int l = 0; l < bottoms[i]; ++l) {
+      LevelInfo &L = p->lv[I.level0 + l];
+      L.rows_per_warp = strip_rows(L.ny, L.nx, std::min(down_ow, up_ow), target_warps);
+    }
+  }
   p->fine_base = (int)p->tiles.size();
   for (int i = 0; i < p->n; ++i) {
     InstInfo &I = p->inst[i];
@@ -319,9 +364,10 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     p->down_base[l] = (int)p->tiles.size();
     for (int i = 0; i < p->n; ++i) {
       if (bottoms[i] <= l) continue;
-      const LevelInfo &C = p->lv[p->inst[i].level0 + l + 1];
-      for (int ty = 0; ty < ceil_div(C.ny, CY); ++ty)
-        for (int tx = 0; tx < ceil_div(C.nx, CX); ++tx)
+      const LevelInfo &F = p->lv[p->inst[i].level0 + l];
+      const int rows = st::kWarps * F.rows_per_warp;
+      for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
+        for (int tx = 0; tx < ceil_div(F.nx, down_ow); ++tx)
           p->tiles.push_back(Tile{p->inst[i].level0 + l, i, ty, tx});
     }
     p->down_count[l] = (int)p->tiles.size() - p->down_base[l];
@@ -332,9 +378,10 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       InstInfo &I = p->inst[i];
       if (bottoms[i] <= l) continue;
       const LevelInfo &F = p->lv[I.level0 + l];
+      const int rows = st::kWarps * F.rows_per_warp;
       if (l == 0) I.up0_begin = (int)p->tiles.size() - p->up_base[0];
-      for (int ty = 0; ty < ceil_div(F.ny, UTY); ++ty)
-        for (int tx = 0; tx < ceil_div(F.nx, UTX); ++tx)
+      for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
+        for (int tx = 0; tx < ceil_div(F.nx, up_ow); ++tx)
           p->tiles.push_back(Tile{I.level0 + l, i, ty, tx});
       if (l == 0) I.up0_end = (int)p->tiles.size() - p->up_base[0];
     }
@@ -521,7 +568,7 @@ int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
   const Args<T> fine = Runner<T>::at_tiles(a, p->fine_base);
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
   k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  k_resid<T, true><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  st::k_resid_s<T, true><<<p->fine_count, st::kThreads, 0, st>>>(fine);
   prof_end(p, st);
   GD_CHECK_LAUNCH();
   GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),

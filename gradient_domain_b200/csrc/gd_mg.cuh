@@ -12,9 +12,11 @@ namespace gd {
 constexpr int kCoarsestCells = 64;
 constexpr int kBottomCells = 4096;
 
-// Fine-level Krylov kernels: 16 x 64 cells per CTA, 256 threads.
-constexpr int kFTY = 16, kFTX = 64, kFThreads = 256;
-constexpr int kVThreads = 256;     // down / up kernels
+// Fine-level (level 0) kernels: 64 rows x 128 columns per CTA of 128 threads
+// (four warps, each 16 rows x 128 columns).  Down / up kernels use the same
+// CTA shape with a per-level strip height.
+constexpr int kFTY = 64, kFTX = 128, kFThreads = 128;
+constexpr int kVThreads = 128;     // down / up kernels
 constexpr int kBThreads = 512;     // bottom kernel
 constexpr int kLastWarps = kFThreads / 32;
 
@@ -25,8 +27,10 @@ struct LevelInfo {
   int ny, nx, pitch, inst;
   int bc, level, coarse, is_bottom;
   float wall, pad0;
-  int pad1, pad2;
+  int rows_per_warp;  // strip height of the down / up kernels on this level (even)
+  int pad2;
   long long b_off, u_off;  // element offsets into the T arena
+  long long w_off;         // pre-smoothed iterate written by down, read by up
   long long code_off;      // byte offset into the code arena, -1 if rectangle
   long long inv_off;       // coarsest level: element offset of its dense inverse, else -1
 };
@@ -47,7 +51,7 @@ struct InstInfo {
 };
 
 struct InstState {
-  double rz, beta, pAp, alpha, rr, rr_ref, ff, rr_true, mean, fmean;
+  double rz, beta, pAp, alpha, rr, rr_ref, ff, rr_true, mean, fmean, rr_prev;
   int status, iters, flags, first;
   int pcur, pad;  // which of the two p buffers holds the current direction
 };
@@ -94,25 +98,5 @@ __device__ __forceinline__ int cell_class(const LevelInfo &L, const unsigned cha
 __host__ __device__ __forceinline__ double class_diag(int c, float w) {
   return 4.0 - (double)(c - 1) * (1.0 - (double)w);
 }
-
-// Shared-memory layout of the down / up kernels (host and device agree).
-template <typename T, int S1, int S2>
-struct VCfg {
-  static constexpr int CY = sizeof(T) == 4 ? 16 : 8;  // down: coarse output tile
-  static constexpr int CX = 32;
-  static constexpr int DWH = 2 * CY + 4 * S1 + 4;
-  static constexpr int DWW = 2 * CX + 4 * S1 + 4;
-  static constexpr int UTY = 2 * CY, UTX = 2 * CX;  // up: fine output tile
-  static constexpr int UH = 2 * S1 + 2 * S2;
-  static constexpr int UWH = UTY + 2 * UH;
-  static constexpr int UWW = UTX + 2 * UH;
-  static constexpr int UCH = UWH / 2 + 4, UCW = UWW / 2 + 4;
-  static constexpr size_t down_smem() {
-    return (size_t)DWH * DWW * (2 * sizeof(T) + 1) + 16;
-  }
-  static constexpr size_t up_smem() {
-    return (size_t)UWH * UWW * (2 * sizeof(T) + 1) + (size_t)UCH * UCW * sizeof(T) + 16;
-  }
-};
 
 }  // namespace gd

@@ -12,10 +12,11 @@
 // Neumann ghosts mirror, Dirichlet ghosts zero), restriction R = P^T,
 // red-black Gauss-Seidel with colour 0 then 1 before restriction and colour 1
 // then 0 after prolongation, so the cycle is a symmetric operator.  Each level
-// costs two passes over HBM: `k_down` smooths from zero, forms the residual and
-// restricts it in one shared-memory tile; `k_up` recomputes that pre-smoothed
-// iterate from b instead of storing it, adds P e and post-smooths.  Small
-// levels run in `k_bottom`, one CTA per instance, down to a dense FP64 solve.
+// costs two passes over HBM (the register-streaming kernels of gd_stream.cuh):
+// `down` smooths from zero, forms the residual and restricts it; `up`
+// recomputes that pre-smoothed iterate from b instead of storing it, adds P e
+// and post-smooths.  Small levels run in `k_bottom` (this file), one CTA per
+// instance, down to a dense FP64 solve.
 #pragma once
 
 #include "gd_mg.cuh"
@@ -66,28 +67,6 @@ __device__ __forceinline__ void finish_rz(InstState &S, double rz) {
   S.rz = rz;
 }
 
-// ---------------------------------------------------------------------------
-// Red-black half sweep on a shared-memory window of H x W cells whose (0, 0)
-// sits at global (Y0, X0).  Edge rows and columns of the window are never
-// updated, so after h half sweeps the values are exact at distance >= h from
-// the window edge; callers size the window for that.
-template <typename T>
-__device__ __forceinline__ void rb_half_window(T *su, const T *sb, const unsigned char *sc,
-                                               const T *dinv, int H, int W, int Y0, int X0,
-                                               int colour) {
-  const int hw = (W - 1) >> 1;
-  const int n = (H - 2) * hw;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const int r = k / hw;
-    const int wy = 1 + r;
-    const int wx = 1 + ((colour - (Y0 + wy) - X0 - 1) & 1) + 2 * (k - r * hw);
-    if (wx > W - 2) continue;
-    const int idx = wy * W + wx;
-    const int c = sc[idx];
-    if (c) su[idx] = (sb[idx] + su[idx - W] + su[idx + W] + su[idx - 1] + su[idx + 1]) * dinv[c];
-  }
-}
-
 template <typename T>
 __device__ __forceinline__ void make_tables(T *diag, T *dinv, float wall) {
   if (threadIdx.x < 8) {
@@ -108,178 +87,6 @@ __device__ __forceinline__ int mirror_fine(int f, int n, bool neumann) {
   if (f == -1) return 0;
   if (f == n && !(n & 1)) return n - 1;
   return f;
-}
-
-// ---------------------------------------------------------------------------
-// Down: pre-smooth S1 sweeps from zero, residual, restrict to the coarse RHS.
-template <typename T, int S1>
-__global__ void __launch_bounds__(kVThreads) k_down(Args<T> a, int tile_base) {
-  using C = VCfg<T, S1, 1>;
-  constexpr int H = C::DWH, W = C::DWW;
-  const Tile tl = a.tiles[tile_base + blockIdx.x];
-  if (a.st[tl.inst].status != GD_ACTIVE) return;
-  const LevelInfo L = a.lv[tl.level];
-  const LevelInfo Lc = a.lv[L.coarse];
-  extern __shared__ __align__(16) unsigned char smem[];
-  T *sb = reinterpret_cast<T *>(smem);
-  T *su = sb + H * W;
-  unsigned char *sc = reinterpret_cast<unsigned char *>(su + H * W);
-  __shared__ T diag[8], dinv[8];
-  make_tables(diag, dinv, L.wall);
-
-  const int I0 = tl.ty * C::CY, J0 = tl.tx * C::CX;
-  const int Y0 = 2 * I0 - 2 * S1 - 2, X0 = 2 * J0 - 2 * S1 - 2;
-  const T *B = a.arena + L.b_off;
-  for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-    const int wy = k / W, wx = k - wy * W;
-    const int gy = Y0 + wy, gx = X0 + wx;
-    const int c = cell_class(L, a.codes, gy, gx);
-    sc[k] = (unsigned char)c;
-    sb[k] = c ? B[(long long)gy * L.pitch + gx] : T(0);
-    su[k] = T(0);
-  }
-  __syncthreads();
-#pragma unroll 1
-  for (int s = 0; s < S1; ++s) {
-    rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
-    __syncthreads();
-    rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
-    __syncthreads();
-  }
-  // residual, in place over the window interior
-  for (int k = threadIdx.x; k < (H - 2) * (W - 2); k += blockDim.x) {
-    const int r = k / (W - 2);
-    const int idx = (1 + r) * W + 1 + (k - r * (W - 2));
-    const int c = sc[idx];
-    const T nb = su[idx - W] + su[idx + W] + su[idx - 1] + su[idx + 1];
-    sb[idx] = c ? sb[idx] - (diag[c] * su[idx] - nb) : T(0);
-  }
-  __syncthreads();
-  const bool neu = L.bc == BC_NEU;
-  T *Bc = a.arena + Lc.b_off;
-  for (int k = threadIdx.x; k < C::CY * C::CX; k += blockDim.x) {
-    const int I = I0 + k / C::CX, J = J0 + k % C::CX;
-    if (I >= Lc.ny || J >= Lc.nx) continue;
-    T acc = T(0);
-    if (cell_class(Lc, a.codes, I, J)) {
-#pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int wy = mirror_fine(2 * I - 1 + p, L.ny, neu) - Y0;
-        T row = T(0);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int wx = mirror_fine(2 * J - 1 + q, L.nx, neu) - X0;
-          row += (T)rweight(q) * sb[wy * W + wx];
-        }
-        acc += (T)rweight(p) * row;
-      }
-    }
-    Bc[(long long)I * Lc.pitch + J] = acc;
-  }
-}
-
-// Coarse value for interpolation: Neumann ghosts mirror the edge, Dirichlet
-// ghosts are zero.
-template <typename T>
-__device__ __forceinline__ T coarse_at(const T *E, const LevelInfo &Lc, int cy, int cx, bool neu) {
-  if (neu) {
-    cy = min(max(cy, 0), Lc.ny - 1);
-    cx = min(max(cx, 0), Lc.nx - 1);
-  } else if (cy < 0 || cy >= Lc.ny || cx < 0 || cx >= Lc.nx) {
-    return T(0);
-  }
-  return E[(long long)cy * Lc.pitch + cx];
-}
-
-// ---------------------------------------------------------------------------
-// Up: recompute the pre-smoothed iterate, add P e, post-smooth S2 sweeps.
-// On level 0 it also accumulates r.z for the Krylov step.
-template <typename T, int S1, int S2, bool LEVEL0>
-__global__ void __launch_bounds__(kVThreads) k_up(Args<T> a, int tile_base) {
-  using C = VCfg<T, S1, S2>;
-  constexpr int H = C::UWH, W = C::UWW, CH = C::UCH, CW = C::UCW;
-  const Tile tl = a.tiles[tile_base + blockIdx.x];
-  const bool active = a.st[tl.inst].status == GD_ACTIVE;
-  double part = 0.0;
-  if (active) {
-    const LevelInfo L = a.lv[tl.level];
-    const LevelInfo Lc = a.lv[L.coarse];
-    extern __shared__ __align__(16) unsigned char smem[];
-    T *sb = reinterpret_cast<T *>(smem);
-    T *su = sb + H * W;
-    T *se = su + H * W;
-    unsigned char *sc = reinterpret_cast<unsigned char *>(se + CH * CW);
-    __shared__ T diag[8], dinv[8];
-    make_tables(diag, dinv, L.wall);
-    const int Y0 = tl.ty * C::UTY - C::UH, X0 = tl.tx * C::UTX - C::UH;
-    const int CY0 = (Y0 >> 1) - 1, CX0 = (X0 >> 1) - 1;
-    const T *B = a.arena + L.b_off;
-    const T *E = a.arena + Lc.u_off;
-    const bool neu = L.bc == BC_NEU;
-    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-      const int wy = k / W, wx = k - wy * W;
-      const int gy = Y0 + wy, gx = X0 + wx;
-      const int c = cell_class(L, a.codes, gy, gx);
-      sc[k] = (unsigned char)c;
-      sb[k] = c ? B[(long long)gy * L.pitch + gx] : T(0);
-      su[k] = T(0);
-    }
-    for (int k = threadIdx.x; k < CH * CW; k += blockDim.x) {
-      const int cy = k / CW, cx = k - cy * CW;
-      se[k] = coarse_at(E, Lc, CY0 + cy, CX0 + cx, neu);
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int s = 0; s < S1; ++s) {
-      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
-      __syncthreads();
-      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
-      __syncthreads();
-    }
-    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-      if (!sc[k]) continue;
-      const int wy = k / W, wx = k - wy * W;
-      const int gy = Y0 + wy, gx = X0 + wx;
-      const int cy = (gy >> 1) - CY0, cx = (gx >> 1) - CX0;
-      const int cy2 = (gy & 1) ? cy + 1 : cy - 1;
-      const int cx2 = (gx & 1) ? cx + 1 : cx - 1;
-      const T e = (T)0.5625 * se[cy * CW + cx] +
-                  (T)0.1875 * (se[cy2 * CW + cx] + se[cy * CW + cx2]) +
-                  (T)0.0625 * se[cy2 * CW + cx2];
-      su[k] += e;
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int s = 0; s < S2; ++s) {
-      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 1);
-      __syncthreads();
-      rb_half_window(su, sb, sc, dinv, H, W, Y0, X0, 0);
-      __syncthreads();
-    }
-    T *U = a.arena + L.u_off;
-    for (int k = threadIdx.x; k < C::UTY * C::UTX; k += blockDim.x) {
-      const int oy = k / C::UTX, ox = k - oy * C::UTX;
-      const int gy = Y0 + C::UH + oy, gx = X0 + C::UH + ox;
-      if (gy >= L.ny || gx >= L.nx) continue;
-      const int idx = (C::UH + oy) * W + C::UH + ox;
-      const T v = sc[idx] ? su[idx] : T(0);
-      U[(long long)gy * L.pitch + gx] = v;
-      if (LEVEL0) part += (double)sb[idx] * (double)v;
-    }
-  }
-  if (!LEVEL0) return;
-  part = block_sum<kVThreads>(part);
-  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
-  if (!last_block(a.counter + 3)) return;
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int i = warp; i < a.ninst; i += nw) {
-    const InstInfo &I = a.inst[i];
-    if (I.up0_end <= I.up0_begin) continue;
-    InstState &S = a.st[i];
-    if (S.status != GD_ACTIVE) continue;
-    const double rz = warp_range_sum(a.part0, I.up0_begin, I.up0_end);
-    if ((threadIdx.x & 31) == 0) finish_rz(S, rz);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -477,136 +284,8 @@ __global__ void __launch_bounds__(kBThreads) k_bottom(Args<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// Fine-level Krylov kernels over 16 x 64 tiles of level 0.
-
-template <typename T, typename V>
-__device__ __forceinline__ T apply_tile(const V *s, int idx, int c, const T *diag) {
-  constexpr int W = kFTX + 2;
-  return c ? (T)(diag[c] * (T)s[idx] - (T)(s[idx - W] + s[idx + W] + s[idx - 1] + s[idx + 1]))
-           : T(0);
-}
-
-// p = z + beta p and the partial p.Ap; the last CTA forms alpha = rz / pAp.
-template <typename T>
-__global__ void __launch_bounds__(kFThreads) k_pupdate(Args<T> a) {
-  constexpr int W = kFTX + 2, H = kFTY + 2;
-  const Tile tl = a.tiles[blockIdx.x];
-  const bool active = a.st[tl.inst].status == GD_ACTIVE;
-  double part = 0.0;
-  if (active) {
-    const InstInfo &I = a.inst[tl.inst];
-    const LevelInfo L = a.lv[I.level0];
-    __shared__ T sp[H * W];
-    __shared__ T diag[8], dinv[8];
-    make_tables(diag, dinv, L.wall);
-    const T beta = (T)a.st[tl.inst].beta;
-    const int cur = a.st[tl.inst].pcur;
-    const T *z = a.arena + I.z_off;
-    const T *p = a.arena + p_offset(I, cur);
-    T *pn = a.arena + p_offset(I, cur ^ 1);
-    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
-    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-      const int wy = k / W, wx = k - wy * W;
-      const int gy = Y0 + wy, gx = X0 + wx;
-      T v = T(0);
-      if (in_grid(L, gy, gx)) {
-        const long long g = (long long)gy * L.pitch + gx;
-        v = z[g] + beta * p[g];
-      }
-      sp[k] = v;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-      const int oy = k / kFTX, ox = k - oy * kFTX;
-      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
-      if (gy >= L.ny || gx >= L.nx) continue;
-      const int idx = (1 + oy) * W + 1 + ox;
-      const int c = cell_class(L, a.codes, gy, gx);
-      const T pv = sp[idx];
-      part += (double)pv * (double)apply_tile<T, T>(sp, idx, c, diag);
-      pn[(long long)gy * L.pitch + gx] = pv;
-    }
-  }
-  part = block_sum<kFThreads>(part);
-  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
-  if (!last_block(a.counter + 0)) return;
-  const int warp = threadIdx.x >> 5;
-  for (int i = warp; i < a.ninst; i += kLastWarps) {
-    InstState &S = a.st[i];
-    if (S.status != GD_ACTIVE) continue;
-    const InstInfo &I = a.inst[i];
-    const double pAp = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
-    if ((threadIdx.x & 31) == 0) {
-      const double alpha = S.rz / pAp;
-      S.pAp = pAp;
-      S.pcur ^= 1;
-      if (!(pAp > 0.0) || !isfinite(alpha)) {
-        S.status = GD_BREAKDOWN;
-        S.flags |= FLAG_RU;
-      } else {
-        S.alpha = alpha;
-      }
-    }
-  }
-}
-
-// d += alpha p, r -= alpha A p and the partial r.r; the last CTA counts the
-// iteration and schedules an FP64 residual refresh when due.
-template <typename T>
-__global__ void __launch_bounds__(kFThreads) k_cgupdate(Args<T> a) {
-  constexpr int W = kFTX + 2, H = kFTY + 2;
-  const Tile tl = a.tiles[blockIdx.x];
-  const bool active = a.st[tl.inst].status == GD_ACTIVE;
-  double part = 0.0;
-  if (active) {
-    const InstInfo &I = a.inst[tl.inst];
-    const LevelInfo L = a.lv[I.level0];
-    __shared__ T sp[H * W];
-    __shared__ T diag[8], dinv[8];
-    make_tables(diag, dinv, L.wall);
-    const T alpha = (T)a.st[tl.inst].alpha;
-    const T *p = a.arena + p_offset(I, a.st[tl.inst].pcur);
-    T *d = a.arena + I.d_off;
-    T *r = a.arena + I.r_off;
-    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
-    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-      const int wy = k / W, wx = k - wy * W;
-      const int gy = Y0 + wy, gx = X0 + wx;
-      sp[k] = in_grid(L, gy, gx) ? p[(long long)gy * L.pitch + gx] : T(0);
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-      const int oy = k / kFTX, ox = k - oy * kFTX;
-      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
-      if (gy >= L.ny || gx >= L.nx) continue;
-      const int idx = (1 + oy) * W + 1 + ox;
-      const int c = cell_class(L, a.codes, gy, gx);
-      const long long g = (long long)gy * L.pitch + gx;
-      const T ap = apply_tile<T, T>(sp, idx, c, diag);
-      d[g] += alpha * sp[idx];
-      const T rn = r[g] - alpha * ap;
-      r[g] = rn;
-      part += (double)rn * (double)rn;
-    }
-  }
-  part = block_sum<kFThreads>(part);
-  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
-  if (!last_block(a.counter + 1)) return;
-  const int warp = threadIdx.x >> 5;
-  for (int i = warp; i < a.ninst; i += kLastWarps) {
-    InstState &S = a.st[i];
-    if (S.status != GD_ACTIVE) continue;
-    const InstInfo &I = a.inst[i];
-    const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
-    if ((threadIdx.x & 31) == 0) {
-      S.rr = rr;
-      S.iters += 1;
-      if (rr <= a.delta2 * S.rr_ref || rr <= a.tol2 * S.ff || S.iters >= a.max_iter ||
-          !isfinite(rr))
-        S.flags |= FLAG_RU;
-    }
-  }
-}
+// Elementwise level-0 kernels over 64 x 128 tiles (the Krylov kernels with
+// halos are in gd_stream.cuh).
 
 // x += d, d = 0 for instances with a pending FP64 refresh.
 template <typename T>
@@ -622,107 +301,6 @@ __global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
     const long long g = (long long)gy * I.pitch + gx;
     I.x[(long long)gy * I.upitch + gx] += (double)d[g];
     d[g] = T(0);
-  }
-}
-
-// FP64 residual r = scale f - A x of the refreshed (or, with INIT, initial)
-// iterate, its norm, and the convergence decision.
-template <typename T, bool INIT>
-__global__ void __launch_bounds__(kFThreads) k_resid(Args<T> a) {
-  constexpr int W = kFTX + 2, H = kFTY + 2;
-  const Tile tl = a.tiles[blockIdx.x];
-  const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
-  double part = 0.0, part_f = 0.0;
-  if (work) {
-    const InstInfo &I = a.inst[tl.inst];
-    const LevelInfo L = a.lv[I.level0];
-    __shared__ double sx[H * W];
-    __shared__ double diag[8], dinv[8];
-    make_tables(diag, dinv, L.wall);
-    const int Y0 = tl.ty * kFTY - 1, X0 = tl.tx * kFTX - 1;
-    for (int k = threadIdx.x; k < H * W; k += blockDim.x) {
-      const int wy = k / W, wx = k - wy * W;
-      const int gy = Y0 + wy, gx = X0 + wx;
-      const int c = cell_class(L, a.codes, gy, gx);
-      sx[k] = c ? I.x[(long long)gy * I.upitch + gx] : 0.0;
-    }
-    __syncthreads();
-    T *r = a.arena + I.r_off;
-    const double fmean = a.st[tl.inst].fmean;
-    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-      const int oy = k / kFTX, ox = k - oy * kFTX;
-      const int gy = Y0 + 1 + oy, gx = X0 + 1 + ox;
-      if (gy >= L.ny || gx >= L.nx) continue;
-      const int idx = (1 + oy) * W + 1 + ox;
-      const int c = cell_class(L, a.codes, gy, gx);
-      const long long g = (long long)gy * L.pitch + gx;
-      const long long gu = (long long)gy * I.upitch + gx;
-      const double f = c ? I.scale * (I.f[gu] - fmean) : 0.0;
-      const double r64 = c ? f - apply_tile<double, double>(sx, idx, c, diag) : 0.0;
-      r[g] = (T)r64;
-      part += r64 * r64;
-      if (INIT) {
-        part_f += f * f;
-        a.arena[I.d_off + g] = T(0);
-        a.arena[I.p_off + g] = T(0);
-        a.arena[I.q_off + g] = T(0);
-        a.arena[I.z_off + g] = T(0);
-        if (!c) I.x[gu] = 0.0;
-      }
-    }
-  }
-  part = block_sum<kFThreads>(part);
-  if (INIT) {
-    __syncthreads();
-    part_f = block_sum<kFThreads>(part_f);
-  }
-  if (threadIdx.x == 0) {
-    a.part0[blockIdx.x] = part;
-    if (INIT) a.part1[blockIdx.x] = part_f;
-  }
-  if (!last_block(a.counter + 2)) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int active = 0;
-  for (int i = warp; i < a.ninst; i += kLastWarps) {
-    InstState &S = a.st[i];
-    const InstInfo &I = a.inst[i];
-    const bool part_of = INIT || (S.flags & FLAG_RU);
-    if (part_of) {
-      const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
-      double ff = 0.0;
-      if (INIT) ff = warp_range_sum(a.part1, I.fine_begin, I.fine_end);
-      if (lane == 0) {
-        if (INIT) {
-          S.ff = ff;
-          S.iters = 0;
-          S.first = 1;
-          S.rz = 0.0;
-          S.beta = 0.0;
-          S.pcur = 0;
-          S.status = GD_ACTIVE;
-        }
-        S.rr_true = rr;
-        S.rr_ref = rr;
-        S.rr = rr;
-        if (rr <= a.tol2 * S.ff) {
-          S.status = GD_CONVERGED;
-        } else if (!isfinite(rr)) {
-          S.status = GD_BREAKDOWN;
-        } else if (S.status == GD_ACTIVE && S.iters >= a.max_iter) {
-          S.status = GD_MAX_ITERATIONS;
-        }
-        S.flags = 0;
-      }
-    }
-    if (lane == 0 && S.status == GD_ACTIVE) ++active;
-  }
-  __shared__ int cnt[kLastWarps];
-  if (lane == 0) cnt[warp] = active;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int t = 0;
-    for (int w = 0; w < kLastWarps; ++w) t += cnt[w];
-    *a.n_active = t;
   }
 }
 

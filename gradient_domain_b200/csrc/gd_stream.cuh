@@ -1,0 +1,1129 @@
+// Register-streaming kernels of the batched cell-centred MGPCG.
+//
+// Every kernel here works on vertical strips.  A warp owns 128 consecutive
+// columns (4 per lane, one 128-bit vector for FP32) and walks down its strip
+// one row at a time; the rows it still needs live in small register windows,
+// vertical neighbours are window entries and horizontal neighbours at lane
+// boundaries come from warp shuffles.  Nothing is staged in shared memory.
+//
+// The smoothing kernels pipeline the red-black half sweeps: when row y is
+// loaded, half sweep 1 runs on row y, half sweep 2 on row y-1, ..., so after
+// the last stage a row has seen every sweep and the residual / restriction /
+// prolongation / output stages follow further up the window.  Each half sweep
+// widens the set of cells whose value depends on data outside the strip by
+// one column, so the outermost lanes of a warp ("halo lanes") compute values
+// that are never written; rows at the top of a strip are likewise warm-up
+// rows.  Halo lanes and warm-up rows are the only redundant work.
+#pragma once
+
+#include <cuda_pipeline.h>
+
+#include "gd_mg_kernels.cuh"
+
+namespace gd {
+namespace st {
+
+constexpr int kLanes = 32;
+constexpr int kWarps = 4;          // warps per CTA
+constexpr int kThreads = kWarps * kLanes;
+constexpr int kKrylovRows = 16;    // rows per warp in the Krylov kernels
+constexpr int kKrylovCols = 128;   // columns per warp (and per CTA)
+
+template <typename T>
+struct V4 {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ V4<T> ld4(const T *p) {
+  V4<T> r;
+  if constexpr (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4 *>(p);
+    r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y;
+  }
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void st4(T *p, const V4<T> &r) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  } else {
+    *reinterpret_cast<double2 *>(p) = make_double2(r.v[0], r.v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(r.v[2], r.v[3]);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ V4<T> zero4() {
+  V4<T> r;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) r.v[j] = T(0);
+  return r;
+}
+
+// Per-level constants: 1/d and d for each wall count 0..4 (classes 1..5).
+template <typename T>
+struct Diag {
+  T d[5], inv[5];
+  __device__ __forceinline__ void init(float wall) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double dd = 4.0 - (double)k * (1.0 - (double)wall);
+      d[k] = (T)dd;
+      inv[k] = dd > 0.0 ? (T)(1.0 / dd) : T(0);
+    }
+  }
+  // class 0 (no unknown) -> 0
+  __device__ __forceinline__ T inv_of(int c) const {
+    T r = T(0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r = (c == k + 1) ? inv[k] : r;
+    return r;
+  }
+  __device__ __forceinline__ T d_of(int c) const {
+    T r = T(0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r = (c == k + 1) ? d[k] : r;
+    return r;
+  }
+};
+
+// Classes of the 4 cells x0..x0+3 of row y, packed one byte each.
+__device__ __forceinline__ unsigned row_classes(const LevelInfo &L, const unsigned char *codes,
+                                                int y, int x0) {
+  if (y < 0 || y >= L.ny || x0 >= L.nx || x0 + 3 < 0) return 0u;
+  if (L.code_off >= 0) {
+    if (x0 < 0) return 0u;  // x0 is a multiple of 4: a lane is wholly left of the grid or in it
+    return *reinterpret_cast<const unsigned *>(codes + L.code_off + (long long)y * L.pitch + x0);
+  }
+  const int wy = (y == 0) + (y == L.ny - 1);
+  unsigned packed = 0u;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int x = x0 + j;
+    if (x >= 0 && x < L.nx) {
+      const unsigned c = 1u + wy + (x == 0) + (x == L.nx - 1);
+      packed |= c << (8 * j);
+    }
+  }
+  return packed;
+}
+
+__device__ __forceinline__ int cls(unsigned packed, int j) { return (packed >> (8 * j)) & 0xff; }
+
+// Row of T values at (y, x0..x0+3); zero outside the grid.
+template <typename T>
+__device__ __forceinline__ V4<T> load_row(const T *A, const LevelInfo &L, int y, int x0) {
+  if (y < 0 || y >= L.ny || x0 < 0 || x0 >= L.nx) return zero4<T>();
+  return ld4(A + (long long)y * L.pitch + x0);
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename T>
+__device__ __forceinline__ T shfl_dn1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// One red-black half sweep of colour `colour` on row window U[k] (row y_k):
+// cells j with (y_k + x0 + j) odd/even = colour; x0 is a multiple of 4.
+template <typename T>
+__device__ __forceinline__ void half_sweep(V4<T> &u, const V4<T> &up, const V4<T> &dn,
+                                           const V4<T> &b, unsigned c, const Diag<T> &D,
+                                           int yk, int colour) {
+  const int j0 = (colour + yk) & 1;  // warp-uniform
+  if (j0 == 0) {
+    const T left = shfl_up1(u.v[3]);
+    u.v[0] = (b.v[0] + up.v[0] + dn.v[0] + left + u.v[1]) * D.inv_of(cls(c, 0));
+    u.v[2] = (b.v[2] + up.v[2] + dn.v[2] + u.v[1] + u.v[3]) * D.inv_of(cls(c, 2));
+  } else {
+    const T right = shfl_dn1(u.v[0]);
+    u.v[1] = (b.v[1] + up.v[1] + dn.v[1] + u.v[0] + u.v[2]) * D.inv_of(cls(c, 1));
+    u.v[3] = (b.v[3] + up.v[3] + dn.v[3] + u.v[2] + right) * D.inv_of(cls(c, 3));
+  }
+}
+
+// First half sweep from a zero iterate: only the cells of the colour change.
+template <typename T>
+__device__ __forceinline__ void half_sweep_from_zero(V4<T> &u, const V4<T> &b, unsigned c,
+                                                     const Diag<T> &D, int yk) {
+  const int j0 = yk & 1;  // colour 0
+#pragma unroll
+  for (int j = 0; j < 4; ++j) u.v[j] = ((j & 1) == j0) ? b.v[j] * D.inv_of(cls(c, j)) : T(0);
+}
+
+// A u on one row: d u - (up + down + left + right), zero where there is no unknown.
+template <typename T>
+__device__ __forceinline__ V4<T> apply_row(const V4<T> &u, const V4<T> &up, const V4<T> &dn,
+                                           T left, T right, unsigned c, const Diag<T> &D) {
+  V4<T> r;
+  const T lf[4] = {left, u.v[0], u.v[1], u.v[2]};
+  const T rt[4] = {u.v[1], u.v[2], u.v[3], right};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int cj = cls(c, j);
+    r.v[j] = cj ? D.d_of(cj) * u.v[j] - (up.v[j] + dn.v[j] + lf[j] + rt[j]) : T(0);
+  }
+  return r;
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void shift(V4<T> (&w)[N]) {
+#pragma unroll
+  for (int k = N - 1; k > 0; --k) w[k] = w[k - 1];
+}
+
+template <int N>
+__device__ __forceinline__ void shift(unsigned (&w)[N]) {
+#pragma unroll
+  for (int k = N - 1; k > 0; --k) w[k] = w[k - 1];
+}
+
+// Per-lane ring of RS row slices (4 elements each) in shared memory, filled
+// with cp.async so that RS - 1 rows per lane are in flight while the current
+// row is processed.  A lane only ever reads back the bytes it copied itself,
+// so a per-thread wait_group is the only synchronisation.  Slot s of a lane
+// sits at ((s * kThreads) + threadIdx.x) * 4 elements: a warp touches 512
+// (FP32) contiguous bytes per slot, free of bank conflicts.
+constexpr int kRing = 8;
+
+template <typename T>
+struct Ring {
+  T *base;
+  __device__ __forceinline__ explicit Ring(T *smem) : base(smem + threadIdx.x * 4) {}
+  __device__ __forceinline__ T *slot(int s) const { return base + (s & (kRing - 1)) * kThreads * 4; }
+  // Copy A[y, x0 .. x0 + 3] into slot s, or zeros when the row or lane is outside the grid.
+  __device__ __forceinline__ void issue(int s, const T *A, const LevelInfo &L, int y, int x0) const {
+    const bool ok = y >= 0 && y < L.ny && x0 >= 0 && x0 < L.nx;
+    const T *src = ok ? A + (long long)y * L.pitch + x0 : A;
+    T *dst = slot(s);
+    constexpr int chunks = (int)(4 * sizeof(T) / 16);
+#pragma unroll
+    for (int k = 0; k < chunks; ++k)
+      __pipeline_memcpy_async(dst + k * (16 / sizeof(T)), src + (ok ? k * (16 / sizeof(T)) : 0),
+                              16, ok ? 0 : 16);
+  }
+  __device__ __forceinline__ V4<T> read(int s) const { return ld4(slot(s)); }
+};
+
+// Per-lane ring of packed cell classes of masked levels (4 bytes per row).
+struct CodeRing {
+  unsigned *base;
+  __device__ __forceinline__ explicit CodeRing(unsigned *smem) : base(smem + threadIdx.x) {}
+  __device__ __forceinline__ unsigned *slot(int s) const {
+    return base + (s & (kRing - 1)) * kThreads;
+  }
+  __device__ __forceinline__ void issue(int s, const LevelInfo &L, const unsigned char *codes,
+                                        int y, int x0) const {
+    const bool ok = y >= 0 && y < L.ny && x0 >= 0 && x0 < L.nx;
+    const unsigned char *src = ok ? codes + L.code_off + (long long)y * L.pitch + x0 : codes;
+    __pipeline_memcpy_async(slot(s), src, 4, ok ? 0 : 4);
+  }
+  __device__ __forceinline__ unsigned read(int s) const { return *slot(s); }
+};
+
+// Per-lane ring of one element per row: the column just outside the warp
+// (left of lane 0, right of lane 31), so edge values arrive with their row.
+template <typename T>
+struct EdgeRing {
+  T *base;
+  __device__ __forceinline__ explicit EdgeRing(T *smem) : base(smem + threadIdx.x) {}
+  __device__ __forceinline__ T *slot(int s) const { return base + (s & (kRing - 1)) * kThreads; }
+  __device__ __forceinline__ void issue(int s, const T *A, const LevelInfo &L, int y, int x) const {
+    const bool ok = y >= 0 && y < L.ny && x >= 0 && x < L.nx;
+    __pipeline_memcpy_async(slot(s), ok ? A + (long long)y * L.pitch + x : A, sizeof(T),
+                            ok ? 0 : sizeof(T));
+  }
+  __device__ __forceinline__ T read(int s) const { return *slot(s); }
+};
+
+// Cell classes of row y: computed for rectangles, from the ring for masks.
+__device__ __forceinline__ unsigned classes_at(const LevelInfo &L, const CodeRing &cr, int s,
+                                               int y, int x0) {
+  if (L.code_off >= 0) return cr.read(s);
+  return row_classes(L, nullptr, y, x0);
+}
+
+// Dynamic shared memory of the streaming kernels (rings).
+template <typename T>
+constexpr size_t ring_bytes() { return (size_t)kRing * kThreads * 4 * sizeof(T); }
+template <typename T>
+constexpr size_t level_smem() { return 2 * ring_bytes<T>() + (size_t)kRing * kThreads * 4; }
+template <typename T>
+constexpr size_t edge_bytes() { return (size_t)kRing * kThreads * sizeof(T); }
+template <typename T>
+constexpr size_t pupdate_smem() { return 2 * ring_bytes<T>() + 2 * edge_bytes<T>(); }
+template <typename T>
+constexpr size_t cgupdate_smem() { return 3 * ring_bytes<T>() + edge_bytes<T>(); }
+
+// Lanes whose output is exact for a dependency radius of R columns.
+template <int R>
+struct Halo {
+  static constexpr int HL = (R + 3) / 4;
+  static constexpr int OUT_LANES = kLanes - 2 * HL;
+  static constexpr int OW = 4 * OUT_LANES;  // output columns per strip
+};
+
+// ---------------------------------------------------------------------------
+// Shared by the smoothing kernels.
+//
+// Diagonal entries by cell class, in shared memory: one LDS replaces a chain
+// of compares in the general path.  Strips that touch no grid boundary and no
+// mask ("interior" strips, almost all of them on large rectangles) skip the
+// classes altogether and use the interior diagonal as a constant.
+template <typename T>
+struct ClassTable {
+  T d[8], inv[8];
+};
+
+template <typename T>
+__device__ __forceinline__ void fill_table(ClassTable<T> &t, float wall) {
+  if (threadIdx.x < 8) {
+    const int c = threadIdx.x;
+    const double dd = (c >= 1 && c <= 5) ? 4.0 - (double)(c - 1) * (1.0 - (double)wall) : 0.0;
+    t.d[c] = (T)dd;
+    t.inv[c] = dd > 0.0 ? (T)(1.0 / dd) : T(0);
+  }
+  __syncthreads();
+}
+
+template <typename T, bool INT>
+struct Coef {
+  const ClassTable<T> &tab;
+  T d_int, inv_int;
+  __device__ __forceinline__ T inv(unsigned c, int j) const {
+    if constexpr (INT) return inv_int;
+    else return tab.inv[cls(c, j)];
+  }
+  __device__ __forceinline__ T d(unsigned c, int j) const {
+    if constexpr (INT) return d_int;
+    else return tab.d[cls(c, j)];
+  }
+  __device__ __forceinline__ bool on(unsigned c, int j) const {
+    if constexpr (INT) return true;
+    else return cls(c, j) != 0;
+  }
+};
+
+// Half sweep on one row; J0 (first updated cell of the lane) is compile-time.
+template <int J0, typename T, bool INT>
+__device__ __forceinline__ void hsweep(V4<T> &u, const V4<T> &up, const V4<T> &dn,
+                                       const V4<T> &b, unsigned c, const Coef<T, INT> &K) {
+  if constexpr (J0 == 0) {
+    const T left = shfl_up1(u.v[3]);
+    u.v[0] = (b.v[0] + up.v[0] + dn.v[0] + left + u.v[1]) * K.inv(c, 0);
+    u.v[2] = (b.v[2] + up.v[2] + dn.v[2] + u.v[1] + u.v[3]) * K.inv(c, 2);
+  } else {
+    const T right = shfl_dn1(u.v[0]);
+    u.v[1] = (b.v[1] + up.v[1] + dn.v[1] + u.v[0] + u.v[2]) * K.inv(c, 1);
+    u.v[3] = (b.v[3] + up.v[3] + dn.v[3] + u.v[2] + right) * K.inv(c, 3);
+  }
+}
+
+template <int J0, typename T, bool INT>
+__device__ __forceinline__ void hsweep_zero(V4<T> &u, const V4<T> &b, unsigned c,
+                                            const Coef<T, INT> &K) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) u.v[j] = ((j & 1) == J0) ? b.v[j] * K.inv(c, j) : T(0);
+}
+
+// A u on a row (zero where there is no unknown).
+template <typename T, bool INT>
+__device__ __forceinline__ V4<T> arow(const V4<T> &u, const V4<T> &up, const V4<T> &dn, T left,
+                                      T right, unsigned c, const Coef<T, INT> &K) {
+  V4<T> r;
+  const T lf[4] = {left, u.v[0], u.v[1], u.v[2]};
+  const T rt[4] = {u.v[1], u.v[2], u.v[3], right};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const T v = K.d(c, j) * u.v[j] - (up.v[j] + dn.v[j] + lf[j] + rt[j]);
+    r.v[j] = K.on(c, j) ? v : T(0);
+  }
+  return r;
+}
+
+// Window slot of "row y - k" at unrolled phase PH of a circular window of U rows.
+template <int U>
+__host__ __device__ constexpr int wslot(int ph, int k) {
+  return ((ph - k) % U + U) % U;
+}
+
+// ---------------------------------------------------------------------------
+// Down: S1 pre-sweeps from zero, residual, restriction (P^T) of one strip.
+// Radius: 2 S1 - 1 (sweeps) + 1 (residual) + 1 (restriction) columns.
+template <typename T, int S1>
+struct DownGeom {
+  using H = Halo<2 * S1 + 1>;
+  static constexpr int U = 2 * S1 + 2;  // rows in every circular window (even)
+};
+
+template <typename T, int S1, bool INT>
+__device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
+                                           const LevelInfo &Lc, const ClassTable<T> &tab,
+                                           int x0, bool out_lane, int y_start, int y_last,
+                                           int y_out0, int y_out1, int I_begin, int I_end,
+                                           unsigned char *smem) {
+  constexpr int U = DownGeom<T, S1>::U;
+  constexpr int K = 2 * S1;  // window index of the residual row
+  const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
+  const bool neu = L.bc == BC_NEU;
+  const bool masked = L.code_off >= 0;
+  const T *B = a.arena + L.b_off;
+  T *Bc = a.arena + Lc.b_off;
+  T *Wp = a.arena + L.w_off;
+  const bool store_lane = out_lane && x0 >= 0 && x0 < L.nx;
+  const Ring<T> ring(reinterpret_cast<T *>(smem));
+  const CodeRing cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T>()));
+  V4<T> Bw[U], Uw[U], F[U];
+  unsigned Cw[U];
+#pragma unroll
+  for (int k = 0; k < U; ++k) { Bw[k] = zero4<T>(); Uw[k] = zero4<T>(); F[k] = zero4<T>(); Cw[k] = 0u; }
+  const int m_left = -1 - x0;
+  const int m_right = L.nx - x0;
+  for (int q = 0; q < kRing - 1; ++q) {
+    ring.issue(q, B, L, y_start + q, x0);
+    if (!INT && masked) cring.issue(q, L, a.codes, y_start + q, x0);
+    __pipeline_commit();
+  }
+  for (int base = y_start; base <= y_last; base += U) {
+#pragma unroll
+    for (int ph = 0; ph < U; ++ph) {
+      const int y = base + ph;
+      if (y > y_last) break;
+      const int step = y - y_start;
+      __pipeline_wait_prior(kRing - 2);
+      Bw[wslot<U>(ph, 0)] = ring.read(step);
+      if (!INT) Cw[wslot<U>(ph, 0)] = masked ? cring.read(step) : row_classes(L, nullptr, y, x0);
+      ring.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
+      if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      __pipeline_commit();
+      // y_start is even, so the parity of y is the parity of ph
+      if ((ph & 1) == 0)
+        hsweep_zero<0, T, INT>(Uw[wslot<U>(ph, 0)], Bw[wslot<U>(ph, 0)], Cw[wslot<U>(ph, 0)], C);
+      else
+        hsweep_zero<1, T, INT>(Uw[wslot<U>(ph, 0)], Bw[wslot<U>(ph, 0)], Cw[wslot<U>(ph, 0)], C);
+#pragma unroll
+      for (int h = 2; h <= 2 * S1; ++h) {
+        const int k = h - 1;
+        if (((h - 1 + ph - k) & 1) == 0)
+          hsweep<0, T, INT>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                            Bw[wslot<U>(ph, k)], Cw[wslot<U>(ph, k)], C);
+        else
+          hsweep<1, T, INT>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                            Bw[wslot<U>(ph, k)], Cw[wslot<U>(ph, k)], C);
+      }
+      {  // row y - (2 S1 - 1) has seen every pre-sweep: keep it for the up kernel
+        constexpr int KP = 2 * S1 - 1;
+        const int yw = y - KP;
+        if (yw >= y_out0 && yw < y_out1 && store_lane) {
+          const V4<T> &v = Uw[wslot<U>(ph, KP)];
+          T *dst = Wp + (long long)yw * L.pitch + x0;
+          if (x0 + 3 < L.nx) {
+            st4(dst, v);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (x0 + j < L.nx) dst[j] = v.v[j];
+          }
+        }
+      }
+      // residual of row yr = y - 2 S1
+      const int yr = y - K;
+      const V4<T> &uK = Uw[wslot<U>(ph, K)];
+      const T left = shfl_up1(uK.v[3]);
+      const T right = shfl_dn1(uK.v[0]);
+      const unsigned cK = Cw[wslot<U>(ph, K)];
+      const V4<T> au = arow(uK, Uw[wslot<U>(ph, K + 1)], Uw[wslot<U>(ph, K - 1)], left, right, cK, C);
+      const V4<T> &bK = Bw[wslot<U>(ph, K)];
+      V4<T> res;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) res.v[j] = C.on(cK, j) ? bK.v[j] - au.v[j] : T(0);
+      T e[6];
+      e[0] = shfl_up1(res.v[3]);
+      e[1] = res.v[0]; e[2] = res.v[1]; e[3] = res.v[2]; e[4] = res.v[3];
+      e[5] = shfl_dn1(res.v[0]);
+      if (!INT && neu) {
+        if (m_left == -1) e[0] = e[1];
+        if (!(L.nx & 1)) {
+#pragma unroll
+          for (int m = 0; m <= 4; ++m)
+            if (m == m_right) e[m + 1] = e[m];
+        }
+      }
+      V4<T> &Fr = F[wslot<U>(ph, K)];
+      Fr.v[0] = T(0.25) * e[0] + T(0.75) * e[1] + T(0.75) * e[2] + T(0.25) * e[3];
+      Fr.v[1] = T(0.25) * e[2] + T(0.75) * e[3] + T(0.75) * e[4] + T(0.25) * e[5];
+      // coarse row I = yr / 2 - 1 from residual rows 2I-1 .. 2I+2 (yr even <=> ph even)
+      if ((ph & 1) == 0) {
+        const int I = (yr >> 1) - 1;
+        if (I >= I_begin && I < I_end) {
+          T rows[4][2];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            rows[q][0] = F[wslot<U>(ph, K + 3 - q)].v[0];
+            rows[q][1] = F[wslot<U>(ph, K + 3 - q)].v[1];
+          }
+          if (!INT && neu) {
+            if (I == 0) { rows[0][0] = rows[1][0]; rows[0][1] = rows[1][1]; }
+            if (!(L.ny & 1)) {
+#pragma unroll
+              for (int q = 1; q < 4; ++q)
+                if (2 * I - 1 + q == L.ny) { rows[q][0] = rows[q - 1][0]; rows[q][1] = rows[q - 1][1]; }
+            }
+          }
+          if (out_lane) {
+            const int J0 = x0 >> 1;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int J = J0 + q;
+              if (J >= 0 && J < Lc.nx) {
+                T v = T(0.25) * rows[0][q] + T(0.75) * rows[1][q] + T(0.75) * rows[2][q] +
+                      T(0.25) * rows[3][q];
+                if (!INT && Lc.code_off >= 0 && !a.codes[Lc.code_off + (long long)I * Lc.pitch + J])
+                  v = T(0);
+                Bc[(long long)I * Lc.pitch + J] = v;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  __pipeline_wait_prior(0);  // no copy may land after this warp's shared memory is released
+}
+
+// Is every cell a strip loads an interior cell of an unmasked level?
+__device__ __forceinline__ bool strip_interior(const LevelInfo &L, int y_lo, int y_hi, int x_lo,
+                                               int x_hi) {
+  return L.code_off < 0 && y_lo >= 1 && y_hi <= L.ny - 2 && x_lo >= 1 && x_hi <= L.nx - 2;
+}
+
+template <typename T, int S1>
+__global__ void __launch_bounds__(kThreads) k_down_s(Args<T> a) {
+  using G = DownGeom<T, S1>;
+  using H = typename G::H;
+  __shared__ ClassTable<T> tab;
+  const Tile tl = a.tiles[blockIdx.x];
+  if (a.st[tl.inst].status != GD_ACTIVE) return;
+  const LevelInfo L = a.lv[tl.level];
+  fill_table(tab, L.wall);
+  const LevelInfo Lc = a.lv[L.coarse];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int RB = L.rows_per_warp;  // even
+  const int y_out0 = (tl.ty * kWarps + warp) * RB;
+  if (y_out0 >= L.ny) return;
+  const int xl = tl.tx * H::OW - 4 * H::HL;
+  const int x0 = xl + 4 * lane;
+  const bool out_lane = lane >= H::HL && lane < kLanes - H::HL;
+  const int I_begin = y_out0 >> 1;
+  const int I_end = min((y_out0 + RB) >> 1, Lc.ny);
+  const int y_out1 = min(y_out0 + RB, L.ny);
+  const int y_start = (y_out0 - 1 - 2 * S1) & ~1;  // even, at least the rows the sweeps need
+  const int y_last = max(2 * I_end + 2 * S1, y_out1 - 1 + 2 * S1 - 1);
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (strip_interior(L, y_start, y_last, xl, xl + 127))
+    down_strip<T, S1, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
+                            I_begin, I_end, smem);
+  else
+    down_strip<T, S1, false>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
+                             I_begin, I_end, smem);
+}
+
+// ---------------------------------------------------------------------------
+// Up: u = (pre-smoothed iterate from down) + P e, then S2 post-sweeps (colour
+// 1 first).  Radius: 2 S2 columns.  On level 0 also r.z.  (S1 only selects the
+// matching down kernel's plan; the up kernel does not depend on it.)
+template <typename T, int S1, int S2>
+struct UpGeom {
+  using H = Halo<2 * S2>;
+  static constexpr int O = 2 * S2;   // window index of the output row
+  static constexpr int U = O + 2;    // rows in every circular window (even)
+};
+
+// The lane's two coarse values (columns x0/2, x0/2 + 1) of coarse row cy, with
+// Neumann ghosts mirrored and Dirichlet ghosts zero.
+// Lanes 0 and 31 also load the coarse column just outside the warp (c0 - 1,
+// resp. c0 + 2), so the interpolated row is exact in every lane of the warp.
+template <typename T>
+struct Pair {
+  T v0, v1, outer;
+};
+
+template <typename T>
+__device__ __forceinline__ T coarse_at(const T *row, const LevelInfo &Lc, int c, bool neu) {
+  if (neu) return row[min(max(c, 0), Lc.nx - 1)];
+  return (c >= 0 && c < Lc.nx) ? row[c] : T(0);
+}
+
+template <typename T>
+__device__ __forceinline__ Pair<T> coarse_pair(const T *E, const LevelInfo &Lc, int cy, int x0,
+                                               bool neu) {
+  const int c0 = x0 >> 1;  // x0 may be negative; x0 is a multiple of 4 so this is exact
+  const int lane = threadIdx.x & 31;
+  Pair<T> r{T(0), T(0), T(0)};
+  int yy = cy;
+  bool row_ok = true;
+  if (neu) yy = min(max(cy, 0), Lc.ny - 1);
+  else row_ok = cy >= 0 && cy < Lc.ny;
+  if (row_ok) {
+    const T *row = E + (long long)yy * Lc.pitch;
+    r.v0 = coarse_at(row, Lc, c0, neu);
+    r.v1 = coarse_at(row, Lc, c0 + 1, neu);
+    if (lane == 0) r.outer = coarse_at(row, Lc, c0 - 1, neu);
+    if (lane == 31) r.outer = coarse_at(row, Lc, c0 + 2, neu);
+  }
+  return r;
+}
+
+// Horizontal interpolation of a coarse pair to the lane's four fine columns.
+template <typename T>
+__device__ __forceinline__ V4<T> coarse_interp(const Pair<T> &c) {
+  const T v0 = c.v0, v1 = c.v1;
+  const int lane = threadIdx.x & 31;
+  T lft = shfl_up1(v1);   // coarse column c0 - 1
+  T rgt = shfl_dn1(v0);   // coarse column c0 + 2
+  if (lane == 0) lft = c.outer;
+  if (lane == 31) rgt = c.outer;
+  V4<T> h;
+  h.v[0] = T(0.75) * v0 + T(0.25) * lft;
+  h.v[1] = T(0.75) * v0 + T(0.25) * v1;
+  h.v[2] = T(0.75) * v1 + T(0.25) * v0;
+  h.v[3] = T(0.75) * v1 + T(0.25) * rgt;
+  return h;
+}
+
+template <typename T, int S1, int S2, bool LEVEL0, bool INT>
+__device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
+                                           const LevelInfo &Lc, const ClassTable<T> &tab, int x0,
+                                           bool out_lane, int y_start, int y_out0, int y_out1,
+                                           unsigned char *smem) {
+  using G = UpGeom<T, S1, S2>;
+  constexpr int U = G::U, O = G::O;
+  const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
+  const bool neu = L.bc == BC_NEU;
+  const bool masked = L.code_off >= 0;
+  const T *B = a.arena + L.b_off;
+  const T *Wp = a.arena + L.w_off;
+  const T *E = a.arena + Lc.u_off;
+  T *Uo = a.arena + L.u_off;
+  const int y_last = y_out1 - 1 + O;
+  V4<T> Bw[U], Uw[U], Ce[3];
+  unsigned Cw[U];
+#pragma unroll
+  for (int k = 0; k < U; ++k) { Bw[k] = zero4<T>(); Uw[k] = zero4<T>(); Cw[k] = 0u; }
+  int ce_top = (y_start >> 1) - 1;  // coarse row held in Ce[0]
+#pragma unroll
+  for (int q = 0; q < 3; ++q) Ce[q] = coarse_interp(coarse_pair(E, Lc, ce_top + q, x0, neu));
+  Pair<T> next0 = coarse_pair(E, Lc, ce_top + 3, x0, neu);
+  Pair<T> next1 = coarse_pair(E, Lc, ce_top + 4, x0, neu);
+  const Ring<T> rb(reinterpret_cast<T *>(smem));
+  const Ring<T> rw(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
+  const CodeRing cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T>()));
+  for (int q = 0; q < kRing - 1; ++q) {
+    rb.issue(q, B, L, y_start + q, x0);
+    rw.issue(q, Wp, L, y_start + q, x0);
+    if (!INT && masked) cring.issue(q, L, a.codes, y_start + q, x0);
+    __pipeline_commit();
+  }
+  double part = 0.0;
+  for (int base = y_start; base <= y_last; base += U) {
+#pragma unroll
+    for (int ph = 0; ph < U; ++ph) {
+      const int y = base + ph;
+      if (y > y_last) break;
+      const int step = y - y_start;
+      __pipeline_wait_prior(kRing - 2);
+      Bw[wslot<U>(ph, 0)] = rb.read(step);
+      V4<T> u = rw.read(step);
+      if (!INT) Cw[wslot<U>(ph, 0)] = masked ? cring.read(step) : row_classes(L, nullptr, y, x0);
+      rb.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
+      rw.issue(step + kRing - 1, Wp, L, y + kRing - 1, x0);
+      if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      __pipeline_commit();
+      {  // prolongation of row y; the coarse window holds rows cy - 1, cy, cy + 1
+        const int cy = y >> 1;
+        if (ce_top + 1 < cy) {
+          Ce[0] = Ce[1];
+          Ce[1] = Ce[2];
+          Ce[2] = coarse_interp(next0);
+          next0 = next1;
+          ++ce_top;
+          next1 = coarse_pair(E, Lc, ce_top + 4, x0, neu);
+        }
+        const unsigned c = Cw[wslot<U>(ph, 0)];
+        const V4<T> &oth = (ph & 1) ? Ce[2] : Ce[0];  // y odd <=> ph odd (y_start even)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          u.v[j] = C.on(c, j) ? u.v[j] + T(0.75) * Ce[1].v[j] + T(0.25) * oth.v[j] : T(0);
+        Uw[wslot<U>(ph, 0)] = u;
+      }
+      // post half sweep g runs on row y - g with colour g & 1, so its first
+      // updated cell is (g + y - g) & 1 = ph & 1 for every g
+#pragma unroll
+      for (int g = 1; g <= 2 * S2; ++g) {
+        if ((ph & 1) == 0)
+          hsweep<0, T, INT>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                            Bw[wslot<U>(ph, g)], Cw[wslot<U>(ph, g)], C);
+        else
+          hsweep<1, T, INT>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                            Bw[wslot<U>(ph, g)], Cw[wslot<U>(ph, g)], C);
+      }
+      const int yo = y - O;
+      if (yo >= y_out0 && yo < y_out1 && out_lane) {
+        V4<T> v = Uw[wslot<U>(ph, O)];
+        const unsigned c = Cw[wslot<U>(ph, O)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v.v[j] = C.on(c, j) ? v.v[j] : T(0);
+        T *dst = Uo + (long long)yo * L.pitch + x0;
+        if (x0 + 3 < L.nx) {
+          st4(dst, v);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (x0 + j < L.nx) dst[j] = v.v[j];
+        }
+        if (LEVEL0) {
+          const V4<T> &bO = Bw[wslot<U>(ph, O)];
+          T acc = T(0);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc += bO.v[j] * v.v[j];
+          part += (double)acc;
+        }
+      }
+    }
+  }
+  __pipeline_wait_prior(0);
+  return part;
+}
+
+template <typename T, int S1, int S2, bool LEVEL0>
+__global__ void __launch_bounds__(kThreads) k_up_s(Args<T> a) {
+  using G = UpGeom<T, S1, S2>;
+  using H = typename G::H;
+  __shared__ ClassTable<T> tab;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const LevelInfo L = a.lv[tl.level];
+    fill_table(tab, L.wall);
+    const LevelInfo Lc = a.lv[L.coarse];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int RB = L.rows_per_warp;
+    const int y_out0 = (tl.ty * kWarps + warp) * RB;
+    if (y_out0 < L.ny) {
+      const int y_out1 = min(y_out0 + RB, L.ny);
+      const int xl = tl.tx * H::OW - 4 * H::HL;
+      const int x0 = xl + 4 * lane;
+      const bool out_lane = lane >= H::HL && lane < kLanes - H::HL && x0 >= 0 && x0 < L.nx;
+      const int y_start = (y_out0 - 2 * S2) & ~1;
+      const int y_last = y_out1 - 1 + G::O;
+      extern __shared__ __align__(16) unsigned char smem[];
+      if (strip_interior(L, y_start, y_last, xl, xl + 127))
+        part = up_strip<T, S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
+                                                 y_out1, smem);
+      else
+        part = up_strip<T, S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
+                                                  y_out1, smem);
+    }
+  }
+  if (!LEVEL0) return;
+  part = block_sum<kThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 3)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < a.ninst; i += nw) {
+    const InstInfo &I = a.inst[i];
+    if (I.up0_end <= I.up0_begin) continue;
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const double rz = warp_range_sum(a.part0, I.up0_begin, I.up0_end);
+    if ((threadIdx.x & 31) == 0) finish_rz(S, rz);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov kernels on level 0: a warp covers 128 columns x kKrylovRows rows and
+// the CTA four such row bands.  The one column outside the warp on each side
+// comes from a scalar load by lanes 0 and 31.
+
+template <typename T>
+__device__ __forceinline__ T edge_value(const T *A, const LevelInfo &L, int y, int x) {
+  return (y >= 0 && y < L.ny && x >= 0 && x < L.nx) ? A[(long long)y * L.pitch + x] : T(0);
+}
+
+template <typename T, bool INT>
+__device__ __forceinline__ double pupdate_rows(const Args<T> &a, const InstInfo &I,
+                                               const LevelInfo &L, const ClassTable<T> &tab,
+                                               int lane, int x0, int y0, int y1, T beta,
+                                               const T *z, const T *p, T *pn,
+                                               unsigned char *smem) {
+  const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
+  const Ring<T> rz(reinterpret_cast<T *>(smem));
+  const Ring<T> rp(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
+  const EdgeRing<T> ez(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4);
+  const EdgeRing<T> ep(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4 + kRing * kThreads);
+  const int xe = lane == 0 ? x0 - 1 : x0 + 4;  // edge column of lanes 0 and 31
+  const bool edge_lane = lane == 0 || lane == 31;
+  auto issue = [&](int q) {
+    const int y = y0 - 1 + q;
+    rz.issue(q, z, L, y, x0);
+    rp.issue(q, p, L, y, x0);
+    if (edge_lane) {
+      ez.issue(q, z, L, y, xe);
+      ep.issue(q, p, L, y, xe);
+    }
+    __pipeline_commit();
+  };
+  for (int q = 0; q < kRing - 1; ++q) issue(q);
+  int step = 0;
+  T edge_next = T(0);
+  auto newp = [&]() {
+    __pipeline_wait_prior(kRing - 2);
+    V4<T> zz = rz.read(step), pp = rp.read(step);
+    edge_next = edge_lane ? ez.read(step) + beta * ep.read(step) : T(0);
+    issue(step + kRing - 1);
+    ++step;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) zz.v[j] += beta * pp.v[j];
+    return zz;
+  };
+  double part = 0.0;
+  V4<T> up = newp(), cu = newp(), dn;
+  T edge_cu = edge_next;
+  const bool full = x0 + 3 < L.nx;
+  for (int y = y0; y < y1; ++y) {
+    dn = newp();
+    T left = shfl_up1(cu.v[3]), right = shfl_dn1(cu.v[0]);
+    if (lane == 0) left = edge_cu;
+    if (lane == 31) right = edge_cu;
+    edge_cu = edge_next;
+    const unsigned c = INT ? 0u : row_classes(L, a.codes, y, x0);
+    const V4<T> ap = arow(cu, up, dn, left, right, c, C);
+    T acc = T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc += cu.v[j] * ap.v[j];
+    part += (double)acc;
+    if (x0 < L.nx) {
+      T *dst = pn + (long long)y * L.pitch + x0;
+      if (full) st4(dst, cu);
+      else
+        for (int j = 0; j < 4 && x0 + j < L.nx; ++j) dst[j] = cu.v[j];
+    }
+    up = cu;
+    cu = dn;
+  }
+  __pipeline_wait_prior(0);
+  return part;
+}
+
+// p_new = z + beta p_old (read from one buffer, written to the other) and p.Ap.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pupdate_s(Args<T> a) {
+  __shared__ ClassTable<T> tab;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    fill_table(tab, L.wall);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
+    const int xl = tl.tx * kKrylovCols;
+    const int x0 = xl + 4 * lane;
+    if (y0 < L.ny) {
+      const int y1 = min(y0 + kKrylovRows, L.ny);
+      const T beta = (T)a.st[tl.inst].beta;
+      const int cur = a.st[tl.inst].pcur;
+      const T *z = a.arena + I.z_off;
+      const T *p = a.arena + p_offset(I, cur);
+      T *pn = a.arena + p_offset(I, cur ^ 1);
+      extern __shared__ __align__(16) unsigned char smem[];
+      if (strip_interior(L, y0, y1 - 1, xl, xl + 127))
+        part = pupdate_rows<T, true>(a, I, L, tab, lane, x0, y0, y1, beta, z, p, pn, smem);
+      else
+        part = pupdate_rows<T, false>(a, I, L, tab, lane, x0, y0, y1, beta, z, p, pn, smem);
+    }
+  }
+  part = block_sum<kThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 0)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kWarps) {
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const InstInfo &I = a.inst[i];
+    const double pAp = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+    if ((threadIdx.x & 31) == 0) {
+      const double alpha = S.rz / pAp;
+      S.pAp = pAp;
+      S.pcur ^= 1;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        S.status = GD_BREAKDOWN;
+        S.flags |= FLAG_RU;
+      } else {
+        S.alpha = alpha;
+      }
+    }
+  }
+}
+
+template <typename T, bool INT>
+__device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInfo &L,
+                                                const ClassTable<T> &tab, int lane, int x0,
+                                                int y0, int y1, T alpha, const T *p, T *d, T *r,
+                                                unsigned char *smem) {
+  const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
+  const Ring<T> rp(reinterpret_cast<T *>(smem));
+  const Ring<T> rd(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
+  const Ring<T> rr(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4);
+  const EdgeRing<T> ep(reinterpret_cast<T *>(smem) + 3 * kRing * kThreads * 4);
+  const int xe = lane == 0 ? x0 - 1 : x0 + 4;  // edge column of lanes 0 and 31
+  const bool edge_lane = lane == 0 || lane == 31;
+  // p streams rows y0 - 1 .. y1; d and r stream the same rows, used one step later
+  auto issue = [&](int q) {
+    const int y = y0 - 1 + q;
+    rp.issue(q, p, L, y, x0);
+    rd.issue(q, d, L, y, x0);
+    rr.issue(q, r, L, y, x0);
+    if (edge_lane) ep.issue(q, p, L, y, xe);
+    __pipeline_commit();
+  };
+  for (int q = 0; q < kRing - 1; ++q) issue(q);
+  int step = 0;
+  V4<T> dcur, rcur, dnext = zero4<T>(), rnext = zero4<T>();
+  T edge_next = T(0);
+  auto next = [&]() {
+    __pipeline_wait_prior(kRing - 2);
+    const V4<T> pp = rp.read(step);
+    dcur = dnext;
+    rcur = rnext;
+    dnext = rd.read(step);
+    rnext = rr.read(step);
+    edge_next = edge_lane ? ep.read(step) : T(0);
+    issue(step + kRing - 1);
+    ++step;
+    return pp;
+  };
+  double part = 0.0;
+  V4<T> up = next(), cu = next(), dn;
+  T edge_cu = edge_next;
+  const bool full = x0 + 3 < L.nx;
+  for (int y = y0; y < y1; ++y) {
+    dn = next();
+    T left = shfl_up1(cu.v[3]), right = shfl_dn1(cu.v[0]);
+    if (lane == 0) left = edge_cu;
+    if (lane == 31) right = edge_cu;
+    edge_cu = edge_next;
+    const unsigned c = INT ? 0u : row_classes(L, a.codes, y, x0);
+    const V4<T> ap = arow(cu, up, dn, left, right, c, C);
+    if (x0 < L.nx) {
+      const long long g = (long long)y * L.pitch + x0;
+      if (full) {
+        V4<T> dd = dcur, rv = rcur;
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dd.v[j] += alpha * cu.v[j];
+          rv.v[j] -= alpha * ap.v[j];
+          acc += rv.v[j] * rv.v[j];
+        }
+        part += (double)acc;
+        st4(d + g, dd);
+        st4(r + g, rv);
+      } else {
+        for (int j = 0; j < 4 && x0 + j < L.nx; ++j) {
+          d[g + j] += alpha * cu.v[j];
+          const T rn = r[g + j] - alpha * ap.v[j];
+          r[g + j] = rn;
+          part += (double)rn * (double)rn;
+        }
+      }
+    }
+    up = cu;
+    cu = dn;
+  }
+  __pipeline_wait_prior(0);
+  return part;
+}
+
+// d += alpha p, r -= alpha A p and r.r; schedules FP64 refreshes.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
+  __shared__ ClassTable<T> tab;
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool active = a.st[tl.inst].status == GD_ACTIVE;
+  double part = 0.0;
+  if (active) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    fill_table(tab, L.wall);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
+    const int xl = tl.tx * kKrylovCols;
+    const int x0 = xl + 4 * lane;
+    if (y0 < L.ny) {
+      const int y1 = min(y0 + kKrylovRows, L.ny);
+      const T alpha = (T)a.st[tl.inst].alpha;
+      const T *p = a.arena + p_offset(I, a.st[tl.inst].pcur);
+      T *d = a.arena + I.d_off;
+      T *r = a.arena + I.r_off;
+      extern __shared__ __align__(16) unsigned char smem[];
+      if (strip_interior(L, y0, y1 - 1, xl, xl + 127))
+        part = cgupdate_rows<T, true>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, smem);
+      else
+        part = cgupdate_rows<T, false>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, smem);
+    }
+  }
+  part = block_sum<kThreads>(part);
+  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  if (!last_block(a.counter + 1)) return;
+  const int warp = threadIdx.x >> 5;
+  for (int i = warp; i < a.ninst; i += kWarps) {
+    InstState &S = a.st[i];
+    if (S.status != GD_ACTIVE) continue;
+    const InstInfo &I = a.inst[i];
+    const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+    if ((threadIdx.x & 31) == 0) {
+      S.rr = rr;
+      S.iters += 1;
+      if (rr <= a.delta2 * S.rr_ref || rr <= a.tol2 * S.ff || S.iters >= a.max_iter ||
+          !isfinite(rr))
+        S.flags |= FLAG_RU;
+    }
+  }
+}
+
+// FP64 residual r = scale (f - fmean) - A x of the refreshed (or, with INIT,
+// the initial) iterate, its norm, and the convergence decision per instance.
+// x and f are the caller's FP64 arrays (row pitch upitch, scalar loads).
+template <typename T, bool INIT>
+__global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
+  double part = 0.0, part_f = 0.0;
+  if (work) {
+    const InstInfo &I = a.inst[tl.inst];
+    const LevelInfo L = a.lv[I.level0];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
+    const int x0 = tl.tx * kKrylovCols + 4 * lane;
+    if (y0 < L.ny) {
+      const int y1 = min(y0 + kKrylovRows, L.ny);
+      Diag<double> D;
+      D.init(L.wall);
+      const double fmean = a.st[tl.inst].fmean;
+      auto xrow = [&](int y) {
+        V4<double> v = zero4<double>();
+        if (y < 0 || y >= L.ny) return v;
+        const unsigned c = row_classes(L, a.codes, y, x0);
+        const double *row = I.x + (long long)y * I.upitch;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (cls(c, j)) v.v[j] = row[x0 + j];
+        return v;
+      };
+      auto xedge = [&](int y, int x) {
+        return cell_class(L, a.codes, y, x) ? I.x[(long long)y * I.upitch + x] : 0.0;
+      };
+      T *r = a.arena + I.r_off;
+      V4<double> up = xrow(y0 - 1), cu = xrow(y0), dn;
+      for (int y = y0; y < y1; ++y) {
+        dn = xrow(y + 1);
+        double left = shfl_up1(cu.v[3]), right = shfl_dn1(cu.v[0]);
+        if (lane == 0) left = xedge(y, x0 - 1);
+        if (lane == 31) right = xedge(y, x0 + 4);
+        const unsigned c = row_classes(L, a.codes, y, x0);
+        const V4<double> ax = apply_row(cu, up, dn, left, right, c, D);
+        if (x0 < L.nx) {
+          const long long g = (long long)y * L.pitch + x0;
+          const long long gu = (long long)y * I.upitch + x0;
+          for (int j = 0; j < 4 && x0 + j < L.nx; ++j) {
+            const bool on = cls(c, j) != 0;
+            const double f = on ? I.scale * (I.f[gu + j] - fmean) : 0.0;
+            const double r64 = on ? f - ax.v[j] : 0.0;
+            r[g + j] = (T)r64;
+            part += r64 * r64;
+            if (INIT) {
+              part_f += f * f;
+              a.arena[I.d_off + g + j] = T(0);
+              a.arena[I.p_off + g + j] = T(0);
+              a.arena[I.q_off + g + j] = T(0);
+              a.arena[I.z_off + g + j] = T(0);
+              if (!on) I.x[gu + j] = 0.0;
+            }
+          }
+        }
+        up = cu;
+        cu = dn;
+      }
+    }
+  }
+  part = block_sum<kThreads>(part);
+  if (INIT) {
+    __syncthreads();
+    part_f = block_sum<kThreads>(part_f);
+  }
+  if (threadIdx.x == 0) {
+    a.part0[blockIdx.x] = part;
+    if (INIT) a.part1[blockIdx.x] = part_f;
+  }
+  if (!last_block(a.counter + 2)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int active = 0;
+  for (int i = warp; i < a.ninst; i += kWarps) {
+    InstState &S = a.st[i];
+    const InstInfo &I = a.inst[i];
+    const bool part_of = INIT || (S.flags & FLAG_RU);
+    if (part_of) {
+      const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
+      double ff = 0.0;
+      if (INIT) ff = warp_range_sum(a.part1, I.fine_begin, I.fine_end);
+      if (lane == 0) {
+        if (INIT) {
+          S.ff = ff;
+          S.iters = 0;
+          S.first = 1;
+          S.rz = 0.0;
+          S.beta = 0.0;
+          S.pcur = 0;
+          S.status = GD_ACTIVE;
+        }
+        // A refresh that barely lowers the true residual (less than 3x), once
+        // it is already below 1e-6 of ||f||, means the FP64 rounding floor is
+        // reached: stop with the current iterate instead of iterating on noise.
+        const bool stalled = !INIT && rr > 0.1 * S.rr_prev && rr <= 1e-12 * S.ff;
+        if (INIT || rr < S.rr_prev) S.rr_prev = rr;
+        S.rr_true = rr;
+        S.rr_ref = rr;
+        S.rr = rr;
+        if (rr <= a.tol2 * S.ff) {
+          S.status = GD_CONVERGED;
+        } else if (!isfinite(rr)) {
+          S.status = GD_BREAKDOWN;
+        } else if (S.status == GD_ACTIVE && stalled) {
+          S.status = GD_STAGNATED;
+        } else if (S.status == GD_ACTIVE && S.iters >= a.max_iter) {
+          S.status = GD_MAX_ITERATIONS;
+        }
+        S.flags = 0;
+      }
+    }
+    if (lane == 0 && S.status == GD_ACTIVE) ++active;
+  }
+  __shared__ int cnt[kWarps];
+  if (lane == 0) cnt[warp] = active;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kWarps; ++w) t += cnt[w];
+    *a.n_active = t;
+  }
+}
+
+}  // namespace st
+}  // namespace gd

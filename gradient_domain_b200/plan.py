@@ -36,12 +36,13 @@ class SolveParams:
     reliable_delta: float = 1e-3  # residual drop between FP64 residual refreshes
     check_every: int = 4          # iterations between host polls of the active count
     use_graph: bool = True
+    strip_target_warps: int = 1200  # smoother strip height: warps wanted per level
 
     def c_params(self) -> _lib.Params:
         return _lib.Params(GD_FP64 if self.precision == "fp64" else GD_MIXED, self.sweeps,
                            self.sweeps, int(self.max_iterations), float(self.tolerance),
                            float(self.reliable_delta), int(self.check_every),
-                           1 if self.use_graph else 0)
+                           1 if self.use_graph else 0, int(self.strip_target_warps), 0)
 
 
 @dataclass(frozen=True)

@@ -51,7 +51,9 @@ enum gd_status {
   GD_CONVERGED = 0,
   GD_MAX_ITERATIONS = 1,
   GD_BREAKDOWN = 2,  /* p.Ap <= 0 or a non-finite scalar */
-  GD_ACTIVE = 3      /* internal: still iterating */
+  GD_ACTIVE = 3,     /* internal: still iterating */
+  GD_STAGNATED = 4   /* the FP64 residual stopped decreasing above the tolerance
+                        (the tolerance is below the attainable accuracy) */
 };
 
 typedef struct gd_grid_desc {
@@ -70,6 +72,8 @@ typedef struct gd_params {
   double reliable_delta;  /* mixed precision: residual drop between FP64 refreshes */
   int32_t check_every;    /* iterations between host-side convergence polls        */
   int32_t use_graph;      /* capture one iteration as a CUDA graph and replay it    */
+  int32_t strip_target_warps; /* smoother strips: warps wanted per level (0 = 1200) */
+  int32_t reserved;
 } gd_params;
 
 typedef struct gd_report {
