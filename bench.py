@@ -41,8 +41,8 @@ FALLBACK_HBM_GBS = 6650.0
 # mixed plan; the FP64 plan doubles the FP32 terms).  Level kernels count the
 # cells of the level they work on; coarse arrays are a quarter of that.
 BYTES_PER_CELL_MIXED = {
-    "down0": 4 + 1, "down": 4 + 1,          # read b, write coarse b
-    "up0": 4 + 1 + 4, "up": 4 + 1 + 4,      # read b and coarse e, write u
+    "down0": 4 + 4 + 1, "down": 4 + 4 + 1,          # read b; write pre-smoothed w, coarse b
+    "up0": 4 + 4 + 1 + 4, "up": 4 + 4 + 1 + 4,      # read b, w, coarse e; write u
     "pupdate": 4 + 4 + 4,                   # read z, p; write p
     "cgupdate": 12 + 8,                     # read p, d, r; write d, r
     "resid": 8 + 8 + 4,                     # read x, f; write r (refresh iterations)
@@ -56,7 +56,7 @@ def bytes_per_cell(kind: str, fp64: bool) -> float:
     b = BYTES_PER_CELL_MIXED.get(kind, 0.0)
     if not fp64:
         return b
-    fp32_part = {"down0": 5, "down": 5, "up0": 9, "up": 9, "pupdate": 12, "cgupdate": 20,
+    fp32_part = {"down0": 9, "down": 9, "up0": 13, "up": 13, "pupdate": 12, "cgupdate": 20,
                  "resid": 4, "fold": 8, "init": 16, "mean": 0}.get(kind, 0)
     return b + fp32_part
 
@@ -202,7 +202,7 @@ def ours(args) -> None:
     x = torch.zeros_like(f)
     insts = [Instance(size, size, "neumann", zero_mean=True) for _ in range(n_ch)]
     plan = PoissonPlan(insts, SolveParams(precision="mixed", tolerance=args.tol,
-                                          sweeps=args.sweeps))
+                                          sweeps=args.sweeps, reliable_delta=args.delta))
     stream = torch.cuda.current_stream()
 
     def step(p):
@@ -323,7 +323,7 @@ def ours(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32/fp64-mixed", "data": "synthetic",
         "config": {"workload": f"tonemap-neumann {size}x{size}x{n_ch}", "tolerance": args.tol,
-                   "sweeps": args.sweeps, "instances_per_gpu": n_ch,
+                   "sweeps": args.sweeps, "reliable_delta": args.delta, "instances_per_gpu": n_ch,
                    "l2": "inputs larger than L2 (3 x 134 MB rhs + solution + hierarchy)",
                    "parallelism": f"replicas x{world}"},
         "clocks": clock,
@@ -352,6 +352,167 @@ def ours(args) -> None:
         dist.destroy_process_group()
 
 
+def _timed_steps(step, steps, warmup, world, dev):
+    """Warm up, then device-time exactly `steps` calls of step() (max over ranks)."""
+    import torch
+    import torch.distributed as dist
+    for _ in range(warmup):
+        out = step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, out
+
+
+def composite(args) -> None:
+    """Masked seamless compositing, 2048 x 2048 x 3, star-polygon selection, tolerance 1e-8."""
+    import torch
+    import torch.distributed as dist
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    import gradient_domain_b200 as gd
+    from gradient_domain_b200 import workloads
+    from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
+    dev = torch.device("cuda", local)
+    size = args.size if args.size != 4096 else 2048
+    src, tgt, mask = workloads.composite_case(size, seed=2 + rank)
+    f_np, unk_np, win = workloads.masked_system(src, tgt, mask)
+    n_ch, hb, wb = f_np.shape
+    unknowns = int(unk_np.sum())
+    f = torch.as_tensor(f_np).to(dev)
+    x = torch.zeros_like(f)
+    unk = torch.as_tensor(unk_np.astype(np.uint8)).to(dev)
+    plan = PoissonPlan([Instance(hb, wb, "masked") for _ in range(n_ch)],
+                       SolveParams(tolerance=args.tol, sweeps=args.sweeps,
+                                   reliable_delta=args.delta))
+
+    def step():
+        for k in range(n_ch):
+            plan.set_mask(k, unk)
+        plan.prepare()
+        x.zero_()
+        return plan.solve(list(f), list(x), scale=1.0)
+
+    plan.set_profiling(True)
+    ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
+    kt = plan.kernel_times()
+    plan.set_profiling(False)
+    value = unknowns * n_ch * world / (ms / 1e3) / 1e6
+    # end to end: the public seamless_clone from host arrays (field, RHS and copies included)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.steps // 2)
+    for _ in range(e2e_steps):
+        out, reps = gd.seamless_clone(src, tgt, mask, (0, 0), domain="mask", tolerance=args.tol)
+    e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32/fp64-mixed", "data": "synthetic",
+        "config": {"workload": f"composite-masked {size}x{size}x{n_ch}", "unknowns": unknowns,
+                   "grid": [hb, wb], "tolerance": args.tol, "sweeps": args.sweeps,
+                   "unit_note": "Mpix/s counts unknown pixels x channels"},
+        "iterations": [r.iterations for r in res],
+        "relative_residual": max(r.relative_residual for r in res),
+        "converged": all(r.converged for r in res),
+        "e2e": {"value": unknowns * n_ch / (e2e_ms / 1e3) / 1e6, "unit": "Mpix/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(src.nbytes + tgt.nbytes + mask.nbytes),
+                "d2h_bytes_per_step": int(tgt.nbytes)},
+        "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in kt.items() if v["launches"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import poisson as op
+        # CPU baseline and oracle: the reference's SuperLU masked solve on one channel
+        field, placed, target = op.clone_field(src[..., :1], tgt[..., :1], mask, (0, 0), "import")
+        t0 = time.perf_counter()
+        ref, _ = op.solve_masked(field, target[..., 0], placed)
+        dt = time.perf_counter() - t0
+        got = out[..., 0]
+        inner = np.zeros_like(mask)
+        inner[1:-1, 1:-1] = mask[1:-1, 1:-1]
+        err = float(np.linalg.norm(got[inner] - ref[inner]) / np.linalg.norm(ref[inner]))
+        line["rel_l2_err_vs_splu_oracle_channel0"] = err
+        line["cpu_baseline"] = {"value": unknowns / dt / 1e6, "unit": "Mpix/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"1 channel, SuperLU factorisation + solve of "
+                                          f"{unknowns} unknowns (restated solve_masked), {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def batch(args) -> None:
+    """256 uneven images (1 or 3 channels; Neumann blobs or masked polygons) in one plan."""
+    import torch
+    import torch.distributed as dist
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from gradient_domain_b200 import workloads
+    from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
+    dev = torch.device("cuda", local)
+    items = workloads.batch_instances(args.count, seed=3 + rank)
+    insts, fs, xs, masks = [], [], [], []
+    for it in items:
+        c, h, w = it["f"].shape
+        for k in range(c):
+            insts.append(Instance(h, w, it["boundary"], it["boundary"] == "neumann"))
+            fs.append(torch.as_tensor(np.ascontiguousarray(it["f"][k])).to(dev))
+            masks.append(torch.as_tensor(it["unknown"].astype(np.uint8)).to(dev)
+                         if it["boundary"] == "masked" else None)
+    xs = [torch.zeros_like(t) for t in fs]
+    cells = sum(t.numel() for t in fs)
+    plan = PoissonPlan(insts, SolveParams(tolerance=args.tol, sweeps=args.sweeps,
+                                          reliable_delta=args.delta))
+    for k, m in enumerate(masks):
+        if m is not None:
+            plan.set_mask(k, m)
+    plan.prepare()
+
+    def step():
+        for t in xs:
+            t.zero_()
+        return plan.solve(fs, xs, scale=1.0)
+
+    ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
+    value = cells * world / (ms / 1e3) / 1e6
+    its = [r.iterations for r in res]
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32/fp64-mixed", "data": "synthetic",
+        "config": {"workload": f"batch {args.count} images / {len(insts)} instances, "
+                               f"sides 64-2048, neumann + masked", "cells": cells,
+                   "tolerance": args.tol, "graph": True},
+        "iterations": {"min": min(its), "max": max(its), "mean": float(np.mean(its))},
+        "converged": sum(r.converged for r in res), "instances": len(res),
+        "max_relative_residual": max(r.relative_residual for r in res),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,14 +522,32 @@ def main():
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--sweeps", type=int, default=2)
+    ap.add_argument("--delta", type=float, default=1e-3,
+                    help="residual drop between FP64 refreshes (mixed precision)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the oracle and CPU baseline")
     ap.add_argument("--channels", type=int, default=3)
     ap.add_argument("--solve-only", action="store_true",
                     help="only the mixed-precision solves (small profiling runs): no FP64 plan, "
                          "no end-to-end leg, no oracle")
+    ap.add_argument("--config", choices=["tonemap", "composite", "batch", "serve"],
+                    default="tonemap", help="workload (default: the headline tone-mapping case)")
+    ap.add_argument("--count", type=int, default=256, help="images in the batch workload")
+    ap.add_argument("--rates", type=float, nargs="+", default=[200.0, 1000.0, 5000.0],
+                    help="serving: offered loads in requests per second")
+    ap.add_argument("--requests", type=int, default=2000, help="serving: requests per load")
+    ap.add_argument("--requests-1mp", type=int, default=400,
+                    help="serving: 1 MP requests for the latency target")
+    ap.add_argument("--pool", type=int, default=12, help="serving: distinct requests per type")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.config == "composite":
+        composite(args)
+    elif args.config == "batch":
+        batch(args)
+    elif args.config == "serve":
+        from gradient_domain_b200 import serving
+        serving.bench_main(args)
     else:
         ours(args)
 

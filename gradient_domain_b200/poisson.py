@@ -191,11 +191,15 @@ def _place(source, mask, target_shape, offset):
 
 
 def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
-                   domain: str = "mask", method: str = "mgcg", margin: int = 24):
+                   domain: str = "mask", method: str = "mgcg", margin: int = 24,
+                   tolerance: float | None = None):
     """Paste ``source[mask]`` into ``target`` at ``offset`` without a visible seam.
 
-    Raises ``ValueError`` for an unknown ``mode`` or ``domain``, or a patch that
-    does not fit (poisson.py:310-335).
+    ``tolerance`` (an addition) overrides the solver's relative residual: the
+    masked domain otherwise runs at the direct-solver level 1e-12 and the
+    rectangle at 1e-8, as in the reference.  Raises ``ValueError`` for an
+    unknown ``mode`` or ``domain``, or a patch that does not fit
+    (poisson.py:310-335).
     """
     target = np.asarray(target, dtype=float)
     source = np.asarray(source, dtype=float)
@@ -215,7 +219,9 @@ def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
         raise ValueError(f"unknown mode {mode!r}")
     field = inside.select(placed_mask, target_field)
     if domain == "mask":
-        return solve_masked(field, target, placed_mask)
+        if tolerance is None:
+            return solve_masked(field, target, placed_mask)
+        return solve_masked(field, target, placed_mask, tolerance=tolerance)
     if domain != "rectangle":
         raise ValueError(f"unknown domain {domain!r}")
     rows, columns = np.nonzero(placed_mask)
@@ -225,7 +231,8 @@ def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
     right = min(int(columns.max()) + margin + 1, target.shape[1])
     window = (slice(top, bottom), slice(left, right))
     patch, reports = solve_dirichlet(GuidanceField(field.gx[window], field.gy[window]),
-                                     target[window], method=method)
+                                     target[window], method=method,
+                                     tolerance=1e-8 if tolerance is None else tolerance)
     result = target.copy()
     result[window] = patch
     return result, reports

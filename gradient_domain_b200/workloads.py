@@ -115,3 +115,90 @@ def composite_case(size=2048, seed=2):
     source, target = image(), image()
     mask = star_polygon_mask(size, rng, rmin=300 * scale, rmax=800 * scale)
     return source, target, mask
+
+
+def masked_system(source, target, mask):
+    """Masked Poisson system of seamless cloning in "import" mode at offset (0, 0).
+
+    Returns (f, unknown, window): per-channel right-hand sides of the reference
+    sign convention A x = f (A positive) on the bounding box of the unknowns
+    plus a one-pixel ring, the unknown mask on that box, and the box slices.
+    The system is the one poisson.py:154-244 assembles for
+    seamless_clone(source, target, mask, (0, 0), mode="import", domain="mask").
+    """
+    inner = np.zeros(mask.shape, dtype=bool)
+    inner[1:-1, 1:-1] = mask[1:-1, 1:-1]
+    rows = np.nonzero(inner.any(axis=1))[0]
+    cols = np.nonzero(inner.any(axis=0))[0]
+    win = (slice(rows[0] - 1, rows[-1] + 2), slice(cols[0] - 1, cols[-1] + 2))
+    unk = inner[win]
+    f = []
+    for c in range(target.shape[2]):
+        sgx, sgy = forward_gradient(source[..., c])
+        tgx, tgy = forward_gradient(target[..., c])
+        gx = np.where(mask, sgx, tgx)[win]
+        gy = np.where(mask, sgy, tgy)[win]
+        div = divergence(gx, gy)
+        img = target[..., c][win]
+        b = div.copy()
+        # subtract known neighbour values (the order of poisson.py:218-224)
+        for dy, dx in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+            nb_unk = np.roll(np.roll(unk, -dy, axis=0), -dx, axis=1)
+            nb_val = np.roll(np.roll(img, -dy, axis=0), -dx, axis=1)
+            b = np.where(unk & ~nb_unk, b - nb_val, b)
+        f.append(np.where(unk, -b, 0.0))
+    return np.stack(f), unk, win
+
+
+def batch_instances(count=256, seed=3, side=(64, 2048)):
+    """The uneven batch: `count` images of 1 or 3 channels (p = 0.5).
+
+    Sides are log-uniform in [64, 2048], the aspect ratio uniform in [0.5, 2],
+    both sides rounded to multiples of 8.  Even-numbered images are Neumann
+    integrations of a blob gradient field, odd ones Dirichlet problems on a
+    star-polygon mask.  Returns a list of dicts with keys boundary, f (c, h, w)
+    and, for masks, unknown (h, w).
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        s = float(np.exp(rng.uniform(np.log(side[0]), np.log(side[1]))))
+        aspect = rng.uniform(0.5, 2.0)
+        h = max(8, int(round(s * np.sqrt(aspect) / 8.0)) * 8)
+        w = max(8, int(round(s / np.sqrt(aspect) / 8.0)) * 8)
+        ch = 1 if rng.random() < 0.5 else 3
+        if k % 2 == 0:
+            f = np.stack([-neumann_blobs_shape((h, w), rng) for _ in range(ch)])
+            out.append({"boundary": "neumann", "f": f})
+        else:
+            m = min(h, w)
+            mask = star_polygon_mask_shape((h, w), rng, rmin=0.15 * m, rmax=0.45 * m)
+            unk = np.zeros_like(mask)
+            unk[1:-1, 1:-1] = mask[1:-1, 1:-1]
+            f = np.stack([np.where(unk, rng.standard_normal((h, w)), 0.0) for _ in range(ch)])
+            out.append({"boundary": "masked", "f": f, "unknown": unk})
+    return out
+
+
+def neumann_blobs_shape(shape, rng):
+    src = blob_image(shape, 32, rng, sigma=(0.01 * min(shape), 0.12 * min(shape)))
+    return divergence(*forward_gradient(src))
+
+
+def star_polygon_mask_shape(shape, rng, vertices=12, rmin=10.0, rmax=40.0):
+    """Star polygon centred in an (h, w) canvas, rasterised at pixel centres."""
+    h, w = shape
+    ang = 2 * np.pi * np.arange(vertices) / vertices + rng.uniform(-0.2, 0.2, vertices)
+    rad = rng.uniform(rmin, rmax, vertices)
+    vy, vx = h / 2.0 + rad * np.sin(ang), w / 2.0 + rad * np.cos(ang)
+    yy = np.arange(h)[:, None] + 0.5
+    xx = np.arange(w)[None, :] + 0.5
+    inside = np.zeros((h, w), dtype=bool)
+    j = vertices - 1
+    for i in range(vertices):
+        crosses = (vy[i] > yy) != (vy[j] > yy)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            xint = (vx[j] - vx[i]) * (yy - vy[i]) / (vy[j] - vy[i]) + vx[i]
+        inside ^= crosses & (xx < xint)
+        j = i
+    return inside
