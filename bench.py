@@ -311,6 +311,8 @@ def ours(args) -> None:
     if os.path.exists(tpath):
         with open(tpath) as fh:
             tpc = json.load(fh).get(dom)
+        if not isinstance(tpc, (int, float)):
+            tpc = None
         if tpc:
             traffic = tpc * per_launch_cells
     total_ms = sum(v["ms"] for v in kinds.values())
