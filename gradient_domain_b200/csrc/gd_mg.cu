@@ -465,7 +465,7 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   p->n = n;
   p->prm = *params;
   if (p->prm.check_every <= 0) p->prm.check_every = 4;
-  if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-3;
+  if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-4;
   p->fp64 = params->precision == GD_FP64;
   p->mask_set.assign(n, 0);
   build_plan(p, grids);

@@ -287,19 +287,27 @@ __global__ void __launch_bounds__(kBThreads) k_bottom(Args<T> a) {
 // Elementwise level-0 kernels over 64 x 128 tiles (the Krylov kernels with
 // halos are in gd_stream.cuh).
 
-// x += d, d = 0 for instances with a pending FP64 refresh.
+// x += d, d = 0 for instances with a pending FP64 refresh.  A thread owns one
+// column of the 64 x 128 tile, so every warp access is 32 consecutive
+// elements; the independent rows are unrolled for several loads in flight.
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   if (!(a.st[tl.inst].flags & FLAG_RU)) return;
-  const InstInfo &I = a.inst[tl.inst];
-  T *d = a.arena + I.d_off;
-  const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
-  for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-    const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
-    if (gy >= I.ny || gx >= I.nx) continue;
-    const long long g = (long long)gy * I.pitch + gx;
-    I.x[(long long)gy * I.upitch + gx] += (double)d[g];
+  // descriptor fields in registers: the stores below could alias the descriptor
+  const InstInfo &Ig = a.inst[tl.inst];
+  const int ny = Ig.ny, nx = Ig.nx, pitch = Ig.pitch;
+  const long long upitch = Ig.upitch;
+  double *const X = Ig.x;
+  T *const d = a.arena + Ig.d_off;
+  const int x = tl.tx * kFTX + threadIdx.x;
+  const int y0 = tl.ty * kFTY;
+  if (x >= nx) return;
+  const int y1 = min(y0 + kFTY, ny);
+#pragma unroll 8
+  for (int y = y0; y < y1; ++y) {
+    const long long g = (long long)y * pitch + x;
+    X[(long long)y * upitch + x] += (double)d[g];
     d[g] = T(0);
   }
 }
@@ -358,13 +366,16 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
-  const InstInfo &I = a.inst[tl.inst];
-  if (!I.zero_mean) return;
+  const InstInfo &Ig = a.inst[tl.inst];
+  if (!Ig.zero_mean) return;
+  const int ny = Ig.ny, nx = Ig.nx;
+  const long long upitch = Ig.upitch;
+  double *const X = Ig.x;
   const double m = a.st[tl.inst].mean;
   const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
   for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
     const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
-    if (gy < I.ny && gx < I.nx) I.x[(long long)gy * I.upitch + gx] -= m;
+    if (gy < ny && gx < nx) X[(long long)gy * upitch + gx] -= m;
   }
 }
 

@@ -254,6 +254,7 @@ template <typename T>
 constexpr size_t level_smem() { return 2 * ring_bytes<T>() + (size_t)kRing * kThreads * 4; }
 template <typename T>
 constexpr size_t edge_bytes() { return (size_t)kRing * kThreads * sizeof(T); }
+
 template <typename T>
 constexpr size_t pupdate_smem() { return 2 * ring_bytes<T>() + 2 * edge_bytes<T>(); }
 template <typename T>
@@ -768,27 +769,36 @@ __device__ __forceinline__ double pupdate_rows(const Args<T> &a, const InstInfo 
   const EdgeRing<T> ep(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4 + kRing * kThreads);
   const int xe = lane == 0 ? x0 - 1 : x0 + 4;  // edge column of lanes 0 and 31
   const bool edge_lane = lane == 0 || lane == 31;
+  const bool read_p = beta != T(0);
   auto issue = [&](int q) {
     const int y = y0 - 1 + q;
     rz.issue(q, z, L, y, x0);
-    rp.issue(q, p, L, y, x0);
+    if (read_p) rp.issue(q, p, L, y, x0);
     if (edge_lane) {
       ez.issue(q, z, L, y, xe);
-      ep.issue(q, p, L, y, xe);
+      if (read_p) ep.issue(q, p, L, y, xe);
     }
     __pipeline_commit();
   };
   for (int q = 0; q < kRing - 1; ++q) issue(q);
   int step = 0;
   T edge_next = T(0);
+  // The first direction is p = z: with beta == 0 the old buffer is not read
+  // (it need not be initialised), so the rings for p are left idle.
+  const bool use_p = beta != T(0);
   auto newp = [&]() {
     __pipeline_wait_prior(kRing - 2);
-    V4<T> zz = rz.read(step), pp = rp.read(step);
-    edge_next = edge_lane ? ez.read(step) + beta * ep.read(step) : T(0);
+    V4<T> zz = rz.read(step);
+    T e = edge_lane ? ez.read(step) : T(0);
+    if (use_p) {
+      const V4<T> pp = rp.read(step);
+      if (edge_lane) e += beta * ep.read(step);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) zz.v[j] += beta * pp.v[j];
+    }
+    edge_next = e;
     issue(step + kRing - 1);
     ++step;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) zz.v[j] += beta * pp.v[j];
     return zz;
   };
   double part = 0.0;
@@ -1000,67 +1010,66 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
 
 // FP64 residual r = scale (f - fmean) - A x of the refreshed (or, with INIT,
 // the initial) iterate, its norm, and the convergence decision per instance.
-// x and f are the caller's FP64 arrays (row pitch upitch, scalar loads).
+// x and f are the caller's FP64 arrays (any row pitch).  A thread owns one
+// column of the 64 x 128 tile and walks its rows with x rows y - 1, y, y + 1 in
+// registers; horizontal neighbours come from shuffles, and lanes 0 and 31 load
+// the column just outside their warp.  Every warp access is 32 consecutive
+// elements.
 template <typename T, bool INIT>
 __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
   double part = 0.0, part_f = 0.0;
   if (work) {
-    const InstInfo &I = a.inst[tl.inst];
-    const LevelInfo L = a.lv[I.level0];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
-    const int x0 = tl.tx * kKrylovCols + 4 * lane;
-    if (y0 < L.ny) {
-      const int y1 = min(y0 + kKrylovRows, L.ny);
-      Diag<double> D;
-      D.init(L.wall);
-      const double fmean = a.st[tl.inst].fmean;
-      auto xrow = [&](int y) {
-        V4<double> v = zero4<double>();
-        if (y < 0 || y >= L.ny) return v;
-        const unsigned c = row_classes(L, a.codes, y, x0);
-        const double *row = I.x + (long long)y * I.upitch;
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (cls(c, j)) v.v[j] = row[x0 + j];
-        return v;
-      };
-      auto xedge = [&](int y, int x) {
-        return cell_class(L, a.codes, y, x) ? I.x[(long long)y * I.upitch + x] : 0.0;
-      };
-      T *r = a.arena + I.r_off;
-      V4<double> up = xrow(y0 - 1), cu = xrow(y0), dn;
-      for (int y = y0; y < y1; ++y) {
-        dn = xrow(y + 1);
-        double left = shfl_up1(cu.v[3]), right = shfl_dn1(cu.v[0]);
-        if (lane == 0) left = xedge(y, x0 - 1);
-        if (lane == 31) right = xedge(y, x0 + 4);
-        const unsigned c = row_classes(L, a.codes, y, x0);
-        const V4<double> ax = apply_row(cu, up, dn, left, right, c, D);
-        if (x0 < L.nx) {
-          const long long g = (long long)y * L.pitch + x0;
-          const long long gu = (long long)y * I.upitch + x0;
-          for (int j = 0; j < 4 && x0 + j < L.nx; ++j) {
-            const bool on = cls(c, j) != 0;
-            const double f = on ? I.scale * (I.f[gu + j] - fmean) : 0.0;
-            const double r64 = on ? f - ax.v[j] : 0.0;
-            r[g + j] = (T)r64;
-            part += r64 * r64;
-            if (INIT) {
-              part_f += f * f;
-              a.arena[I.d_off + g + j] = T(0);
-              a.arena[I.p_off + g + j] = T(0);
-              a.arena[I.q_off + g + j] = T(0);
-              a.arena[I.z_off + g + j] = T(0);
-              if (!on) I.x[gu + j] = 0.0;
-            }
-          }
-        }
-        up = cu;
-        cu = dn;
+    // descriptor fields in registers: the stores below could alias the descriptor
+    const InstInfo &Ig = a.inst[tl.inst];
+    double *const X = Ig.x;
+    const double *const Fu = Ig.f;
+    const long long upitch = Ig.upitch;
+    const double scale = Ig.scale;
+    T *const r = a.arena + Ig.r_off;
+    T *const dz = a.arena + Ig.d_off;
+    const LevelInfo L = a.lv[Ig.level0];
+    const int lane = threadIdx.x & 31;
+    const int col = tl.tx * kFTX + threadIdx.x;
+    const int y0 = tl.ty * kFTY;
+    const int y1 = min(y0 + kFTY, L.ny);
+    const bool masked = L.code_off >= 0;
+    const bool in_col = col < L.nx;
+    const double fmean = a.st[tl.inst].fmean;
+    const double omw = 1.0 - (double)L.wall;
+    auto klass = [&](int y, int x) -> int {
+      if (y < 0 || y >= L.ny || x < 0 || x >= L.nx) return 0;
+      if (masked) return a.codes[L.code_off + (long long)y * L.pitch + x];
+      return rect_class(y, x, L.ny, L.nx);
+    };
+    // x at (y, x) where the cell has an unknown, else zero
+    auto xv = [&](int y, int x) -> double {
+      return klass(y, x) ? X[(long long)y * upitch + x] : 0.0;
+    };
+    double xu = xv(y0 - 1, col), xc = xv(y0, col);
+#pragma unroll 4
+    for (int y = y0; y < y1; ++y) {
+      const double xd = xv(y + 1, col);
+      double left = shfl_up1(xc), right = shfl_dn1(xc);
+      if (lane == 0) left = xv(y, col - 1);
+      if (lane == 31) right = xv(y, col + 1);
+      const int c = in_col ? klass(y, col) : 0;
+      if (c) {
+        const long long gu = (long long)y * upitch + col;
+        const double dg = 4.0 - (double)(c - 1) * omw;
+        const double f = scale * (Fu[gu] - fmean);
+        const double r64 = f - (dg * xc - (xu + xd + left + right));
+        r[(long long)y * L.pitch + col] = (T)r64;
+        part += r64 * r64;
+        if (INIT) part_f += f * f;
+      } else if (in_col && y < L.ny) {
+        r[(long long)y * L.pitch + col] = T(0);
+        if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
       }
+      if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
+      xu = xc;
+      xc = xd;
     }
   }
   part = block_sum<kThreads>(part);

@@ -33,7 +33,7 @@ class SolveParams:
     sweeps: int = 2               # RB-GS sweeps before and after each coarse correction
     max_iterations: int = 2000
     tolerance: float = 1e-8
-    reliable_delta: float = 1e-3  # residual drop between FP64 residual refreshes
+    reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
     check_every: int = 4          # iterations between host polls of the active count
     use_graph: bool = True
     strip_target_warps: int = 1200  # smoother strip height: warps wanted per level
