@@ -39,8 +39,8 @@ class FakeBackend:
                 raise RuntimeError("injected backend failure")
             out = []
             for r in requests:
-                ok = np.isfinite(r.f).all()
-                out.append((r.f.copy(), [1] * len(r.f), ["converged" if ok else "breakdown"]
+                ok = np.isfinite(np.asarray(r.f)).all()
+                out.append((np.array(r.f), [1] * len(r.f), ["converged" if ok else "breakdown"]
                             * len(r.f), [0.0] * len(r.f)))
             return out
         finally:
