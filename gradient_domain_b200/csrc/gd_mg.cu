@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "gd_stream.cuh"
@@ -42,8 +44,11 @@ struct gd_plan_s {
   std::vector<char> mask_set;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t cap = nullptr;
+  int cap_device = -1;
+  long long solves = 0;  // completed solves; the graph is captured from the second on
   int *h_nact = nullptr;
   InstState *h_st = nullptr;
+  size_t h_st_bytes = 0;
   // profiling: events around every launch (graphs are bypassed while enabled)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -61,6 +66,67 @@ namespace {
 
 constexpr int kPitchAlign = 4;       // elements; rows start on 16-byte boundaries for FP32
 constexpr size_t kArrayAlign = 256;  // bytes
+
+// Process-wide recycling of the small pinned host blocks and capture streams
+// that every plan needs.  Allocating and freeing page-locked memory
+// synchronises the whole device, which would stall every other stream each
+// time a served request brings a new plan shape; recycled blocks cost nothing.
+struct HostPools {
+  std::mutex mu;
+  std::multimap<size_t, void *> pinned;         // size class -> free block
+  std::multimap<int, cudaStream_t> streams;     // device -> free capture stream
+};
+
+HostPools &pools() {
+  static HostPools *h = new HostPools();  // never destroyed: used until process exit
+  return *h;
+}
+
+size_t pinned_class(size_t bytes) {
+  size_t c = 256;
+  while (c < bytes) c <<= 1;
+  return c;
+}
+
+void *pinned_get(size_t bytes) {
+  const size_t c = pinned_class(bytes);
+  {
+    std::lock_guard<std::mutex> g(pools().mu);
+    auto it = pools().pinned.find(c);
+    if (it != pools().pinned.end()) {
+      void *b = it->second;
+      pools().pinned.erase(it);
+      return b;
+    }
+  }
+  void *b = nullptr;
+  return cudaMallocHost(&b, c) == cudaSuccess ? b : nullptr;
+}
+
+void pinned_put(void *b, size_t bytes) {
+  if (!b) return;
+  std::lock_guard<std::mutex> g(pools().mu);
+  pools().pinned.emplace(pinned_class(bytes), b);
+}
+
+cudaError_t capture_stream_get(int device, cudaStream_t *out) {
+  {
+    std::lock_guard<std::mutex> g(pools().mu);
+    auto it = pools().streams.find(device);
+    if (it != pools().streams.end()) {
+      *out = it->second;
+      pools().streams.erase(it);
+      return cudaSuccess;
+    }
+  }
+  return cudaStreamCreateWithFlags(out, cudaStreamNonBlocking);
+}
+
+void capture_stream_put(int device, cudaStream_t s) {
+  if (!s) return;
+  std::lock_guard<std::mutex> g(pools().mu);
+  pools().streams.emplace(device, s);
+}
 
 // Record an event before a launch of `kind` covering `cells` grid cells.
 void prof_begin(gd_plan p, int kind, double cells, cudaStream_t st) {
@@ -471,8 +537,10 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   build_plan(p, grids);
   if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);
   else Runner<float>::dispatch_attrs(p->prm.pre_sweeps);
-  if (cudaMallocHost(&p->h_nact, sizeof(int)) != cudaSuccess ||
-      cudaMallocHost(&p->h_st, sizeof(InstState) * n) != cudaSuccess) {
+  p->h_st_bytes = sizeof(InstState) * n;
+  p->h_nact = static_cast<int *>(pinned_get(sizeof(int)));
+  p->h_st = static_cast<InstState *>(pinned_get(p->h_st_bytes));
+  if (!p->h_nact || !p->h_st) {
     set_error("gd_plan_create: pinned host allocation failed");
     gd_plan_destroy(p);
     return GD_ERR_CUDA;
@@ -490,9 +558,9 @@ extern "C" void gd_plan_destroy(gd_plan p) {
   if (!p) return;
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
-  if (p->cap) cudaStreamDestroy(p->cap);
-  if (p->h_nact) cudaFreeHost(p->h_nact);
-  if (p->h_st) cudaFreeHost(p->h_st);
+  capture_stream_put(p->cap_device, p->cap);
+  pinned_put(p->h_nact, sizeof(int));
+  pinned_put(p->h_st, p->h_st_bytes);
   delete p;
 }
 
@@ -515,9 +583,9 @@ extern "C" int gd_plan_bind(gd_plan p, void *ws, size_t bytes, cudaStream_t st) 
                                 cudaMemcpyHostToDevice, st));
   GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->inst.data(),
                                 p->inst.size() * sizeof(InstInfo), cudaMemcpyHostToDevice, st));
+  // pageable sources are staged before cudaMemcpyAsync returns: no sync needed
   GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_tiles, p->tiles.data(),
                                 p->tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, st));
-  GD_CHECK_CUDA(cudaStreamSynchronize(st));
   return GD_OK;
 }
 
@@ -574,9 +642,15 @@ int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
   GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
                                 cudaMemcpyDeviceToHost, st));
   GD_CHECK_CUDA(cudaStreamSynchronize(st));
-  const bool graph = p->prm.use_graph && !p->profiling;
+  // A plan solved once runs on direct launches; from its second solve on the
+  // iteration is one graph launch (capture and instantiation cost more than
+  // the launches they save in a single solve).
+  const bool graph = p->prm.use_graph && !p->profiling && p->solves >= 1;
   if (graph && !p->gexec) {
-    if (!p->cap) GD_CHECK_CUDA(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking));
+    if (!p->cap) {
+      GD_CHECK_CUDA(cudaGetDevice(&p->cap_device));
+      GD_CHECK_CUDA(capture_stream_get(p->cap_device, &p->cap));
+    }
     cudaGraph_t g = nullptr;
     GD_CHECK_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
     Runner<T>::dispatch_iteration(p, a, p->cap);
@@ -613,6 +687,7 @@ int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
                                 cudaMemcpyDeviceToHost, st));
   GD_CHECK_CUDA(cudaStreamSynchronize(st));
   prof_collect(p);
+  ++p->solves;
   for (int i = 0; i < p->n; ++i) {
     const InstState &S = p->h_st[i];
     gd_report &R = reports[i];

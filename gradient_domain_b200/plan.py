@@ -87,6 +87,7 @@ class PoissonPlan:
         self._handle = handle
         nbytes = int(lib.gd_plan_workspace_bytes(handle))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        self._stream_obj = stream if stream is not None else torch.cuda.current_stream(self.device)
         self._stream = _lib.stream_handle(stream)
         _lib.check(lib.gd_plan_bind(handle, _lib.ptr(self.workspace), nbytes, self._stream),
                    "gd_plan_bind")
@@ -177,7 +178,8 @@ class PoissonPlan:
 
     def close(self) -> None:
         if getattr(self, "_handle", None):
-            torch.cuda.synchronize(self.device)
+            # only this plan's stream can still use its workspace
+            self._stream_obj.synchronize()
             _lib.lib().gd_plan_destroy(self._handle)
             self._handle = None
             self.workspace = None
