@@ -37,12 +37,12 @@ struct gd_plan_s {
   size_t arena_elems = 0, code_bytes = 0, dense_elems = 0;
   int max_partials = 1;
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
-         o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, total = 0;
+         o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, o_trip = 0, total = 0;
   size_t bottom_smem = 0;
   char *ws = nullptr;
   bool prepared = false;
   std::vector<char> mask_set;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr;  // the whole solve: init, device-side while loop, mean
   cudaStream_t cap = nullptr;
   int cap_device = -1;
   long long solves = 0;  // completed solves; the graph is captured from the second on
@@ -502,6 +502,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   p->o_p1 = sect(p->max_partials * sizeof(double));
   p->o_cnt = sect(16 * sizeof(unsigned));
   p->o_nact = sect(sizeof(int));
+  p->o_trip = sect(sizeof(int));
   p->total = o;
   return GD_OK;
 }
@@ -630,58 +631,149 @@ extern "C" int gd_plan_prepare(gd_plan p, cudaStream_t st) {
 
 namespace {
 
+// Condition of the solve graph's while loop: iterate while any instance is
+// active, at most `cap` times.  `start` resets the trip counter.
+__global__ void k_loop_gate(cudaGraphConditionalHandle h, const int *n_active, int *trips,
+                            int start, int cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int t = start ? 0 : *trips + 1;
+  *trips = t;
+  cudaGraphSetConditional(h, (*n_active > 0 && t < cap) ? 1u : 0u);
+}
+
 template <typename T>
-int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
-  const Args<T> a = Runner<T>::args(p);
-  const Args<T> fine = Runner<T>::at_tiles(a, p->fine_base);
+void launch_init(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
   k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
   st::k_resid_s<T, true><<<p->fine_count, st::kThreads, 0, st>>>(fine);
   prof_end(p, st);
-  GD_CHECK_LAUNCH();
-  GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
-                                cudaMemcpyDeviceToHost, st));
-  GD_CHECK_CUDA(cudaStreamSynchronize(st));
-  // A plan solved once runs on direct launches; from its second solve on the
-  // iteration is one graph launch (capture and instantiation cost more than
-  // the launches they save in a single solve).
-  const bool graph = p->prm.use_graph && !p->profiling && p->solves >= 1;
-  if (graph && !p->gexec) {
-    if (!p->cap) {
-      GD_CHECK_CUDA(cudaGetDevice(&p->cap_device));
-      GD_CHECK_CUDA(capture_stream_get(p->cap_device, &p->cap));
-    }
-    cudaGraph_t g = nullptr;
-    GD_CHECK_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-    Runner<T>::dispatch_iteration(p, a, p->cap);
-    GD_CHECK_CUDA(cudaStreamEndCapture(p->cap, &g));
-    const cudaError_t e = cudaGraphInstantiate(&p->gexec, g, 0);
-    cudaGraphDestroy(g);
-    GD_CHECK_CUDA(e);
+}
+
+template <typename T>
+void launch_mean(gd_plan p, const Args<T> &fine, cudaStream_t st) {
+  prof_begin(p, GD_K_MEAN, p->fine_cells, st);
+  k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  prof_end(p, st);
+}
+
+bool plan_any_mean(gd_plan p) {
+  for (int i = 0; i < p->n; ++i)
+    if (p->inst[i].zero_mean) return true;
+  return false;
+}
+
+int loop_cap(gd_plan p) {
+  return (int)std::min<long long>((long long)p->prm.max_iterations + 8, 1ll << 30);
+}
+
+// One graph per plan for a whole solve: the initial residual, a conditional
+// while node whose body is one Krylov iteration followed by k_loop_gate, and
+// the zero-mean projection.  The device decides when to stop, so a solve is a
+// single graph launch with no host round trip and no iteration past the last
+// active instance.
+template <typename T>
+int build_solve_graph(gd_plan p, const Args<T> &a, const Args<T> &fine) {
+  if (!p->cap) {
+    GD_CHECK_CUDA(cudaGetDevice(&p->cap_device));
+    GD_CHECK_CUDA(capture_stream_get(p->cap_device, &p->cap));
   }
-  const int chunk = p->prm.check_every;
-  const long long cap_iters = (long long)p->prm.max_iterations + 2ll * chunk + 8;
-  long long done = 0;
-  while (*p->h_nact > 0 && done < cap_iters) {
-    for (int c = 0; c < chunk; ++c) {
-      if (graph) GD_CHECK_CUDA(cudaGraphLaunch(p->gexec, st));
-      else Runner<T>::dispatch_iteration(p, a, st);
+  cudaStream_t cs = p->cap;
+  int *trips = reinterpret_cast<int *>(p->ws + p->o_trip);
+  const int cap = loop_cap(p);
+  GD_CHECK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  cudaGraphConditionalHandle h{};
+  cudaGraph_t body = nullptr;
+  do {
+    launch_init(p, fine, cs);
+    cudaStreamCaptureStatus status;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &nd)) != cudaSuccess) break;
+    if ((e = cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault)) !=
+        cudaSuccess)
+      break;
+    k_loop_gate<<<1, 32, 0, cs>>>(h, a.n_active, trips, 1, cap);
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &nd)) != cudaSuccess) break;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    if ((e = cudaGraphAddNode(&wn, cg, deps, nd, &cp)) != cudaSuccess) break;
+    body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamUpdateCaptureDependencies(cs, &wn, 1, cudaStreamSetCaptureDependencies)) !=
+        cudaSuccess)
+      break;
+    if (plan_any_mean(p)) launch_mean(p, fine, cs);
+    e = cudaGetLastError();
+  } while (0);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+  if (e == cudaSuccess) e = ee;
+  if (e == cudaSuccess) {
+    e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      Runner<T>::dispatch_iteration(p, a, cs);
+      k_loop_gate<<<1, 32, 0, cs>>>(h, a.n_active, trips, 0, cap);
+      e = cudaGetLastError();
+      cudaGraph_t bg = nullptr;
+      const cudaError_t eb = cudaStreamEndCapture(cs, &bg);
+      if (e == cudaSuccess) e = eb;
     }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->gexec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    p->gexec = nullptr;
+    set_error("solve graph: %s", cudaGetErrorString(e));
+    return GD_ERR_CUDA;
+  }
+  return GD_OK;
+}
+
+template <typename T>
+int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
+  const Args<T> a = Runner<T>::args(p);
+  const Args<T> fine = Runner<T>::at_tiles(a, p->fine_base);
+  // A plan solved once runs on direct launches with the host polling the
+  // active count every `check_every` iterations; from its second solve on the
+  // whole solve is one graph launch (capture and instantiation cost more than
+  // they save in a single solve).
+  const bool graph = p->prm.use_graph && !p->profiling && p->solves >= 1;
+  if (graph) {
+    if (!p->gexec) {
+      const int rc = build_solve_graph<T>(p, a, fine);
+      if (rc != GD_OK) return rc;
+    }
+    GD_CHECK_CUDA(cudaGraphLaunch(p->gexec, st));
+  } else {
+    launch_init(p, fine, st);
     GD_CHECK_LAUNCH();
-    done += chunk;
     GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
                                   cudaMemcpyDeviceToHost, st));
     GD_CHECK_CUDA(cudaStreamSynchronize(st));
-    prof_collect(p);
-  }
-  bool any_mean = false;
-  for (int i = 0; i < p->n; ++i) any_mean |= p->inst[i].zero_mean != 0;
-  if (any_mean) {
-    prof_begin(p, GD_K_MEAN, p->fine_cells, st);
-    k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-    k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-    prof_end(p, st);
-    GD_CHECK_LAUNCH();
+    const int chunk = p->prm.check_every;
+    const long long cap_iters = loop_cap(p);
+    long long done = 0;
+    while (*p->h_nact > 0 && done < cap_iters) {
+      for (int c = 0; c < chunk; ++c) Runner<T>::dispatch_iteration(p, a, st);
+      GD_CHECK_LAUNCH();
+      done += chunk;
+      GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
+                                    cudaMemcpyDeviceToHost, st));
+      GD_CHECK_CUDA(cudaStreamSynchronize(st));
+      prof_collect(p);
+    }
+    if (plan_any_mean(p)) {
+      launch_mean(p, fine, st);
+      GD_CHECK_LAUNCH();
+    }
   }
   GD_CHECK_CUDA(cudaMemcpyAsync(p->h_st, p->ws + p->o_st, sizeof(InstState) * p->n,
                                 cudaMemcpyDeviceToHost, st));

@@ -34,8 +34,8 @@ class SolveParams:
     max_iterations: int = 2000
     tolerance: float = 1e-8
     reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
-    check_every: int = 4          # iterations between host polls of the active count
-    use_graph: bool = True
+    check_every: int = 4          # host poll interval of solves on direct launches
+    use_graph: bool = True        # from a plan's second solve on: one graph, device-side loop
     strip_target_warps: int = 1200  # smoother strip height: warps wanted per level
 
     def c_params(self) -> _lib.Params:

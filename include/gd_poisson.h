@@ -70,8 +70,9 @@ typedef struct gd_params {
   int32_t max_iterations; /* PCG iteration budget (solvers.py:176 default 2000)    */
   double tolerance;       /* target ||f - A x|| / ||f|| (solvers.py:175 default 1e-8) */
   double reliable_delta;  /* mixed precision: residual drop between FP64 refreshes */
-  int32_t check_every;    /* iterations between host-side convergence polls        */
-  int32_t use_graph;      /* capture one iteration as a CUDA graph and replay it    */
+  int32_t check_every;    /* host poll interval of solves on direct launches         */
+  int32_t use_graph;      /* from a plan's second solve on, run the whole solve as   *
+                           * one CUDA graph whose while node loops on the device     */
   int32_t strip_target_warps; /* smoother strips: warps wanted per level (0 = 1200) */
   int32_t reserved;
 } gd_params;

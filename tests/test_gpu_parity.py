@@ -184,6 +184,39 @@ def test_zero_and_nonfinite_rhs_are_reported_not_raised():
     assert not r1.converged and r1.status in (_lib.GD_BREAKDOWN, _lib.GD_MAX_ITERATIONS)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_graph_solves_equal_direct_solves(precision):
+    """The first solve of a plan runs on direct launches with host polls; later
+    solves are one graph with a device-side while loop.  Same bits, same counts,
+    and the device loop stops at the iteration cap and on zero / NaN inputs."""
+    rng = np.random.default_rng(21)
+    shapes = [(96, 80, "neumann"), (70, 50, "dirichlet"), (33, 129, "neumann"), (40, 40, "dirichlet")]
+    rhs = [torch.as_tensor(rng.standard_normal(s[:2])).cuda() for s in shapes]
+    rhs[3] = torch.zeros((40, 40), dtype=torch.float64, device="cuda")
+    plan = PoissonPlan([Instance(*s[:2], s[2], s[2] == "neumann") for s in shapes],
+                       SolveParams(precision=precision, tolerance=1e-10))
+    runs = []
+    for _ in range(3):
+        xs = [torch.zeros_like(r) for r in rhs]
+        res = plan.solve(rhs, xs, scale=-1.0)
+        runs.append(([t.clone() for t in xs], [(r.iterations, r.status) for r in res]))
+    for xs, st in runs[1:]:
+        assert st == runs[0][1]
+        for a, b in zip(xs, runs[0][0]):
+            assert torch.equal(a, b)
+    assert all(r[1] == _lib.GD_CONVERGED for r in runs[0][1])
+    assert runs[0][1][3][0] == 0
+    capped = PoissonPlan([Instance(96, 80, "neumann", True), Instance(40, 40, "dirichlet")],
+                         SolveParams(precision=precision, tolerance=1e-14, max_iterations=2))
+    bad = torch.ones((40, 40), dtype=torch.float64, device="cuda")
+    bad[3, 5] = float("nan")
+    for _ in range(3):
+        x = [torch.zeros_like(rhs[0]), torch.zeros_like(bad)]
+        r0, r1 = capped.solve([rhs[0], bad], x, scale=-1.0)
+        assert r0.iterations == 2 and r0.status == _lib.GD_MAX_ITERATIONS
+        assert r1.status in (_lib.GD_BREAKDOWN, _lib.GD_MAX_ITERATIONS)
+
+
 def test_masked_and_dirichlet_applications_match_golden(golden):
     field = gd.GuidanceField.of(golden["app_src"])
     got, reps = gd.solve_masked(field, golden["app_img"], golden["app_disc"])
