@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "active"
 EXPORTS = (
     "gd_last_error", "gd_version", "gd_plan_create", "gd_plan_destroy",
     "gd_plan_workspace_bytes", "gd_plan_bind", "gd_plan_set_mask", "gd_plan_prepare",
-    "gd_solve", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
+    "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
     "gd_masked_rhs",
@@ -82,6 +82,9 @@ def _declare(lib: C.CDLL) -> None:
         "gd_solve": (C.c_int, [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                C.POINTER(C.c_int32), C.POINTER(C.c_double), _vp,
                                C.POINTER(Report)]),
+        "gd_solve_async": (C.c_int, [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double), _vp]),
+        "gd_solve_finish": (C.c_int, [_vp, C.POINTER(Report)]),
         "gd_plan_apply_vcycle": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
         "gd_plan_set_profiling": (C.c_int, [_vp, _i32]),
         "gd_plan_kernel_times": (C.c_int, [_vp, C.POINTER(KernelTime), _i32]),

@@ -49,6 +49,8 @@ struct gd_plan_s {
   int *h_nact = nullptr;
   InstState *h_st = nullptr;
   size_t h_st_bytes = 0;
+  cudaEvent_t done_ev = nullptr;  // recorded after the states of an asynchronous solve
+  bool pending = false;           // an asynchronous solve awaits gd_solve_finish
   // profiling: events around every launch (graphs are bypassed while enabled)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -559,6 +561,7 @@ extern "C" void gd_plan_destroy(gd_plan p) {
   if (!p) return;
   for (cudaEvent_t e : p->ev_pool) cudaEventDestroy(e);
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
+  if (p->done_ev) cudaEventDestroy(p->done_ev);
   capture_stream_put(p->cap_device, p->cap);
   pinned_put(p->h_nact, sizeof(int));
   pinned_put(p->h_st, p->h_st_bytes);
@@ -737,8 +740,12 @@ int build_solve_graph(gd_plan p, const Args<T> &a, const Args<T> &fine) {
   return GD_OK;
 }
 
+// Enqueue one solve on `st`.  With the plan's graph the call returns at once
+// (the states are copied to pinned host memory behind the graph and
+// `done_ev` marks them); without it (first solve, profiling) it runs the
+// host-polled loop and returns with the stream drained.
 template <typename T>
-int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
+int enqueue_solve(gd_plan p, cudaStream_t st) {
   const Args<T> a = Runner<T>::args(p);
   const Args<T> fine = Runner<T>::at_tiles(a, p->fine_base);
   // A plan solved once runs on direct launches with the host polling the
@@ -777,9 +784,19 @@ int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
   }
   GD_CHECK_CUDA(cudaMemcpyAsync(p->h_st, p->ws + p->o_st, sizeof(InstState) * p->n,
                                 cudaMemcpyDeviceToHost, st));
-  GD_CHECK_CUDA(cudaStreamSynchronize(st));
-  prof_collect(p);
+  if (!p->done_ev) GD_CHECK_CUDA(cudaEventCreateWithFlags(&p->done_ev, cudaEventDisableTiming));
+  GD_CHECK_CUDA(cudaEventRecord(p->done_ev, st));
   ++p->solves;
+  p->pending = true;
+  return GD_OK;
+}
+
+// Wait for the last enqueued solve and turn its device states into reports.
+int collect_reports(gd_plan p, gd_report *reports) {
+  GD_REQUIRE(p->pending, GD_ERR_STATE, "gd_solve_finish: no solve in flight");
+  GD_CHECK_CUDA(cudaEventSynchronize(p->done_ev));
+  p->pending = false;
+  prof_collect(p);
   for (int i = 0; i < p->n; ++i) {
     const InstState &S = p->h_st[i];
     gd_report &R = reports[i];
@@ -793,10 +810,13 @@ int run_solve(gd_plan p, cudaStream_t st, gd_report *reports) {
 
 }  // namespace
 
-extern "C" int gd_solve(gd_plan p, const double *const *f, double *const *x, const int32_t *pitch,
-                        const double *scale, cudaStream_t st, gd_report *reports) {
-  GD_REQUIRE(p && f && x && pitch && scale && reports, GD_ERR_ARG, "gd_solve: bad arguments");
+namespace {
+int bind_solve(gd_plan p, const double *const *f, double *const *x, const int32_t *pitch,
+               const double *scale, cudaStream_t st) {
+  GD_REQUIRE(p && f && x && pitch && scale, GD_ERR_ARG, "gd_solve: bad arguments");
   GD_REQUIRE(p->ws && p->prepared, GD_ERR_STATE, "gd_solve: plan not bound and prepared");
+  GD_REQUIRE(!p->pending, GD_ERR_STATE, "gd_solve: the previous asynchronous solve of this "
+                                        "plan has not been finished");
   for (int i = 0; i < p->n; ++i) {
     GD_REQUIRE(f[i] && x[i] && pitch[i] >= p->inst[i].nx, GD_ERR_ARG,
                "gd_solve: instance %d has a bad pointer or pitch", i);
@@ -805,9 +825,29 @@ extern "C" int gd_solve(gd_plan p, const double *const *f, double *const *x, con
     p->inst[i].upitch = pitch[i];
     p->inst[i].scale = scale[i];
   }
+  // pageable source: staged before the call returns, so p->inst may change afterwards
   GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->inst.data(),
                                 p->inst.size() * sizeof(InstInfo), cudaMemcpyHostToDevice, st));
-  return p->fp64 ? run_solve<double>(p, st, reports) : run_solve<float>(p, st, reports);
+  return p->fp64 ? enqueue_solve<double>(p, st) : enqueue_solve<float>(p, st);
+}
+}  // namespace
+
+extern "C" int gd_solve(gd_plan p, const double *const *f, double *const *x, const int32_t *pitch,
+                        const double *scale, cudaStream_t st, gd_report *reports) {
+  GD_REQUIRE(reports, GD_ERR_ARG, "gd_solve: bad arguments");
+  const int rc = bind_solve(p, f, x, pitch, scale, st);
+  if (rc != GD_OK) return rc;
+  return collect_reports(p, reports);
+}
+
+extern "C" int gd_solve_async(gd_plan p, const double *const *f, double *const *x,
+                              const int32_t *pitch, const double *scale, cudaStream_t st) {
+  return bind_solve(p, f, x, pitch, scale, st);
+}
+
+extern "C" int gd_solve_finish(gd_plan p, gd_report *reports) {
+  GD_REQUIRE(p && reports, GD_ERR_ARG, "gd_solve_finish: bad arguments");
+  return collect_reports(p, reports);
 }
 
 namespace {

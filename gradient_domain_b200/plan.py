@@ -121,9 +121,7 @@ class PoissonPlan:
         _lib.check(_lib.lib().gd_plan_prepare(self._handle, self._stream), "gd_plan_prepare")
         self._prepared = True
 
-    def solve(self, rhs: list[torch.Tensor], x: list[torch.Tensor],
-              scale: list[float] | float = 1.0) -> list[InstanceResult]:
-        """Solve ``A x_i = scale_i * rhs_i`` in place in ``x`` (FP64 device tensors)."""
+    def _arguments(self, rhs, x, scale):
         if not self._prepared:
             self.prepare()
         n = len(self.instances)
@@ -146,11 +144,39 @@ class PoissonPlan:
             fp[k] = _lib.ptr(rhs[k])
             xp[k] = _lib.ptr(x[k])
             pitch[k] = x[k].stride(0)
+        return fp, xp, pitch, sc
+
+    def _results(self) -> list[InstanceResult]:
+        return [InstanceResult(int(r.iterations), int(r.status), float(r.relative_residual),
+                               float(r.initial_norm)) for r in self._reports]
+
+    def solve(self, rhs: list[torch.Tensor], x: list[torch.Tensor],
+              scale: list[float] | float = 1.0) -> list[InstanceResult]:
+        """Solve ``A x_i = scale_i * rhs_i`` in place in ``x`` (FP64 device tensors)."""
+        fp, xp, pitch, sc = self._arguments(rhs, x, scale)
         with self._lock:
             _lib.check(_lib.lib().gd_solve(self._handle, fp, xp, pitch, sc, self._stream,
                                            self._reports), "gd_solve")
-            return [InstanceResult(int(r.iterations), int(r.status), float(r.relative_residual),
-                                   float(r.initial_norm)) for r in self._reports]
+            return self._results()
+
+    def solve_async(self, rhs: list[torch.Tensor], x: list[torch.Tensor],
+                    scale: list[float] | float = 1.0) -> None:
+        """Enqueue :meth:`solve` on the plan's stream; :meth:`finish` returns the results.
+
+        From the plan's second solve on the call does not wait for the device,
+        so copies and other solves can be queued behind or beside it.  ``rhs``
+        and ``x`` must stay alive until :meth:`finish`.
+        """
+        fp, xp, pitch, sc = self._arguments(rhs, x, scale)
+        with self._lock:
+            _lib.check(_lib.lib().gd_solve_async(self._handle, fp, xp, pitch, sc, self._stream),
+                       "gd_solve_async")
+
+    def finish(self) -> list[InstanceResult]:
+        """Wait for the solve started by :meth:`solve_async` and return its results."""
+        with self._lock:
+            _lib.check(_lib.lib().gd_solve_finish(self._handle, self._reports), "gd_solve_finish")
+            return self._results()
 
     def apply_vcycle(self, index: int, r: torch.Tensor) -> torch.Tensor:
         """One V-cycle of the preconditioner on an FP64 residual (inspection hook)."""

@@ -31,7 +31,9 @@ Every method runs on the device; there is no CPU path.
 
 from __future__ import annotations
 
+import threading
 import time
+from collections import OrderedDict
 from dataclasses import dataclass
 
 import numpy as np
@@ -39,7 +41,7 @@ import torch
 
 from . import _lib
 from .multigrid import MultigridOptions, RefWorkspace
-from .plan import Instance, SolveParams, cached_plan
+from .plan import Instance, PoissonPlan, SolveParams, cached_plan
 
 __all__ = ["SolverReport", "SOLVERS", "solve_system", "solve_neumann", "solve_neumann_batch"]
 
@@ -233,9 +235,20 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
     ``b`` may be a NumPy array or a (preferably pinned) CPU torch tensor; with
     ``out`` (a CPU tensor of the same shape) the solutions are copied there and
     ``out`` is returned, otherwise a new NumPy array is.  All ``n`` problems go
-    through the same kernel launches (they are instances of one plan).
+    through the same kernel launches (they are instances of one plan), except
+    when ``b`` and ``out`` are both pinned FP64 tensors: then each problem has
+    its own plan and stream, so host-device copies overlap the solves (the
+    results are bitwise the same either way).
     """
     dev = _lib.device()
+    if (isinstance(b, torch.Tensor) and isinstance(out, torch.Tensor) and b.dim() == 3
+            and b.shape[0] > 1 and b.dtype == torch.float64 and out.dtype == torch.float64
+            and b.device.type == "cpu" and out.device.type == "cpu" and b.is_pinned()
+            and out.is_pinned() and out.shape == b.shape):
+        params = SolveParams(precision=precision, tolerance=tolerance,
+                             max_iterations=max_iterations)
+        solve_neumann_batch.last_results = _pipelined_neumann(b, out, params)
+        return out
     if isinstance(b, torch.Tensor):
         f = b.to(device=dev, dtype=torch.float64, non_blocking=True)
     else:
@@ -257,3 +270,69 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
 
 
 solve_neumann_batch.last_results = []
+
+_PIPELINES: OrderedDict = OrderedDict()
+_PIPELINE_LOCK = threading.Lock()
+
+
+def _take_pipeline(h: int, w: int, params: SolveParams, n: int):
+    """``n`` single-instance plans, each with its own stream and device buffers.
+
+    A pipeline is removed from the cache while in use, so concurrent callers of
+    the same shape each get their own.
+    """
+    key = (h, w, params, n)
+    with _PIPELINE_LOCK:
+        pipe = _PIPELINES.pop(key, None)
+    if pipe is not None:
+        return key, pipe
+    dev = _lib.device()
+    pipe = []
+    for _ in range(n):
+        stream = torch.cuda.Stream(dev)
+        with torch.cuda.stream(stream):
+            plan = PoissonPlan([Instance(h, w, "neumann", True)], params, stream=stream)
+            f = torch.empty((h, w), dtype=torch.float64, device=dev)
+            x = torch.empty_like(f)
+        pipe.append((plan, stream, f, x))
+    return key, pipe
+
+
+def _return_pipeline(key, pipe) -> None:
+    with _PIPELINE_LOCK:
+        if key in _PIPELINES:
+            for plan, *_ in pipe:
+                plan.close()
+            return
+        _PIPELINES[key] = pipe
+        while len(_PIPELINES) > 4:
+            _, old = _PIPELINES.popitem(last=False)
+            for plan, *_ in old:
+                plan.close()
+
+
+def _pipelined_neumann(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
+    """Channel k's upload, solve and download run on stream k: the copy of one
+    channel overlaps the solves of the others (copy engines and SMs work at the
+    same time), and each solve is one graph with a device-side loop."""
+    n, h, w = b.shape
+    key, pipe = _take_pipeline(h, w, params, n)
+    try:
+        caller = torch.cuda.current_stream()
+        for k, (plan, stream, f, x) in enumerate(pipe):
+            stream.wait_stream(caller)
+            with torch.cuda.stream(stream):
+                f.copy_(b[k], non_blocking=True)
+                x.zero_()
+                plan.solve_async([f], [x], scale=-1.0)
+                out[k].copy_(x, non_blocking=True)
+        results = []
+        for plan, stream, f, x in pipe:
+            results.extend(plan.finish())
+            stream.synchronize()
+    except BaseException:
+        for plan, *_ in pipe:
+            plan.close()
+        raise
+    _return_pipeline(key, pipe)
+    return results

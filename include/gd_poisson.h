@@ -126,6 +126,17 @@ int gd_solve(gd_plan plan, const double *const *f_dev, double *const *x_dev,
              const int32_t *pitch, const double *scale, cudaStream_t stream,
              gd_report *reports);
 
+/* gd_solve in two halves, so that copies and other work can overlap a solve.
+ * gd_solve_async enqueues the solve on `stream` and, once the plan has been
+ * solved before (its whole solve is then one CUDA graph with a device-side
+ * loop), returns without waiting; a plan's first solve and profiled solves
+ * still poll the host and return with the stream drained.  gd_solve_finish
+ * waits for that solve and fills reports[n].  One solve per plan may be in
+ * flight; gd_solve on a plan with an unfinished solve returns GD_ERR_STATE. */
+int gd_solve_async(gd_plan plan, const double *const *f_dev, double *const *x_dev,
+                   const int32_t *pitch, const double *scale, cudaStream_t stream);
+int gd_solve_finish(gd_plan plan, gd_report *reports);
+
 /* One application of the preconditioner (a single V-cycle from zero) to the
  * FP64 residual r of instance i: z = M r.  Test and inspection hook. */
 int gd_plan_apply_vcycle(gd_plan plan, int32_t instance, const double *r_dev,

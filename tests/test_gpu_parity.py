@@ -217,6 +217,33 @@ def test_graph_solves_equal_direct_solves(precision):
         assert r1.status in (_lib.GD_BREAKDOWN, _lib.GD_MAX_ITERATIONS)
 
 
+def test_async_solve_and_pipelined_batch():
+    rng = np.random.default_rng(23)
+    f = torch.as_tensor(rng.standard_normal((70, 50))).cuda()
+    plan = PoissonPlan([Instance(70, 50, "dirichlet")], SolveParams(tolerance=1e-10))
+    x_sync = torch.zeros_like(f)
+    (r_sync,) = plan.solve([f], [x_sync])
+    for _ in range(2):  # direct launches, then the graph
+        x = torch.zeros_like(f)
+        plan.solve_async([f], [x])
+        with pytest.raises(_lib.GDError):
+            plan.solve([f], [torch.zeros_like(f)])  # one solve in flight per plan
+        (r,) = plan.finish()
+        assert torch.equal(x, x_sync) and r.iterations == r_sync.iterations
+    with pytest.raises(_lib.GDError):
+        plan.finish()
+    stack = -np.stack([rng.standard_normal((64, 96)) for _ in range(3)])
+    stack -= stack.mean(axis=(1, 2), keepdims=True)
+    want = gd.solve_neumann_batch(stack, tolerance=1e-12)
+    host_in = torch.as_tensor(stack).pin_memory()
+    for _ in range(3):
+        host_out = torch.full_like(host_in, 5.0).pin_memory()
+        got = gd.solve_neumann_batch(host_in, tolerance=1e-12, out=host_out)
+        assert got is host_out
+        assert np.array_equal(host_out.numpy(), want)
+        assert all(r.converged for r in gd.solve_neumann_batch.last_results)
+
+
 def test_masked_and_dirichlet_applications_match_golden(golden):
     field = gd.GuidanceField.of(golden["app_src"])
     got, reps = gd.solve_masked(field, golden["app_img"], golden["app_disc"])
