@@ -15,6 +15,7 @@
 // once as a CUDA graph.
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -180,7 +181,7 @@ struct Runner {
   template <int S>
   static void set_attrs() {
     cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
+                         kBottomSmem);
     const int lvl = (int)st::level_smem<T>();
     cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, lvl);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -294,6 +295,51 @@ void strip_widths(gd_plan p, int *down_ow, int *up_ow) {
   }
 }
 
+// Shared-memory layout of a bottom holding levels first..last (padded b, u and
+// classes per level, then the dense solve's FP64 right-hand side); returns its
+// size in bytes and, with `write`, records the offsets in the levels.
+int bottom_layout(gd_plan p, int first, int last, size_t es, bool write) {
+  size_t off = 0;
+  auto a16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+  for (int l = first; l <= last; ++l) {
+    LevelInfo &L = p->lv[l];
+    const size_t px = (size_t)L.nx + 3, cells = px * ((size_t)L.ny + 3);
+    const size_t b = off;
+    off = a16(off + cells * es);
+    const size_t u = off;
+    off = a16(off + cells * es);
+    const size_t c = off;
+    off = a16(off + cells);
+    if (write) {
+      L.sm_b = (int)b;
+      L.sm_u = (int)u;
+      L.sm_c = (int)c;
+      L.sm_px = (int)px;
+    }
+  }
+  const size_t d = off;
+  off = a16(off + (size_t)kCoarsestCells * sizeof(double));
+  if (write) {
+    p->lv[last].sm_d = (int)d;
+    for (int l = first; l <= last; ++l) p->lv[l].sm_end = (int)off;
+  }
+  return off > (size_t)INT_MAX ? INT_MAX : (int)off;
+}
+
+// The bottom of one instance (levels level0 .. level0 + last): the first level
+// with at most bottom_cells (default kBottomCells) cells whose levels fit
+// kBottomSmem bytes and kBottomLevels levels, else the coarsest.
+int choose_bottom(gd_plan p, int level0, int last, size_t es) {
+  const long long max_cells = p->prm.bottom_cells > 0 ? p->prm.bottom_cells : kBottomCells;
+  for (int l = 0; l <= last; ++l) {
+    const LevelInfo &L = p->lv[level0 + l];
+    if ((long long)L.ny * L.nx > max_cells) continue;
+    if (last - l + 1 > kBottomLevels) continue;
+    if (bottom_layout(p, level0 + l, level0 + last, es, false) <= kBottomSmem) return l;
+  }
+  return last;
+}
+
 // Strip height for one level: the tallest of 64, 32, 16, 8 rows that still
 // gives `target` warps for this level, else 8 (taller strips amortise the
 // warm-up rows, shorter ones give small levels enough parallelism).
@@ -375,8 +421,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       }
       L.inv_off = -1;
       const long long cells = (long long)ny * nx;
-      if (bottom < 0 && cells <= kBottomCells) bottom = level;
-      L.is_bottom = (bottom == level);
+      L.is_bottom = 0;
       const bool coarsest = cells <= kCoarsestCells;
       L.coarse = coarsest ? -1 : (int)p->lv.size() + 1;
       if (coarsest) {
@@ -390,6 +435,8 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       ++level;
     }
     I.nlevels = level + 1;
+    bottom = choose_bottom(p, I.level0, level, es);
+    p->lv[I.level0 + bottom].is_bottom = 1;
     I.bottom = I.level0 + bottom;
     I.coarsest = I.level0 + level;
     bottoms[i] = bottom;
@@ -406,7 +453,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   }
   int down_ow = 0, up_ow = 0;
   strip_widths(p, &down_ow, &up_ow);
-  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 1200;
+  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 600;
   for (int i = 0; i < p->n; ++i) {
     const InstInfo &I = p->inst[i];
     for (int l = 0; l < bottoms[i]; ++l) {
@@ -469,19 +516,9 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   }
   // bottom shared memory
   size_t bsm = 0;
-  for (int i = 0; i < p->n; ++i) {
-    const InstInfo &I = p->inst[i];
-    size_t telems = 0, cbytes = 0;
-    for (int l = I.bottom; l <= I.coarsest; ++l) {
-      const size_t c = (size_t)p->lv[l].ny * p->lv[l].nx;
-      telems += 2 * c;
-      cbytes += c;
-    }
-    telems += (size_t)p->lv[I.bottom].ny * p->lv[I.bottom].nx;
-    telems = (telems * es + 7) / 8 * 8 / es;
-    telems += 2 * kCoarsestCells * (sizeof(double) / es);
-    bsm = std::max(bsm, telems * es + cbytes + 64);
-  }
+  for (int i = 0; i < p->n; ++i)
+    bsm = std::max(bsm, (size_t)bottom_layout(p, p->inst[i].bottom, p->inst[i].coarsest, es,
+                                              true));
   p->bottom_smem = bsm;
   p->arena_elems = arena;
   p->code_bytes = std::max<size_t>(codes, kArrayAlign);
@@ -520,6 +557,7 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
              GD_ERR_UNSUPPORTED, "gd_plan_create: pre_sweeps == post_sweeps in 1..3 required");
   GD_REQUIRE(params->precision == GD_MIXED || params->precision == GD_FP64, GD_ERR_ARG,
              "gd_plan_create: unknown precision %d", params->precision);
+  GD_REQUIRE(params->bottom_cells >= 0, GD_ERR_ARG, "gd_plan_create: negative bottom_cells");
   GD_REQUIRE(params->max_iterations >= 0 && params->tolerance >= 0.0, GD_ERR_ARG,
              "gd_plan_create: bad tolerance / iteration budget");
   for (int i = 0; i < n; ++i) {
@@ -548,7 +586,7 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
     gd_plan_destroy(p);
     return GD_ERR_CUDA;
   }
-  if (p->bottom_smem > 200 * 1024) {
+  if (p->bottom_smem > (size_t)kBottomSmem) {
     set_error("gd_plan_create: bottom levels need %zu bytes of shared memory", p->bottom_smem);
     gd_plan_destroy(p);
     return GD_ERR_UNSUPPORTED;

@@ -7,17 +7,21 @@ namespace gd {
 
 // Hierarchy rules.  A level is coarsened (ceil(ny/2) x ceil(nx/2)) while it has
 // more than kCoarsestCells cells; the first level with at most kBottomCells
-// cells and everything below it is handled by one CTA per instance in shared
-// memory; the coarsest level is solved with a dense FP64 inverse.
+// cells (a plan may choose another limit) whose levels down to the coarsest
+// fit in kBottomSmem bytes of shared memory (padded b, u and classes) is
+// handled, with everything below it, by one CTA per instance; the coarsest
+// level is solved with a dense FP64 inverse.
 constexpr int kCoarsestCells = 64;
 constexpr int kBottomCells = 4096;
+constexpr int kBottomSmem = 220 * 1024;
+constexpr int kBottomLevels = 24;  // most levels one bottom holds
 
 // Fine-level (level 0) kernels: 64 rows x 128 columns per CTA of 128 threads
 // (four warps, each 16 rows x 128 columns).  Down / up kernels use the same
 // CTA shape with a per-level strip height.
 constexpr int kFTY = 64, kFTX = 128, kFThreads = 128;
 constexpr int kVThreads = 128;     // down / up kernels
-constexpr int kBThreads = 512;     // bottom kernel
+constexpr int kBThreads = 1024;    // bottom kernel
 constexpr int kLastWarps = kFThreads / 32;
 
 enum : int { BC_DIR = 0, BC_NEU = 1, BC_MASK = 2 };
@@ -29,6 +33,10 @@ struct LevelInfo {
   float wall, pad0;
   int rows_per_warp;  // strip height of the down / up kernels on this level (even)
   int pad2;
+  // bottom levels: byte offsets of the padded b, u and class arrays in the
+  // bottom kernel's shared memory, their row pitch (nx + 3), the FP64 right-
+  // hand side of the dense solve (coarsest level) and the end of the layout
+  int sm_b, sm_u, sm_c, sm_px, sm_d, sm_end;
   long long b_off, u_off;  // element offsets into the T arena
   long long w_off;         // pre-smoothed iterate written by down, read by up
   long long code_off;      // byte offset into the code arena, -1 if rectangle

@@ -90,192 +90,208 @@ __device__ __forceinline__ int mirror_fine(int f, int n, bool neumann) {
 }
 
 // ---------------------------------------------------------------------------
-// Bottom: the remaining V-cycle of one instance in shared memory.
-struct BottomLevel {
-  int ny, nx, bc;
-  float wall;
-  int off_b, off_u, off_c;  // shared-memory offsets (T elements / bytes)
-};
+// Bottom: the remaining V-cycle of one instance, every level in shared memory,
+// one CTA of kBThreads threads per instance.
+//
+// Each level keeps b, u and the cell classes in arrays padded with a ring of
+// zero ghosts (one row / column before the grid, two after; the restriction of
+// an odd-sized level reaches two cells past its edge).  A missing neighbour
+// then reads 0, as the operator defines, and Dirichlet / masked transfers read
+// zero ghosts, so no stencil needs a bounds check.  A warp works on whole rows
+// and its lanes on columns, so no index is divided.  The residual overwrites b
+// in place and the up pass reloads b from the arena, where the restriction also
+// writes it.
 
 template <typename T>
-__device__ __forceinline__ T sm_at(const T *u, int y, int x, int ny, int nx) {
-  return (y >= 0 && y < ny && x >= 0 && x < nx) ? u[y * nx + x] : T(0);
-}
-
-template <typename T>
-__device__ void bottom_smooth(T *u, const T *b, const unsigned char *c, const BottomLevel &L,
-                              const T *dinv, int colour) {
-  const int hw = (L.nx + 1) >> 1;
-  for (int k = threadIdx.x; k < L.ny * hw; k += blockDim.x) {
-    const int y = k / hw;
-    const int x = 2 * (k - y * hw) + ((colour + y) & 1);
-    if (x >= L.nx) continue;
-    const int i = y * L.nx + x;
-    const int cl = c[i];
-    if (cl)
-      u[i] = (b[i] + sm_at(u, y - 1, x, L.ny, L.nx) + sm_at(u, y + 1, x, L.ny, L.nx) +
-              sm_at(u, y, x - 1, L.ny, L.nx) + sm_at(u, y, x + 1, L.ny, L.nx)) * dinv[cl];
+__device__ __forceinline__ void bot_sweep(T *u, const T *b, const unsigned char *c, int ny,
+                                          int nx, int px, const T *dinv, int colour) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int y = warp; y < ny; y += kBThreads / 32) {
+    const int row = (y + 1) * px + 1;
+    for (int x = 2 * lane + ((colour + y) & 1); x < nx; x += 64) {
+      const int i = row + x;
+      const int cl = c[i];
+      if (cl) u[i] = (b[i] + u[i - px] + u[i + px] + u[i - 1] + u[i + 1]) * dinv[cl];
+    }
   }
   __syncthreads();
 }
 
+// Padded index of fine row / column f for the restriction: Neumann mirrors the
+// ghost at -1 and, for an even size n, the ghost at n (the adjoint of the
+// clamped prolongation); every other ghost reads zero.
+__device__ __forceinline__ int bot_mirror(int f, int n, bool neu) {
+  if (neu) {
+    if (f == -1) return 0;
+    if (f == n && !(n & 1)) return n - 1;
+  }
+  return f;
+}
+
 template <typename T, int S1, int S2>
-__global__ void __launch_bounds__(kBThreads) k_bottom(Args<T> a) {
+__global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
   const int inst = blockIdx.x;
   InstState &S = a.st[inst];
   if (S.status != GD_ACTIVE) return;
   const InstInfo &I = a.inst[inst];
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ BottomLevel bl[24];
-  __shared__ T tdiag[24][8], tdinv[24][8];
-  __shared__ int nb_s, res_off_s, dense_off_s, cbytes_off_s;
-  if (threadIdx.x == 0) {
-    int nb = 0, off = 0;
-    for (int l = I.bottom;; ++l) {
-      const LevelInfo &L = a.lv[l];
-      BottomLevel &B = bl[nb++];
-      B.ny = L.ny; B.nx = L.nx; B.bc = L.bc; B.wall = L.wall;
-      B.off_b = off; off += L.ny * L.nx;
-      B.off_u = off; off += L.ny * L.nx;
-      if (l == I.coarsest || nb == 24) break;
-    }
-    nb_s = nb;
-    res_off_s = off;
-    off += bl[0].ny * bl[0].nx;
-    // double buffer for the dense solve, 8-byte aligned in T units
-    off = (off * (int)sizeof(T) + 7) / 8 * 8 / (int)sizeof(T);
-    dense_off_s = off;
-    off += 2 * kCoarsestCells * (int)(sizeof(double) / sizeof(T));
-    int cb = off * (int)sizeof(T);
-    for (int q = 0; q < nb; ++q) { bl[q].off_c = cb; cb += bl[q].ny * bl[q].nx; }
-    cbytes_off_s = cb;
+  __shared__ T tdiag[kBottomLevels][8], tdinv[kBottomLevels][8];
+  const int nb = I.coarsest - I.bottom + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = kBThreads / 32;
+  {  // zero every padded array (ghost rings stay zero for the whole launch)
+    const int bytes = a.lv[I.coarsest].sm_end;
+    uint4 *z = reinterpret_cast<uint4 *>(smem);
+    for (int k = threadIdx.x; k < bytes / 16; k += kBThreads) z[k] = make_uint4(0, 0, 0, 0);
+  }
+  for (int q = threadIdx.x; q < nb * 8; q += kBThreads) {
+    const int l = q >> 3, c = q & 7;
+    const float w = a.lv[I.bottom + l].wall;
+    const double d = c >= 1 && c <= 5 ? class_diag(c, w) : 1.0;
+    tdiag[l][c] = (T)d;
+    tdinv[l][c] = (c >= 1 && c <= 5 && d > 0.0) ? (T)(1.0 / d) : T(0);
   }
   __syncthreads();
-  const int nb = nb_s;
-  T *sm = reinterpret_cast<T *>(smem);
-  for (int q = threadIdx.x; q < nb * 8; q += blockDim.x) {
-    const int l = q >> 3, c = q & 7;
-    const double d = c >= 1 && c <= 5 ? class_diag(c, bl[l].wall) : 1.0;
-    tdiag[l][c] = (T)d;
-    tdinv[l][c] = (c >= 1 && c <= 5) ? (T)(1.0 / d) : T(0);
-  }
-  // classes of every level, and b of the bottom level
+  // classes of every level, and b of the top level
   for (int q = 0; q < nb; ++q) {
     const LevelInfo &L = a.lv[I.bottom + q];
-    unsigned char *c = smem + bl[q].off_c;
-    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
-      const int y = k / L.nx, x = k - y * L.nx;
-      c[k] = (unsigned char)cell_class(L, a.codes, y, x);
-    }
+    unsigned char *c = smem + L.sm_c;
+    const int px = L.sm_px;
+    for (int y = warp; y < L.ny; y += NW)
+      for (int x = lane; x < L.nx; x += 32)
+        c[(y + 1) * px + 1 + x] = (unsigned char)cell_class(L, a.codes, y, x);
   }
   {
     const LevelInfo &L = a.lv[I.bottom];
     const T *B = a.arena + L.b_off;
-    T *b0 = sm + bl[0].off_b;
-    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
-      const int y = k / L.nx, x = k - y * L.nx;
-      b0[k] = B[(long long)y * L.pitch + x];
-    }
+    T *b = reinterpret_cast<T *>(smem + L.sm_b);
+    for (int y = warp; y < L.ny; y += NW)
+      for (int x = lane; x < L.nx; x += 32)
+        b[(y + 1) * L.sm_px + 1 + x] = B[(long long)y * L.pitch + x];
   }
   __syncthreads();
-  T *res = sm + res_off_s;
+  // down: smooth from zero, residual (into b), restriction
   for (int q = 0; q + 1 < nb; ++q) {
-    const BottomLevel &L = bl[q];
-    T *u = sm + L.off_u;
-    const T *b = sm + L.off_b;
-    const unsigned char *c = smem + L.off_c;
-    const int n = L.ny * L.nx;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) u[k] = T(0);
-    __syncthreads();
+    const LevelInfo &L = a.lv[I.bottom + q];
+    const LevelInfo &C = a.lv[I.bottom + q + 1];
+    T *u = reinterpret_cast<T *>(smem + L.sm_u);
+    T *b = reinterpret_cast<T *>(smem + L.sm_b);
+    const unsigned char *c = smem + L.sm_c;
+    const int px = L.sm_px;
     for (int s = 0; s < S1; ++s) {
-      bottom_smooth(u, b, c, L, tdinv[q], 0);
-      bottom_smooth(u, b, c, L, tdinv[q], 1);
+      bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 0);
+      bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 1);
     }
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int y = k / L.nx, x = k - y * L.nx;
-      const int cl = c[k];
-      const T nbs = sm_at(u, y - 1, x, L.ny, L.nx) + sm_at(u, y + 1, x, L.ny, L.nx) +
-                    sm_at(u, y, x - 1, L.ny, L.nx) + sm_at(u, y, x + 1, L.ny, L.nx);
-      res[k] = cl ? b[k] - (tdiag[q][cl] * u[k] - nbs) : T(0);
-    }
-    __syncthreads();
-    const BottomLevel &Cl = bl[q + 1];
-    T *bc = sm + Cl.off_b;
-    const unsigned char *cc = smem + Cl.off_c;
-    const bool neu = L.bc == BC_NEU;
-    for (int k = threadIdx.x; k < Cl.ny * Cl.nx; k += blockDim.x) {
-      const int Iy = k / Cl.nx, Jx = k - Iy * Cl.nx;
-      T acc = T(0);
-      if (cc[k]) {
-        for (int p = 0; p < 4; ++p) {
-          const int fy = mirror_fine(2 * Iy - 1 + p, L.ny, neu);
-          T row = T(0);
-          for (int r = 0; r < 4; ++r) {
-            const int fx = mirror_fine(2 * Jx - 1 + r, L.nx, neu);
-            row += (T)rweight(r) * sm_at(res, fy, fx, L.ny, L.nx);
-          }
-          acc += (T)rweight(p) * row;
-        }
+    for (int y = warp; y < L.ny; y += NW) {
+      const int row = (y + 1) * px + 1;
+      for (int x = lane; x < L.nx; x += 32) {
+        const int i = row + x;
+        const int cl = c[i];
+        const T nbs = u[i - px] + u[i + px] + u[i - 1] + u[i + 1];
+        b[i] = cl ? b[i] - (tdiag[q][cl] * u[i] - nbs) : T(0);
       }
-      bc[k] = acc;
     }
     __syncthreads();
-  }
-  {  // coarsest: dense FP64 inverse
-    const BottomLevel &L = bl[nb - 1];
-    const int n = L.ny * L.nx;
-    double *bd = reinterpret_cast<double *>(sm + dense_off_s);
-    const T *b = sm + L.off_b;
-    T *u = sm + L.off_u;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) bd[k] = (double)b[k];
-    __syncthreads();
-    const double *inv = a.dense + a.lv[I.coarsest].inv_off;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      double acc = 0.0;
-      for (int j = 0; j < n; ++j) acc += inv[(long long)t * n + j] * bd[j];
-      u[t] = (T)acc;
-    }
-    __syncthreads();
-  }
-  for (int q = nb - 2; q >= 0; --q) {
-    const BottomLevel &L = bl[q];
-    const BottomLevel &Cl = bl[q + 1];
-    T *u = sm + L.off_u;
-    const T *b = sm + L.off_b;
-    const T *e = sm + Cl.off_u;
-    const unsigned char *c = smem + L.off_c;
+    T *bc = reinterpret_cast<T *>(smem + C.sm_b);
+    const unsigned char *cc = smem + C.sm_c;
+    T *Bg = a.arena + C.b_off;
     const bool neu = L.bc == BC_NEU;
-    for (int k = threadIdx.x; k < L.ny * L.nx; k += blockDim.x) {
-      if (!c[k]) continue;
-      const int y = k / L.nx, x = k - y * L.nx;
-      const int cy = y >> 1, cx = x >> 1;
-      const int cy2 = (y & 1) ? cy + 1 : cy - 1, cx2 = (x & 1) ? cx + 1 : cx - 1;
-      auto E = [&](int yy, int xx) -> T {
-        if (neu) {
-          yy = min(max(yy, 0), Cl.ny - 1);
-          xx = min(max(xx, 0), Cl.nx - 1);
-          return e[yy * Cl.nx + xx];
+    const int cpx = C.sm_px;
+    for (int Iy = warp; Iy < C.ny; Iy += NW) {
+      int fy[4];
+#pragma unroll
+      for (int pp = 0; pp < 4; ++pp) fy[pp] = (bot_mirror(2 * Iy - 1 + pp, L.ny, neu) + 1) * px + 1;
+      for (int Jx = lane; Jx < C.nx; Jx += 32) {
+        const int ci = (Iy + 1) * cpx + 1 + Jx;
+        T acc = T(0);
+        if (cc[ci]) {
+          int fx[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) fx[r] = bot_mirror(2 * Jx - 1 + r, L.nx, neu);
+#pragma unroll
+          for (int pp = 0; pp < 4; ++pp) {
+            T rowv = T(0);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) rowv += (T)rweight(r) * b[fy[pp] + fx[r]];
+            acc += (T)rweight(pp) * rowv;
+          }
         }
-        return sm_at(e, yy, xx, Cl.ny, Cl.nx);
-      };
-      u[k] += (T)0.5625 * E(cy, cx) + (T)0.1875 * (E(cy2, cx) + E(cy, cx2)) +
-              (T)0.0625 * E(cy2, cx2);
+        bc[ci] = acc;
+        Bg[(long long)Iy * C.pitch + Jx] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  {  // coarsest: dense FP64 inverse, one warp per row
+    const LevelInfo &L = a.lv[I.coarsest];
+    const int n = L.ny * L.nx;
+    const int px = L.sm_px;
+    double *bd = reinterpret_cast<double *>(smem + L.sm_d);
+    const T *b = reinterpret_cast<const T *>(smem + L.sm_b);
+    T *u = reinterpret_cast<T *>(smem + L.sm_u);
+    for (int k = threadIdx.x; k < n; k += kBThreads) {
+      const int y = k / L.nx, x = k - y * L.nx;
+      bd[k] = (double)b[(y + 1) * px + 1 + x];
+    }
+    __syncthreads();
+    const double *inv = a.dense + L.inv_off;
+    for (int t = warp; t < n; t += NW) {
+      double acc = 0.0;
+      for (int j = lane; j < n; j += 32) acc += inv[(long long)t * n + j] * bd[j];
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        const int y = t / L.nx, x = t - y * L.nx;
+        u[(y + 1) * px + 1 + x] = (T)acc;
+      }
+    }
+    __syncthreads();
+  }
+  // up: reload b, add the prolonged correction, post-smooth
+  for (int q = nb - 2; q >= 0; --q) {
+    const LevelInfo &L = a.lv[I.bottom + q];
+    const LevelInfo &C = a.lv[I.bottom + q + 1];
+    T *u = reinterpret_cast<T *>(smem + L.sm_u);
+    T *b = reinterpret_cast<T *>(smem + L.sm_b);
+    const T *e = reinterpret_cast<const T *>(smem + C.sm_u);
+    const unsigned char *c = smem + L.sm_c;
+    const T *Bg = a.arena + L.b_off;
+    const bool neu = L.bc == BC_NEU;
+    const int px = L.sm_px, cpx = C.sm_px;
+    for (int y = warp; y < L.ny; y += NW) {
+      const int row = (y + 1) * px + 1;
+      const int cy = y >> 1;
+      int cy2 = (y & 1) ? cy + 1 : cy - 1;
+      if (neu) cy2 = min(max(cy2, 0), C.ny - 1);
+      const int r1 = (cy + 1) * cpx + 1, r2 = (cy2 + 1) * cpx + 1;
+      for (int x = lane; x < L.nx; x += 32) {
+        const int i = row + x;
+        b[i] = Bg[(long long)y * L.pitch + x];
+        if (!c[i]) continue;
+        const int cx = x >> 1;
+        int cx2 = (x & 1) ? cx + 1 : cx - 1;
+        if (neu) cx2 = min(max(cx2, 0), C.nx - 1);
+        u[i] += (T)0.5625 * e[r1 + cx] + (T)0.1875 * (e[r2 + cx] + e[r1 + cx2]) +
+                (T)0.0625 * e[r2 + cx2];
+      }
     }
     __syncthreads();
     for (int s = 0; s < S2; ++s) {
-      bottom_smooth(u, b, c, L, tdinv[q], 1);
-      bottom_smooth(u, b, c, L, tdinv[q], 0);
+      bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 1);
+      bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 0);
     }
   }
   const LevelInfo &L0 = a.lv[I.bottom];
   T *U = a.arena + L0.u_off;
-  const T *u0 = sm + bl[0].off_u;
-  const T *b0 = sm + bl[0].off_b;
+  const T *u0 = reinterpret_cast<const T *>(smem + L0.sm_u);
+  const T *b0 = reinterpret_cast<const T *>(smem + L0.sm_b);
   double part = 0.0;
-  for (int k = threadIdx.x; k < L0.ny * L0.nx; k += blockDim.x) {
-    const int y = k / L0.nx, x = k - y * L0.nx;
-    U[(long long)y * L0.pitch + x] = u0[k];
-    part += (double)b0[k] * (double)u0[k];
+  for (int y = warp; y < L0.ny; y += NW) {
+    const int row = (y + 1) * L0.sm_px + 1;
+    for (int x = lane; x < L0.nx; x += 32) {
+      const T v = u0[row + x];
+      U[(long long)y * L0.pitch + x] = v;
+      part += (double)b0[row + x] * (double)v;
+    }
   }
   if (I.bottom == I.level0) {
     part = block_sum<kBThreads>(part);

@@ -36,13 +36,15 @@ class SolveParams:
     reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
     check_every: int = 4          # host poll interval of solves on direct launches
     use_graph: bool = True        # from a plan's second solve on: one graph, device-side loop
-    strip_target_warps: int = 1200  # smoother strip height: warps wanted per level
+    strip_target_warps: int = 600   # smoother strip height: warps wanted per level
+    bottom_cells: int = 0         # largest level solved inside the one-CTA bottom (0 = 4096)
 
     def c_params(self) -> _lib.Params:
         return _lib.Params(GD_FP64 if self.precision == "fp64" else GD_MIXED, self.sweeps,
                            self.sweeps, int(self.max_iterations), float(self.tolerance),
                            float(self.reliable_delta), int(self.check_every),
-                           1 if self.use_graph else 0, int(self.strip_target_warps), 0)
+                           1 if self.use_graph else 0, int(self.strip_target_warps),
+                           int(self.bottom_cells))
 
 
 @dataclass(frozen=True)

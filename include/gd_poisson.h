@@ -73,8 +73,8 @@ typedef struct gd_params {
   int32_t check_every;    /* host poll interval of solves on direct launches         */
   int32_t use_graph;      /* from a plan's second solve on, run the whole solve as   *
                            * one CUDA graph whose while node loops on the device     */
-  int32_t strip_target_warps; /* smoother strips: warps wanted per level (0 = 1200) */
-  int32_t reserved;
+  int32_t strip_target_warps; /* smoother strips: warps wanted per level (0 = 600)  */
+  int32_t bottom_cells;       /* largest level the one-CTA bottom takes (0 = 4096)   */
 } gd_params;
 
 typedef struct gd_report {

@@ -113,6 +113,26 @@ def test_fp32_vcycle_matches_model(sweeps):
         assert _rel(z, ref) < 2e-5
 
 
+@pytest.mark.parametrize("bottom_cells", [64, 1024, 16384])
+def test_bottom_sizes_give_the_same_vcycle(bottom_cells):
+    """Whichever level the one-CTA bottom starts at, the V-cycle is the same."""
+    rng = np.random.default_rng(bottom_cells)
+    yy, xx = np.mgrid[0:300, 0:260]
+    active = ((yy - 150.0) ** 2 + (xx - 130.0) ** 2 < 110.0 ** 2) & (xx % 17 != 3)
+    r = rng.standard_normal((300, 260))
+    for boundary in ("neumann", "dirichlet", "masked"):
+        mask = active if boundary == "masked" else None
+        rb = np.where(active, r, 0.0) if mask is not None else r
+        for precision, tol in (("fp64", 1e-11), ("mixed", 2e-5)):
+            plan = PoissonPlan([Instance(300, 260, boundary)],
+                               SolveParams(precision=precision, bottom_cells=bottom_cells))
+            if mask is not None:
+                plan.set_mask(0, torch.as_tensor(mask.astype(np.uint8)).cuda())
+            z = plan.apply_vcycle(0, torch.as_tensor(rb)).cpu().numpy()
+            ref = M.vcycle(M.build_levels(rb.shape, boundary, mask), rb, sweeps=2)
+            assert _rel(z, ref) < tol, (boundary, precision)
+
+
 def test_masked_vcycle_matches_model():
     rng = np.random.default_rng(7)
     yy, xx = np.mgrid[0:300, 0:260]
