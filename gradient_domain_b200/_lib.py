@@ -42,7 +42,8 @@ class Params(C.Structure):
                 ("post_sweeps", C.c_int32), ("max_iterations", C.c_int32),
                 ("tolerance", C.c_double), ("reliable_delta", C.c_double),
                 ("check_every", C.c_int32), ("use_graph", C.c_int32),
-                ("strip_target_warps", C.c_int32), ("bottom_cells", C.c_int32)]
+                ("strip_target_warps", C.c_int32), ("bottom_cells", C.c_int32),
+                ("tile_cells", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Report(C.Structure):

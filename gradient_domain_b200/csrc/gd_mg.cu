@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "gd_stream.cuh"
+#include "gd_tile.cuh"
 
 using namespace gd;
 
@@ -34,7 +35,8 @@ struct gd_plan_s {
   std::vector<LevelInfo> lv;
   std::vector<Tile> tiles;
   int fine_base = 0, fine_count = 0, depth = 0;
-  std::vector<int> down_base, down_count, up_base, up_count;
+  std::vector<int> down_base, down_count, up_base, up_count;     // strip maps per level
+  std::vector<int> tdown_base, tdown_count, tup_base, tup_count;  // tile maps per level
   size_t arena_elems = 0, code_bytes = 0, dense_elems = 0;
   int max_partials = 1;
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
@@ -62,6 +64,7 @@ struct gd_plan_s {
   double prof_cells[GD_KERNEL_KINDS] = {0};
   long long prof_launches[GD_KERNEL_KINDS] = {0};
   std::vector<double> launch_cells;  // fine cells covered by each launch map
+  std::vector<double> tile_cells;    // cells covered by the tile maps of each level
   double fine_cells = 0;
 };
 
@@ -188,6 +191,10 @@ struct Runner {
                          lvl);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          lvl);
+    cudaFuncSetAttribute(tile::k_down_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tile::DownT<T, S>::smem);
+    cudaFuncSetAttribute(tile::k_up_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)tile::UpT<T, S>::smem);
     cudaFuncSetAttribute(st::k_pupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)st::pupdate_smem<T>());
     cudaFuncSetAttribute(st::k_cgupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -222,16 +229,29 @@ struct Runner {
   template <int S>
   static void vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
     for (int l = 0; l < p->depth; ++l) {
-      if (p->down_count[l] <= 0) continue;
-      prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
-      st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-          at_tiles(a, p->down_base[l]));
-      prof_end(p, st);
+      if (p->down_count[l] > 0) {
+        prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
+        st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+            at_tiles(a, p->down_base[l]));
+        prof_end(p, st);
+      }
+      if (p->tdown_count[l] > 0) {
+        prof_begin(p, GD_K_DOWN, p->tile_cells[l], st);
+        tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
+            at_tiles(a, p->tdown_base[l]));
+        prof_end(p, st);
+      }
     }
     prof_begin(p, GD_K_BOTTOM, 0.0, st);
     k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
     prof_end(p, st);
     for (int l = p->depth - 1; l >= 0; --l) {
+      if (p->tup_count[l] > 0) {
+        prof_begin(p, GD_K_UP, p->tile_cells[l], st);
+        tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
+            at_tiles(a, p->tup_base[l]));
+        prof_end(p, st);
+      }
       if (p->up_count[l] <= 0) continue;
       prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
       if (l == 0)
@@ -475,10 +495,35 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   p->down_count.assign(p->depth, 0);
   p->up_base.assign(p->depth, 0);
   p->up_count.assign(p->depth, 0);
+  p->tdown_base.assign(p->depth, 0);
+  p->tdown_count.assign(p->depth, 0);
+  p->tup_base.assign(p->depth, 0);
+  p->tup_count.assign(p->depth, 0);
+  p->tile_cells.assign(std::max(p->depth, 1), 0.0);
+  // coarse levels up to tile_max cells run on the shared-memory tile kernels
+  const long long tile_max = p->prm.tile_cells > 0 ? p->prm.tile_cells : kTileCells;
+  auto on_tiles = [&](int i, int l) {
+    const LevelInfo &F = p->lv[p->inst[i].level0 + l];
+    return l >= 1 && (long long)F.ny * F.nx <= tile_max;
+  };
+  for (int l = 1; l < p->depth; ++l) {
+    p->tdown_base[l] = (int)p->tiles.size();
+    for (int i = 0; i < p->n; ++i) {
+      if (bottoms[i] <= l || !on_tiles(i, l)) continue;
+      const LevelInfo &F = p->lv[p->inst[i].level0 + l];
+      for (int ty = 0; ty < ceil_div(F.ny, tile::kTY); ++ty)
+        for (int tx = 0; tx < ceil_div(F.nx, tile::kTX); ++tx)
+          p->tiles.push_back(Tile{p->inst[i].level0 + l, i, ty, tx});
+      p->tile_cells[l] += (double)F.ny * F.nx;
+    }
+    p->tdown_count[l] = (int)p->tiles.size() - p->tdown_base[l];
+    p->tup_base[l] = p->tdown_base[l];  // the up kernel uses the same tiles
+    p->tup_count[l] = p->tdown_count[l];
+  }
   for (int l = 0; l < p->depth; ++l) {
     p->down_base[l] = (int)p->tiles.size();
     for (int i = 0; i < p->n; ++i) {
-      if (bottoms[i] <= l) continue;
+      if (bottoms[i] <= l || on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[p->inst[i].level0 + l];
       const int rows = st::kWarps * F.rows_per_warp;
       for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
@@ -491,7 +536,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     p->up_base[l] = (int)p->tiles.size();
     for (int i = 0; i < p->n; ++i) {
       InstInfo &I = p->inst[i];
-      if (bottoms[i] <= l) continue;
+      if (bottoms[i] <= l || on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[I.level0 + l];
       const int rows = st::kWarps * F.rows_per_warp;
       if (l == 0) I.up0_begin = (int)p->tiles.size() - p->up_base[0];
@@ -509,6 +554,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     const InstInfo &I = p->inst[i];
     p->fine_cells += (double)I.ny * I.nx;
     for (int l = 0; l < bottoms[i]; ++l) {
+      if (on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[I.level0 + l];
       p->launch_cells[2 * l] += (double)F.ny * F.nx;
       p->launch_cells[2 * l + 1] += (double)F.ny * F.nx;
@@ -557,7 +603,8 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
              GD_ERR_UNSUPPORTED, "gd_plan_create: pre_sweeps == post_sweeps in 1..3 required");
   GD_REQUIRE(params->precision == GD_MIXED || params->precision == GD_FP64, GD_ERR_ARG,
              "gd_plan_create: unknown precision %d", params->precision);
-  GD_REQUIRE(params->bottom_cells >= 0, GD_ERR_ARG, "gd_plan_create: negative bottom_cells");
+  GD_REQUIRE(params->bottom_cells >= 0 && params->tile_cells >= 0, GD_ERR_ARG,
+             "gd_plan_create: negative bottom_cells / tile_cells");
   GD_REQUIRE(params->max_iterations >= 0 && params->tolerance >= 0.0, GD_ERR_ARG,
              "gd_plan_create: bad tolerance / iteration budget");
   for (int i = 0; i < n; ++i) {
@@ -803,7 +850,9 @@ int enqueue_solve(gd_plan p, cudaStream_t st) {
     GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact, p->ws + p->o_nact, sizeof(int),
                                   cudaMemcpyDeviceToHost, st));
     GD_CHECK_CUDA(cudaStreamSynchronize(st));
-    const int chunk = p->prm.check_every;
+    // profiled solves poll every iteration, so that no launch is timed after
+    // the last instance stopped (its kernels would return at once)
+    const int chunk = p->profiling ? 1 : p->prm.check_every;
     const long long cap_iters = loop_cap(p);
     long long done = 0;
     while (*p->h_nact > 0 && done < cap_iters) {

@@ -15,6 +15,9 @@ constexpr int kCoarsestCells = 64;
 constexpr int kBottomCells = 4096;
 constexpr int kBottomSmem = 220 * 1024;
 constexpr int kBottomLevels = 24;  // most levels one bottom holds
+// Coarse levels (below level 0, above the bottom) with at most kTileCells
+// cells run on the shared-memory tile kernels; larger ones on the strips.
+constexpr int kTileCells = 1 << 18;
 
 // Fine-level (level 0) kernels: 64 rows x 128 columns per CTA of 128 threads
 // (four warps, each 16 rows x 128 columns).  Down / up kernels use the same

@@ -75,6 +75,8 @@ typedef struct gd_params {
                            * one CUDA graph whose while node loops on the device     */
   int32_t strip_target_warps; /* smoother strips: warps wanted per level (0 = 600)  */
   int32_t bottom_cells;       /* largest level the one-CTA bottom takes (0 = 4096)   */
+  int32_t tile_cells;         /* largest coarse level on shared-memory tiles (0 = 262144) */
+  int32_t reserved;
 } gd_params;
 
 typedef struct gd_report {

@@ -133,6 +133,27 @@ def test_bottom_sizes_give_the_same_vcycle(bottom_cells):
             assert _rel(z, ref) < tol, (boundary, precision)
 
 
+@pytest.mark.parametrize("tile_cells,sweeps", [(1, 2), (1 << 30, 1), (1 << 30, 2), (1 << 30, 3)])
+def test_tile_and_strip_levels_give_the_same_vcycle(tile_cells, sweeps):
+    """Coarse levels on the shared-memory tile kernels or on the strips: same V-cycle."""
+    rng = np.random.default_rng(sweeps)
+    yy, xx = np.mgrid[0:520, 0:300]
+    active = ((yy - 260.0) ** 2 + (xx - 150.0) ** 2 < 140.0 ** 2) & (xx % 13 != 5)
+    r = rng.standard_normal((520, 300))
+    for boundary in ("neumann", "dirichlet", "masked"):
+        mask = active if boundary == "masked" else None
+        rb = np.where(active, r, 0.0) if mask is not None else r
+        for precision, tol in (("fp64", 1e-11), ("mixed", 2e-5)):
+            plan = PoissonPlan([Instance(520, 300, boundary)],
+                               SolveParams(precision=precision, sweeps=sweeps,
+                                           tile_cells=tile_cells))
+            if mask is not None:
+                plan.set_mask(0, torch.as_tensor(mask.astype(np.uint8)).cuda())
+            z = plan.apply_vcycle(0, torch.as_tensor(rb)).cpu().numpy()
+            ref = M.vcycle(M.build_levels(rb.shape, boundary, mask), rb, sweeps=sweeps)
+            assert _rel(z, ref) < tol, (boundary, precision)
+
+
 def test_masked_vcycle_matches_model():
     rng = np.random.default_rng(7)
     yy, xx = np.mgrid[0:300, 0:260]
