@@ -1,4 +1,4 @@
-// Shared-memory tile kernels for the small coarse levels of the V-cycle.
+// Shared-memory tile kernels for the coarse levels of the V-cycle.
 //
 // The register-streaming kernels of gd_stream.cuh walk every strip row by row;
 // on a small level a launch has too few strips to fill the GPU and each warp
@@ -7,39 +7,46 @@
 // halo into shared memory and runs every phase (a red-black half sweep, the
 // residual, the restriction or the prolongation) over the whole tile at once,
 // with a barrier between phases: all cells of a phase are independent, so the
-// CTA's threads work in parallel and a small level costs a few microseconds.
+// CTA's threads work in parallel.
 //
-// Tiles are kTY x kTX cells of the level.  A half sweep that reads neighbours
-// leaves the outermost exact ring of the loaded region one cell further in, so
-// the down kernel (whose first half sweep, from zero, reads only b) loads a
-// halo of 2 S1 + 1 cells (2 S1 - 1 for the sweeps, one for the residual's
-// neighbours, one for the restriction's reach) and the up kernel 2 S2.  Cells
-// outside the grid have class 0: they hold zeros and are never updated, which
-// is the operator's definition of a missing neighbour.
+// A thread works on groups of four consecutive cells of a row (one 16-byte
+// shared-memory access per array, the four cell classes in one word); region
+// rows start on 16-byte boundaries because the horizontal halo is kHX = 8
+// cells and tiles start on multiples of kTX.  A half sweep that reads
+// neighbours leaves the outermost exact ring of the loaded region one cell
+// further in, so the down kernel (whose first half sweep, from zero, reads
+// only b and is applied while loading) needs 2 S1 + 1 halo rows (2 S1 - 1 for
+// the sweeps, one for the residual's neighbours, one for the restriction's
+// reach) and the up kernel 2 S2; kHX covers both in x for up to 3 sweeps.
+// Cells outside the grid have class 0: they hold zeros and are never updated,
+// which is the operator's definition of a missing neighbour.
 #pragma once
 
-#include "gd_mg_kernels.cuh"
+#include "gd_stream.cuh"
 
 namespace gd {
 namespace tile {
 
 constexpr int kTY = 32, kTX = 64;  // cells of a tile (even: whole coarse cells)
+constexpr int kHX = 8;             // halo columns on each side
 constexpr int kThreads = 256;
 
 template <typename T, int S1>
 struct DownT {
   static constexpr int H = 2 * S1 + 1;
-  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * H, N = RY * RX;
+  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * kHX, N = RY * RX, GX = RX / 4;
   static constexpr size_t smem = (size_t)N * (2 * sizeof(T) + 1) + 16;
 };
 
 template <typename T, int S2>
 struct UpT {
   static constexpr int H = 2 * S2;
-  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * H, N = RY * RX;
+  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * kHX, N = RY * RX, GX = RX / 4;
   static constexpr int CY = RY / 2 + 3, CX = RX / 2 + 3, CN = CY * CX;
   static constexpr size_t smem = (size_t)(2 * N + CN) * sizeof(T) + N + 16;
 };
+
+static_assert(kHX % 4 == 0 && kTX % 4 == 0 && kHX >= 7, "tile geometry");
 
 template <typename T>
 __device__ __forceinline__ void diag_tables(T *tdiag, T *tdinv, float wall) {
@@ -51,33 +58,72 @@ __device__ __forceinline__ void diag_tables(T *tdiag, T *tdinv, float wall) {
   }
 }
 
-// One red-black half sweep over the interior of an RY x RX region whose
-// corner is grid cell (gy0, gx0); colour is the parity of (row + column).
-// The cells of one colour only read cells of the other, so each thread first
-// gathers the operands of all its cells and then writes them: the shared-memory
-// loads of different cells overlap instead of waiting behind earlier stores.
+// Cells x .. x + 3 of row y (x a multiple of 4), zero outside the grid.
+template <typename T>
+__device__ __forceinline__ st::V4<T> load_group(const T *A, const LevelInfo &L, int y, int x) {
+  if (y < 0 || y >= L.ny || x < 0 || x >= L.nx) return st::zero4<T>();
+  const T *p = A + (long long)y * L.pitch + x;
+  if (x + 3 < L.nx) return st::ld4(p);
+  st::V4<T> r;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) r.v[j] = (x + j < L.nx) ? p[j] : T(0);
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_group(T *A, const LevelInfo &L, int y, int x,
+                                            const st::V4<T> &v) {
+  if (y >= L.ny || x >= L.nx) return;
+  T *p = A + (long long)y * L.pitch + x;
+  if (x + 3 < L.nx) {
+    st::st4(p, v);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (x + j < L.nx) p[j] = v.v[j];
+  }
+}
+
+// One red-black half sweep over the interior rows of an RY x RX region;
+// `par0` is the parity of the region corner's grid coordinates.  A cell of one
+// colour only reads cells of the other, so every thread gathers the operands
+// of all its groups before it writes: the loads of different groups overlap.
 template <typename T, int RY, int RX>
-__device__ __forceinline__ void tsweep(T *u, const T *b, const unsigned char *c, const T *dinv,
-                                       int colour, int gy0, int gx0) {
-  constexpr int HX = (RX - 1) / 2;  // cells of one colour in a row interior, at most
-  constexpr int M = (RY - 2) * HX;
-  constexpr int IT = (M + kThreads - 1) / kThreads;
-  int idx[IT];
-  T val[IT];
+__device__ __forceinline__ void tsweep(T *u, const T *b, const unsigned *c, const T *dinv,
+                                       int colour, int par0) {
+  constexpr int GX = RX / 4, M = (RY - 2) * GX, IT = (M + kThreads - 1) / kThreads;
+  int at[IT];
+  T v0[IT], v1[IT];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
-    const int k = threadIdx.x + it * kThreads;
-    const int ry = 1 + k / HX;
-    const int j = k - (ry - 1) * HX;
-    const int rx = 1 + 2 * j + ((colour + gy0 + gx0 + ry + 1) & 1);
-    const int i = ry * RX + rx;
-    const int cl = (k < M && rx < RX - 1) ? c[i] : 0;
-    idx[it] = cl ? i : -1;
-    val[it] = cl ? (b[i] + u[i - RX] + u[i + RX] + u[i - 1] + u[i + 1]) * dinv[cl] : T(0);
+    const int g = threadIdx.x + it * kThreads;
+    at[it] = -1;
+    if (g < M) {
+      const int ry = 1 + g / GX, gx = g - (ry - 1) * GX;
+      const int i = ry * RX + 4 * gx;
+      const st::V4<T> uc = st::ld4(u + i), up = st::ld4(u + i - RX), dn = st::ld4(u + i + RX);
+      const st::V4<T> bb = st::ld4(b + i);
+      const unsigned cl = c[g + GX];
+      if (((colour + par0 + ry) & 1) == 0) {
+        const T left = gx > 0 ? u[i - 1] : T(0);
+        v0[it] = (bb.v[0] + up.v[0] + dn.v[0] + left + uc.v[1]) * dinv[st::cls(cl, 0)];
+        v1[it] = (bb.v[2] + up.v[2] + dn.v[2] + uc.v[1] + uc.v[3]) * dinv[st::cls(cl, 2)];
+        at[it] = i;
+      } else {
+        const T right = gx < GX - 1 ? u[i + 4] : T(0);
+        v0[it] = (bb.v[1] + up.v[1] + dn.v[1] + uc.v[0] + uc.v[2]) * dinv[st::cls(cl, 1)];
+        v1[it] = (bb.v[3] + up.v[3] + dn.v[3] + uc.v[2] + right) * dinv[st::cls(cl, 3)];
+        at[it] = i + 1;
+      }
+    }
   }
 #pragma unroll
-  for (int it = 0; it < IT; ++it)
-    if (idx[it] >= 0) u[idx[it]] = val[it];
+  for (int it = 0; it < IT; ++it) {
+    if (at[it] >= 0) {
+      u[at[it]] = v0[it];
+      u[at[it] + 2] = v1[it];
+    }
+  }
   __syncthreads();
 }
 
@@ -96,7 +142,7 @@ __device__ __forceinline__ int tmirror(int f, int n, bool neu) {
 template <typename T, int S1>
 __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
   using G = DownT<T, S1>;
-  constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N;
+  constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX;
   const Tile tl = a.tiles[blockIdx.x];
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   const LevelInfo L = a.lv[tl.level];
@@ -104,71 +150,87 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
   extern __shared__ __align__(16) unsigned char smem[];
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
-  unsigned char *sc = reinterpret_cast<unsigned char *>(su + N);
+  unsigned *sc = reinterpret_cast<unsigned *>(su + N);
   __shared__ T tdiag[8], tdinv[8];
   diag_tables(tdiag, tdinv, L.wall);
   __syncthreads();
   const int y0 = tl.ty * kTY, x0 = tl.tx * kTX;
-  const int gy0 = y0 - H, gx0 = x0 - H;
-  const T *B = a.arena + L.b_off;
-  // load, with the first half sweep (colour 0 from zero reads only b) applied
-  // on the whole region, its outermost ring included; every load of a thread
-  // is issued before the first is used
-  {
-    constexpr int IT = (N + kThreads - 1) / kThreads;
-    T bv[IT];
-    int cl[IT];
+  const int gy0 = y0 - H, gx0 = x0 - kHX;
+  const int par0 = (gy0 + gx0) & 1;
+  {  // load, applying the first half sweep (colour 0 from zero: u = b / d)
+    const T *B = a.arena + L.b_off;
+    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    st::V4<T> bv[IT];
+    unsigned cv[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      const int ry = k / RX, rx = k - ry * RX;
-      const int y = gy0 + ry, x = gx0 + rx;
-      const bool in = k < N && y >= 0 && y < L.ny && x >= 0 && x < L.nx;
-      bv[it] = in ? B[(long long)y * L.pitch + x] : T(0);
-      cl[it] = in ? cell_class(L, a.codes, y, x) : 0;
+      const int g = threadIdx.x + it * kThreads;
+      const int ry = g / GX, gx = g - ry * GX;
+      const int y = gy0 + ry, x = gx0 + 4 * gx;
+      bv[it] = g < NG ? load_group(B, L, y, x) : st::zero4<T>();
+      cv[it] = g < NG ? st::row_classes(L, a.codes, y, x) : 0u;
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      if (k >= N) break;
-      const int ry = k / RX, rx = k - ry * RX;
-      sb[k] = bv[it];
-      su[k] = ((gy0 + ry + gx0 + rx) & 1) == 0 ? bv[it] * tdinv[cl[it]] : T(0);
-      sc[k] = (unsigned char)cl[it];
+      const int g = threadIdx.x + it * kThreads;
+      if (g >= NG) break;
+      const int ry = g / GX;
+      const int p = (par0 + ry) & 1;  // cells j with (j & 1) == p have colour 0
+      st::V4<T> u0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        u0.v[j] = ((j & 1) == p) ? bv[it].v[j] * tdinv[st::cls(cv[it], j)] : T(0);
+      st::st4(sb + 4 * g, bv[it]);  // RX = 4 GX: group g starts at cell 4 g
+      st::st4(su + 4 * g, u0);
+      sc[g] = cv[it];
     }
   }
   __syncthreads();
-  tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, gy0, gx0);
+  tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
   for (int s = 1; s < S1; ++s) {
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, gy0, gx0);
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, gy0, gx0);
+    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, par0);
+    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
   }
-  T *W = a.arena + L.w_off;
-  for (int k = threadIdx.x; k < kTY * kTX; k += kThreads) {
-    const int ty = k / kTX, tx = k - ty * kTX;
-    const int y = y0 + ty, x = x0 + tx;
-    if (y < L.ny && x < L.nx) W[(long long)y * L.pitch + x] = su[(ty + H) * RX + tx + H];
+  {  // the pre-smoothed iterate of the tile, for the up kernel
+    T *W = a.arena + L.w_off;
+    constexpr int TG = kTX / 4, M = kTY * TG;
+    for (int g = threadIdx.x; g < M; g += kThreads) {
+      const int ty = g / TG, q = g - ty * TG;
+      store_group(W, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
+    }
   }
-  // residual on the tile plus one ring, in place into b (each cell reads only
-  // its own b and the unchanged u)
-  {
-    constexpr int QY = kTY + 2, QX = kTX + 2, M = QY * QX;
-    constexpr int IT = (M + kThreads - 1) / kThreads;
-    T val[IT];
+  {  // residual on the tile plus one ring, in place into b (groups 1 .. kTX/4 + 2)
+    constexpr int QG = kTX / 4 + 2, M = (kTY + 2) * QG, IT = (M + kThreads - 1) / kThreads;
+    st::V4<T> res[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      const int qy = k / QX, qx = k - qy * QX;
-      const int i = (qy + H - 1) * RX + (qx + H - 1);
-      const int cl = k < M ? sc[i] : 0;
-      const T nbs = cl ? su[i - RX] + su[i + RX] + su[i - 1] + su[i + 1] : T(0);
-      val[it] = cl ? sb[i] - (tdiag[cl] * su[i] - nbs) : T(0);
+      const int g = threadIdx.x + it * kThreads;
+      res[it] = st::zero4<T>();
+      if (g < M) {
+        const int qy = g / QG, q = g - qy * QG;
+        const int ry = qy + H - 1, gx = q + 1;
+        const int i = ry * RX + 4 * gx;
+        const st::V4<T> uc = st::ld4(su + i), up = st::ld4(su + i - RX),
+                        dn = st::ld4(su + i + RX), bb = st::ld4(sb + i);
+        const T left = su[i - 1], right = su[i + 4];
+        const unsigned cl = sc[ry * GX + gx];
+        const T lf[4] = {left, uc.v[0], uc.v[1], uc.v[2]};
+        const T rt[4] = {uc.v[1], uc.v[2], uc.v[3], right};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = st::cls(cl, j);
+          res[it].v[j] = k ? bb.v[j] - (tdiag[k] * uc.v[j] - (up.v[j] + dn.v[j] + lf[j] + rt[j]))
+                           : T(0);
+        }
+      }
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      const int qy = k / QX, qx = k - qy * QX;
-      if (k < M) sb[(qy + H - 1) * RX + (qx + H - 1)] = val[it];
+      const int g = threadIdx.x + it * kThreads;
+      if (g < M) {
+        const int qy = g / QG, q = g - qy * QG;
+        st::st4(sb + (qy + H - 1) * RX + 4 * (q + 1), res[it]);
+      }
     }
   }
   __syncthreads();
@@ -202,7 +264,7 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
 template <typename T, int S2>
 __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
   using G = UpT<T, S2>;
-  constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, CX = G::CX;
+  constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX, CX = G::CX;
   const Tile tl = a.tiles[blockIdx.x];
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   const LevelInfo L = a.lv[tl.level];
@@ -211,22 +273,24 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
   T *se = su + N;
-  unsigned char *sc = reinterpret_cast<unsigned char *>(se + G::CN);
+  unsigned *sc = reinterpret_cast<unsigned *>(se + G::CN);
   __shared__ T tdiag[8], tdinv[8];
   diag_tables(tdiag, tdinv, L.wall);
   const int y0 = tl.ty * kTY, x0 = tl.tx * kTX;
-  const int gy0 = y0 - H, gx0 = x0 - H;
+  const int gy0 = y0 - H, gx0 = x0 - kHX;
+  const int par0 = (gy0 + gx0) & 1;
   const bool neu = L.bc == BC_NEU;
-  // coarse correction around the region: coarse rows (gy0 >> 1) - 1 ..
+  // coarse correction around the region, from coarse row / column cy0 / cx0
   const int cy0 = (gy0 >> 1) - 1, cx0 = (gx0 >> 1) - 1;
-  const T *E = a.arena + Lc.u_off;
-  const T *B = a.arena + L.b_off;
-  const T *W = a.arena + L.w_off;
   {  // every load of a thread is issued before the first is used
+    const T *E = a.arena + Lc.u_off;
+    const T *B = a.arena + L.b_off;
+    const T *W = a.arena + L.w_off;
     constexpr int ITC = (G::CN + kThreads - 1) / kThreads;
-    constexpr int IT = (N + kThreads - 1) / kThreads;
-    T ev[ITC], bv[IT], wv[IT];
-    int cl[IT];
+    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    T ev[ITC];
+    st::V4<T> bv[IT], wv[IT];
+    unsigned cv[IT];
 #pragma unroll
     for (int it = 0; it < ITC; ++it) {
       const int k = threadIdx.x + it * kThreads;
@@ -243,13 +307,12 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      const int ry = k / RX, rx = k - ry * RX;
-      const int y = gy0 + ry, x = gx0 + rx;
-      const bool in = k < N && y >= 0 && y < L.ny && x >= 0 && x < L.nx;
-      cl[it] = in ? cell_class(L, a.codes, y, x) : 0;
-      bv[it] = in ? B[(long long)y * L.pitch + x] : T(0);
-      wv[it] = cl[it] ? W[(long long)y * L.pitch + x] : T(0);
+      const int g = threadIdx.x + it * kThreads;
+      const int ry = g / GX, gx = g - ry * GX;
+      const int y = gy0 + ry, x = gx0 + 4 * gx;
+      cv[it] = g < NG ? st::row_classes(L, a.codes, y, x) : 0u;
+      bv[it] = g < NG ? load_group(B, L, y, x) : st::zero4<T>();
+      wv[it] = g < NG ? load_group(W, L, y, x) : st::zero4<T>();
     }
 #pragma unroll
     for (int it = 0; it < ITC; ++it) {
@@ -258,46 +321,70 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      if (k >= N) break;
-      sb[k] = bv[it];
-      su[k] = wv[it];
-      sc[k] = (unsigned char)cl[it];
+      const int g = threadIdx.x + it * kThreads;
+      if (g >= NG) break;
+      st::V4<T> w = wv[it];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (!st::cls(cv[it], j)) w.v[j] = T(0);
+      st::st4(sb + 4 * g, bv[it]);  // RX = 4 GX: group g starts at cell 4 g
+      st::st4(su + 4 * g, w);
+      sc[g] = cv[it];
     }
   }
   __syncthreads();
-  {  // u += P e (each cell reads the coarse values and only its own u)
-    constexpr int IT = (N + kThreads - 1) / kThreads;
-    T val[IT];
+  {  // u += P e on cells with an unknown (each group reads the coarse values
+     // and only its own u)
+    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    st::V4<T> pe[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      val[it] = T(0);
-      if (k < N && sc[k]) {
-        const int ry = k / RX, rx = k - ry * RX;
-        const int y = gy0 + ry, x = gx0 + rx;
-        const int cy = y >> 1, cx = x >> 1;
-        const int cy2 = (y & 1) ? cy + 1 : cy - 1, cx2 = (x & 1) ? cx + 1 : cx - 1;
-        const T *r1 = se + (cy - cy0) * CX - cx0, *r2 = se + (cy2 - cy0) * CX - cx0;
-        val[it] = (T)0.5625 * r1[cx] + (T)0.1875 * (r2[cx] + r1[cx2]) + (T)0.0625 * r2[cx2];
+      const int g = threadIdx.x + it * kThreads;
+      pe[it] = st::zero4<T>();
+      const unsigned cl = g < NG ? sc[g] : 0u;
+      if (cl) {
+        const int ry = g / GX, gx = g - ry * GX;
+        const int y = gy0 + ry;
+        const int cy = y >> 1, cy2 = (y & 1) ? cy + 1 : cy - 1;
+        // coarse columns x/2 - 1 .. x/2 + 2 of rows cy and cy2 (x = gx0 + 4 gx)
+        const T *r1 = se + (cy - cy0) * CX + 2 * gx;
+        const T *r2 = se + (cy2 - cy0) * CX + 2 * gx;
+        T e1[4], e2[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          e1[k] = r1[k];
+          e2[k] = r2[k];
+        }
+        const T v[4] = {
+            (T)0.5625 * e1[1] + (T)0.1875 * (e2[1] + e1[0]) + (T)0.0625 * e2[0],
+            (T)0.5625 * e1[1] + (T)0.1875 * (e2[1] + e1[2]) + (T)0.0625 * e2[2],
+            (T)0.5625 * e1[2] + (T)0.1875 * (e2[2] + e1[1]) + (T)0.0625 * e2[1],
+            (T)0.5625 * e1[2] + (T)0.1875 * (e2[2] + e1[3]) + (T)0.0625 * e2[3]};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pe[it].v[j] = st::cls(cl, j) ? v[j] : T(0);
       }
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int k = threadIdx.x + it * kThreads;
-      if (k < N) su[k] += val[it];
+      const int g = threadIdx.x + it * kThreads;
+      if (g < NG && sc[g]) {
+        st::V4<T> u = st::ld4(su + 4 * g);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) u.v[j] += pe[it].v[j];
+        st::st4(su + 4 * g, u);
+      }
     }
   }
   __syncthreads();
   for (int s = 0; s < S2; ++s) {
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, gy0, gx0);
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, gy0, gx0);
+    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
+    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, par0);
   }
   T *U = a.arena + L.u_off;
-  for (int k = threadIdx.x; k < kTY * kTX; k += kThreads) {
-    const int ty = k / kTX, tx = k - ty * kTX;
-    const int y = y0 + ty, x = x0 + tx;
-    if (y < L.ny && x < L.nx) U[(long long)y * L.pitch + x] = su[(ty + H) * RX + tx + H];
+  constexpr int TG = kTX / 4, M = kTY * TG;
+  for (int g = threadIdx.x; g < M; g += kThreads) {
+    const int ty = g / TG, q = g - ty * TG;
+    store_group(U, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
   }
 }
 
