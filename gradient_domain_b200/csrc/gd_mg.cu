@@ -52,6 +52,8 @@ struct gd_plan_s {
   int *h_nact = nullptr;
   InstState *h_st = nullptr;
   size_t h_st_bytes = 0;
+  InstInfo *h_inst = nullptr;  // pinned staging of the per-solve instance table
+  size_t h_inst_bytes = 0;
   cudaEvent_t done_ev = nullptr;  // recorded after the states of an asynchronous solve
   bool pending = false;           // an asynchronous solve awaits gd_solve_finish
   // profiling: events around every launch (graphs are bypassed while enabled)
@@ -628,7 +630,9 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   p->h_st_bytes = sizeof(InstState) * n;
   p->h_nact = static_cast<int *>(pinned_get(sizeof(int)));
   p->h_st = static_cast<InstState *>(pinned_get(p->h_st_bytes));
-  if (!p->h_nact || !p->h_st) {
+  p->h_inst_bytes = sizeof(InstInfo) * n;
+  p->h_inst = static_cast<InstInfo *>(pinned_get(p->h_inst_bytes));
+  if (!p->h_nact || !p->h_st || !p->h_inst) {
     set_error("gd_plan_create: pinned host allocation failed");
     gd_plan_destroy(p);
     return GD_ERR_CUDA;
@@ -650,6 +654,7 @@ extern "C" void gd_plan_destroy(gd_plan p) {
   capture_stream_put(p->cap_device, p->cap);
   pinned_put(p->h_nact, sizeof(int));
   pinned_put(p->h_st, p->h_st_bytes);
+  pinned_put(p->h_inst, p->h_inst_bytes);
   delete p;
 }
 
@@ -912,9 +917,12 @@ int bind_solve(gd_plan p, const double *const *f, double *const *x, const int32_
     p->inst[i].upitch = pitch[i];
     p->inst[i].scale = scale[i];
   }
-  // pageable source: staged before the call returns, so p->inst may change afterwards
-  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->inst.data(),
-                                p->inst.size() * sizeof(InstInfo), cudaMemcpyHostToDevice, st));
+  // through pinned memory: a copy from pageable memory may wait for the work
+  // already queued on the stream, which would serialise pipelined solves; the
+  // staging buffer is not reused before this solve is finished
+  std::memcpy(p->h_inst, p->inst.data(), p->h_inst_bytes);
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->ws + p->o_inst, p->h_inst, p->h_inst_bytes,
+                                cudaMemcpyHostToDevice, st));
   return p->fp64 ? enqueue_solve<double>(p, st) : enqueue_solve<float>(p, st);
 }
 }  // namespace
