@@ -268,15 +268,18 @@ class PoissonServer:
             self._cv.notify_all()
         return fut
 
-    def warm(self, requests: list[PoissonRequest]) -> None:
-        """Solve each request once on every worker, so their plans (hierarchies,
-        device buffers, CUDA graphs) are resident before traffic arrives."""
+    def warm(self, requests: list[PoissonRequest], batch_sizes=(1,)) -> None:
+        """Solve batches of ``b`` copies of each request (for every ``b`` in
+        ``batch_sizes``) on every worker, so that the plans of the batches the
+        dispatcher will form (hierarchies, device buffers, CUDA graphs) and the
+        host and device allocations behind them exist before traffic arrives."""
         for wid in range(self.workers):
             if self._states[wid] is None:
                 self._states[wid] = self.backend.new_worker_state()
             for r in requests:
-                for _ in range(2):  # the second solve captures the plan's graph
-                    self.backend.solve(self._states[wid], [r])
+                for b in batch_sizes:
+                    for _ in range(2):  # the second solve captures the plan's graph
+                        self.backend.solve(self._states[wid], [r] * b)
 
     # -- lifecycle -----------------------------------------------------------
     def start(self):
@@ -511,7 +514,7 @@ def bench_main(args) -> None:
             r = run_load(server, pool, rate, args.requests, seed=int(rate))
             loads.append(r.__dict__)
         out["loads"] = loads
-        server.warm(one_mp[:1])
+        server.warm(one_mp[:1], batch_sizes=(1, 2, 3))
         r1 = run_load(server, one_mp, 100.0, args.requests_1mp, seed=3)
         out["one_mp"] = r1.__dict__
         # the floor: one warm worker solving 1 MP requests back to back, no queue
