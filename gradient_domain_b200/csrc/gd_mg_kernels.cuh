@@ -320,12 +320,42 @@ __global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
   const int y0 = tl.ty * kFTY;
   if (x >= nx) return;
   const int y1 = min(y0 + kFTY, ny);
-#pragma unroll 8
-  for (int y = y0; y < y1; ++y) {
-    const long long g = (long long)y * pitch + x;
-    X[(long long)y * upitch + x] += (double)d[g];
-    d[g] = T(0);
+  // eight rows at a time: every load of a chunk is issued before its stores
+  for (int yb = y0; yb < y1; yb += 8) {
+    double xv[8];
+    T dv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int y = yb + k;
+      xv[k] = y < y1 ? X[(long long)y * upitch + x] : 0.0;
+      dv[k] = y < y1 ? d[(long long)y * pitch + x] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int y = yb + k;
+      if (y < y1) {
+        X[(long long)y * upitch + x] = xv[k] + (double)dv[k];
+        d[(long long)y * pitch + x] = T(0);
+      }
+    }
   }
+}
+
+// Sum of column x over rows y0 .. y1 - 1 of an FP64 array, eight independent
+// loads in flight per thread and a fixed summation tree.
+__device__ __forceinline__ double column_sum(const double *A, long long pitch, int y0, int y1,
+                                             int x) {
+  double s[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = 0.0;
+  for (int yb = y0; yb < y1; yb += 8) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = yb + k < y1 ? A[(long long)(yb + k) * pitch + x] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[k] += v[k];
+  }
+  return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
 }
 
 // Mean of the right-hand side of zero-mean (Neumann) instances: the constant
@@ -337,11 +367,8 @@ __global__ void __launch_bounds__(kFThreads) k_fmean(Args<T> a) {
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
   if (I.zero_mean) {
-    const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
-    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-      const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
-      if (gy < I.ny && gx < I.nx) part += I.f[(long long)gy * I.upitch + gx];
-    }
+    const int Y0 = tl.ty * kFTY, gx = tl.tx * kFTX + threadIdx.x;
+    if (gx < I.nx) part = column_sum(I.f, I.upitch, Y0, min(Y0 + kFTY, I.ny), gx);
   }
   part = block_sum<kFThreads>(part);
   if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
@@ -361,11 +388,8 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
   if (I.zero_mean) {
-    const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
-    for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-      const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
-      if (gy < I.ny && gx < I.nx) part += I.x[(long long)gy * I.upitch + gx];
-    }
+    const int Y0 = tl.ty * kFTY, gx = tl.tx * kFTX + threadIdx.x;
+    if (gx < I.nx) part = column_sum(I.x, I.upitch, Y0, min(Y0 + kFTY, I.ny), gx);
   }
   part = block_sum<kFThreads>(part);
   if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
@@ -388,10 +412,16 @@ __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   const long long upitch = Ig.upitch;
   double *const X = Ig.x;
   const double m = a.st[tl.inst].mean;
-  const int Y0 = tl.ty * kFTY, X0 = tl.tx * kFTX;
-  for (int k = threadIdx.x; k < kFTY * kFTX; k += blockDim.x) {
-    const int gy = Y0 + k / kFTX, gx = X0 + k % kFTX;
-    if (gy < ny && gx < nx) X[(long long)gy * upitch + gx] -= m;
+  const int Y0 = tl.ty * kFTY, gx = tl.tx * kFTX + threadIdx.x;
+  if (gx >= nx) return;
+  const int y1 = min(Y0 + kFTY, ny);
+  for (int yb = Y0; yb < y1; yb += 8) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = yb + k < y1 ? X[(long long)(yb + k) * upitch + gx] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (yb + k < y1) X[(long long)(yb + k) * upitch + gx] = v[k] - m;
   }
 }
 

@@ -1048,28 +1048,46 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
       return klass(y, x) ? X[(long long)y * upitch + x] : 0.0;
     };
     double xu = xv(y0 - 1, col), xc = xv(y0, col);
-#pragma unroll 4
-    for (int y = y0; y < y1; ++y) {
-      const double xd = xv(y + 1, col);
-      double left = shfl_up1(xc), right = shfl_dn1(xc);
-      if (lane == 0) left = xv(y, col - 1);
-      if (lane == 31) right = xv(y, col + 1);
-      const int c = in_col ? klass(y, col) : 0;
-      if (c) {
-        const long long gu = (long long)y * upitch + col;
-        const double dg = 4.0 - (double)(c - 1) * omw;
-        const double f = scale * (Fu[gu] - fmean);
-        const double r64 = f - (dg * xc - (xu + xd + left + right));
-        r[(long long)y * L.pitch + col] = (T)r64;
-        part += r64 * r64;
-        if (INIT) part_f += f * f;
-      } else if (in_col && y < L.ny) {
-        r[(long long)y * L.pitch + col] = T(0);
-        if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
+    // CH rows at a time: the loads of a chunk (x one row ahead, f, the edge
+    // columns of lanes 0 and 31) are all issued before its stores (two rows
+    // measured best: longer chunks cost occupancy)
+    constexpr int CH = 2;
+    for (int yb = y0; yb < y1; yb += CH) {
+      double xn[CH], fv[CH], ev[CH];
+      int cl[CH];
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int y = yb + k;
+        const bool row = y < y1;
+        xn[k] = row ? xv(y + 1, col) : 0.0;
+        cl[k] = (row && in_col) ? klass(y, col) : 0;
+        fv[k] = cl[k] ? Fu[(long long)y * upitch + col] : 0.0;
+        ev[k] = !row ? 0.0 : lane == 0 ? xv(y, col - 1) : lane == 31 ? xv(y, col + 1) : 0.0;
       }
-      if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
-      xu = xc;
-      xc = xd;
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int y = yb + k;
+        if (y >= y1) break;  // the same for every lane of the warp
+        const double xd = xn[k];
+        double left = shfl_up1(xc), right = shfl_dn1(xc);
+        if (lane == 0) left = ev[k];
+        if (lane == 31) right = ev[k];
+        const int c = cl[k];
+        if (c) {
+          const double dg = 4.0 - (double)(c - 1) * omw;
+          const double f = scale * (fv[k] - fmean);
+          const double r64 = f - (dg * xc - (xu + xd + left + right));
+          r[(long long)y * L.pitch + col] = (T)r64;
+          part += r64 * r64;
+          if (INIT) part_f += f * f;
+        } else if (in_col) {
+          r[(long long)y * L.pitch + col] = T(0);
+          if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
+        }
+        if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
+        xu = xc;
+        xc = xd;
+      }
     }
   }
   part = block_sum<kThreads>(part);
