@@ -281,7 +281,7 @@ struct Runner {
     k_fold<T><<<p->fine_count, kFThreads, 0, st>>>(f);
     prof_end(p, st);
     prof_begin(p, GD_K_RESID, c, st);
-    st::k_resid_s<T, false><<<p->fine_count, st::kThreads, 0, st>>>(f);
+    st::k_resid_s<T, false><<<p->fine_count, st::kThreads, st::resid_smem<T>(), st>>>(f);
     prof_end(p, st);
   }
 
@@ -738,7 +738,7 @@ template <typename T>
 void launch_init(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
   k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  st::k_resid_s<T, true><<<p->fine_count, st::kThreads, 0, st>>>(fine);
+  st::k_resid_s<T, true><<<p->fine_count, st::kThreads, st::resid_smem<T>(), st>>>(fine);
   prof_end(p, st);
 }
 

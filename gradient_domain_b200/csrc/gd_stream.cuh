@@ -1012,14 +1012,22 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
 // the initial) iterate, its norm, and the convergence decision per instance.
 // x and f are the caller's FP64 arrays (any row pitch).  A thread owns one
 // column of the 64 x 128 tile and walks its rows with x rows y - 1, y, y + 1 in
-// registers; horizontal neighbours come from shuffles, and lanes 0 and 31 load
+// registers; horizontal neighbours come from shuffles, and lanes 0 and 31 take
 // the column just outside their warp.  Every warp access is 32 consecutive
-// elements.
+// elements.  The rows arrive through per-thread cp.async rings in shared
+// memory (x one row ahead, f, and the edge column of lanes 0 and 31),
+// kResidRing - 1 rows in flight per thread without holding registers.
+constexpr int kResidRing = 8;
+
+template <typename T>
+constexpr size_t resid_smem() { return (size_t)3 * kResidRing * kThreads * sizeof(double); }
+
 template <typename T, bool INIT>
 __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
   double part = 0.0, part_f = 0.0;
+  extern __shared__ __align__(16) unsigned char smem[];
   if (work) {
     // descriptor fields in registers: the stores below could alias the descriptor
     const InstInfo &Ig = a.inst[tl.inst];
@@ -1047,48 +1055,67 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
     auto xv = [&](int y, int x) -> double {
       return klass(y, x) ? X[(long long)y * upitch + x] : 0.0;
     };
+    // rings: slot q holds x of row y0 + 1 + q, f of row y0 + q and the edge
+    // column of row y0 + q (lane 0: col - 1, lane 31: col + 1)
+    double *const rx = reinterpret_cast<double *>(smem) + threadIdx.x;
+    double *const rf = rx + kResidRing * kThreads;
+    double *const re = rf + kResidRing * kThreads;
+    const int ecol = lane == 0 ? col - 1 : col + 1;
+    const bool edge_lane = lane == 0 || lane == 31;
+    auto issue = [&](int q) {
+      const int sl = (q & (kResidRing - 1)) * kThreads;
+      const int yx = y0 + 1 + q, yf = y0 + q;
+      const bool okx = in_col && yx < L.ny;
+      const bool okf = in_col && yf < y1;
+      __pipeline_memcpy_async(rx + sl, okx ? X + (long long)yx * upitch + col : X, 8,
+                              okx ? 0 : 8);
+      __pipeline_memcpy_async(rf + sl, okf ? Fu + (long long)yf * upitch + col : Fu, 8,
+                              okf ? 0 : 8);
+      if (edge_lane) {
+        const bool oke = yf < y1 && ecol >= 0 && ecol < L.nx;
+        __pipeline_memcpy_async(re + sl, oke ? X + (long long)yf * upitch + ecol : X, 8,
+                                oke ? 0 : 8);
+      }
+    };
     double xu = xv(y0 - 1, col), xc = xv(y0, col);
-    // CH rows at a time: the loads of a chunk (x one row ahead, f, the edge
-    // columns of lanes 0 and 31) are all issued before its stores (two rows
-    // measured best: longer chunks cost occupancy)
-    constexpr int CH = 2;
-    for (int yb = y0; yb < y1; yb += CH) {
-      double xn[CH], fv[CH], ev[CH];
-      int cl[CH];
-#pragma unroll
-      for (int k = 0; k < CH; ++k) {
-        const int y = yb + k;
-        const bool row = y < y1;
-        xn[k] = row ? xv(y + 1, col) : 0.0;
-        cl[k] = (row && in_col) ? klass(y, col) : 0;
-        fv[k] = cl[k] ? Fu[(long long)y * upitch + col] : 0.0;
-        ev[k] = !row ? 0.0 : lane == 0 ? xv(y, col - 1) : lane == 31 ? xv(y, col + 1) : 0.0;
-      }
-#pragma unroll
-      for (int k = 0; k < CH; ++k) {
-        const int y = yb + k;
-        if (y >= y1) break;  // the same for every lane of the warp
-        const double xd = xn[k];
-        double left = shfl_up1(xc), right = shfl_dn1(xc);
-        if (lane == 0) left = ev[k];
-        if (lane == 31) right = ev[k];
-        const int c = cl[k];
-        if (c) {
-          const double dg = 4.0 - (double)(c - 1) * omw;
-          const double f = scale * (fv[k] - fmean);
-          const double r64 = f - (dg * xc - (xu + xd + left + right));
-          r[(long long)y * L.pitch + col] = (T)r64;
-          part += r64 * r64;
-          if (INIT) part_f += f * f;
-        } else if (in_col) {
-          r[(long long)y * L.pitch + col] = T(0);
-          if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
-        }
-        if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
-        xu = xc;
-        xc = xd;
-      }
+    for (int q = 0; q < kResidRing - 1; ++q) {
+      issue(q);
+      __pipeline_commit();
     }
+    for (int y = y0; y < y1; ++y) {
+      const int q = y - y0;
+      __pipeline_wait_prior(kResidRing - 2);
+      const int sl = (q & (kResidRing - 1)) * kThreads;
+      double xd = rx[sl];
+      const double fraw = rf[sl];
+      const double eraw = edge_lane ? re[sl] : 0.0;
+      issue(q + kResidRing - 1);
+      __pipeline_commit();
+      double ev = eraw;
+      if (masked) {  // values of cells without an unknown read as zero
+        if (!klass(y + 1, col)) xd = 0.0;
+        if (edge_lane && !klass(y, ecol)) ev = 0.0;
+      }
+      double left = shfl_up1(xc), right = shfl_dn1(xc);
+      if (lane == 0) left = ev;
+      if (lane == 31) right = ev;
+      const int c = in_col ? klass(y, col) : 0;
+      if (c) {
+        const double dg = 4.0 - (double)(c - 1) * omw;
+        const double f = scale * (fraw - fmean);
+        const double r64 = f - (dg * xc - (xu + xd + left + right));
+        r[(long long)y * L.pitch + col] = (T)r64;
+        part += r64 * r64;
+        if (INIT) part_f += f * f;
+      } else if (in_col) {
+        r[(long long)y * L.pitch + col] = T(0);
+        if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
+      }
+      if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
+      xu = xc;
+      xc = xd;
+    }
+    __pipeline_wait_prior(0);  // no copy may land after the shared memory is released
   }
   part = block_sum<kThreads>(part);
   if (INIT) {
