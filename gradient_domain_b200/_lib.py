@@ -28,7 +28,7 @@ EXPORTS = (
     "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
-    "gd_masked_rhs",
+    "gd_masked_rhs", "gd_guidance_divergence",
 )
 
 
@@ -49,6 +49,18 @@ class Params(C.Structure):
 class Report(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("status", C.c_int32),
                 ("relative_residual", C.c_double), ("initial_norm", C.c_double)]
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("height", C.c_int32), ("width", C.c_int32),
+                ("channels", C.c_int32), ("channel", C.c_int32), ("pad", C.c_int32),
+                ("target", C.c_void_p), ("source", C.c_void_p), ("select", C.c_void_p),
+                ("weights", C.c_void_p), ("alpha_pow_beta", C.c_double), ("beta", C.c_double),
+                ("epsilon", C.c_double)]
+
+
+GD_FIELD_IMPORT, GD_FIELD_MIXED, GD_FIELD_AVERAGE, GD_FIELD_WEIGHTED, GD_FIELD_ILLUMINATION = \
+    range(5)
 
 
 class KernelTime(C.Structure):
@@ -101,6 +113,8 @@ def _declare(lib: C.CDLL) -> None:
         "gd_divergence": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_fold_dirichlet": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),
         "gd_masked_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+        "gd_guidance_divergence": (C.c_int, [_vp, C.POINTER(FieldDesc), _i32, _i32, _i32, _i32,
+                                             _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -90,6 +90,85 @@ __global__ void k_masked_rhs(double *__restrict__ f, const double *__restrict__ 
   f[k] = __dmul_rn(scale, v);
 }
 
+// Guidance fields built on the fly (poisson.py:52-92 and the field set-up of
+// seamless_clone, texture_flatten and illumination_change, poisson.py:306-431):
+// the forward-difference gradient of an interleaved (H, W, C) image channel,
+// combined per cell as the field kind says.
+struct FieldView {
+  gd_field_desc d;
+  __device__ __forceinline__ double at(const double *img, int y, int x) const {
+    return img[((long long)y * d.width + x) * d.channels + d.channel];
+  }
+  // forward differences of one image (operators.py:30-50)
+  __device__ __forceinline__ void grad(const double *img, int y, int x, double &gx,
+                                       double &gy) const {
+    const double c = at(img, y, x);
+    gx = x < d.width - 1 ? __dsub_rn(at(img, y, x + 1), c) : 0.0;
+    gy = y < d.height - 1 ? __dsub_rn(at(img, y + 1, x), c) : 0.0;
+  }
+  __device__ __forceinline__ void field(int y, int x, double &gx, double &gy) const {
+    double tx, ty;
+    grad(d.target, y, x, tx, ty);
+    switch (d.kind) {
+      case GD_FIELD_IMPORT:
+      case GD_FIELD_MIXED:
+      case GD_FIELD_AVERAGE: {
+        if (!d.select[(long long)y * d.width + x]) {  // GuidanceField.select: target outside
+          gx = tx;
+          gy = ty;
+          return;
+        }
+        double sx, sy;
+        grad(d.source, y, x, sx, sy);
+        if (d.kind == GD_FIELD_IMPORT) {
+          gx = sx;
+          gy = sy;
+        } else if (d.kind == GD_FIELD_MIXED) {  // mix_by_magnitude: the larger, source on ties
+          gx = fabs(sx) >= fabs(tx) ? sx : tx;
+          gy = fabs(sy) >= fabs(ty) ? sy : ty;
+        } else {
+          gx = __dmul_rn(0.5, __dadd_rn(sx, tx));
+          gy = __dmul_rn(0.5, __dadd_rn(sy, ty));
+        }
+        return;
+      }
+      case GD_FIELD_WEIGHTED: {  // texture_flatten: gradient times the edge weights
+        const double w = d.weights[(long long)y * d.width + x];
+        gx = __dmul_rn(tx, w);
+        gy = __dmul_rn(ty, w);
+        return;
+      }
+      default: {  // illumination_change: alpha^beta * max(|g|, eps)^(-beta)
+        const double m = sqrt(__dadd_rn(__dmul_rn(tx, tx), __dmul_rn(ty, ty)));
+        const double f = __dmul_rn(d.alpha_pow_beta, pow(fmax(m, d.epsilon), -d.beta));
+        gx = __dmul_rn(tx, f);
+        gy = __dmul_rn(ty, f);
+        return;
+      }
+    }
+  }
+};
+
+// Divergence (operators.py:53-83, interior formula) of the field over the
+// interior cells of a window whose corner is image cell (row0, col0); the
+// window's outer ring is written 0 (no consumer reads it).
+__global__ void k_guidance_div(double *__restrict__ out, FieldView fv, int row0, int col0, int h,
+                               int w) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (long long)h * w) return;
+  const int i = (int)(k / w), j = (int)(k % w);
+  if (i == 0 || j == 0 || i == h - 1 || j == w - 1) {
+    out[k] = 0.0;
+    return;
+  }
+  const int y = row0 + i, x = col0 + j;
+  double gx, gy, gxl, gyl, unused;
+  fv.field(y, x, gx, gy);
+  fv.field(y, x - 1, gxl, unused);
+  fv.field(y - 1, x, unused, gyl);
+  out[k] = __dadd_rn(__dsub_rn(gx, gxl), __dsub_rn(gy, gyl));
+}
+
 inline unsigned blocks(long long work) { return (unsigned)((work + 255) / 256); }
 
 }  // namespace
@@ -121,6 +200,27 @@ extern "C" int gd_fold_dirichlet(double *f, const double *div, const double *bnd
                                  int32_t w, double scale, cudaStream_t st) {
   GD_REQUIRE(f && div && bnd && h > 2 && w > 2, GD_ERR_ARG, "gd_fold_dirichlet: bad arguments");
   k_fold<<<blocks((long long)(h - 2) * (w - 2)), 256, 0, st>>>(f, div, bnd, h, w, scale);
+  GD_CHECK_LAUNCH();
+  return GD_OK;
+}
+
+extern "C" int gd_guidance_divergence(double *div, const gd_field_desc *field, int32_t row0,
+                                      int32_t col0, int32_t h, int32_t w, cudaStream_t st) {
+  GD_REQUIRE(div && field && field->target && h > 2 && w > 2, GD_ERR_ARG,
+             "gd_guidance_divergence: bad arguments");
+  const gd_field_desc &d = *field;
+  GD_REQUIRE(d.kind >= GD_FIELD_IMPORT && d.kind <= GD_FIELD_ILLUMINATION, GD_ERR_ARG,
+             "gd_guidance_divergence: unknown field kind %d", d.kind);
+  GD_REQUIRE(d.height > 0 && d.width > 0 && d.channels > 0 && d.channel >= 0 &&
+                 d.channel < d.channels,
+             GD_ERR_ARG, "gd_guidance_divergence: bad image geometry");
+  GD_REQUIRE(row0 >= 0 && col0 >= 0 && row0 + h <= d.height && col0 + w <= d.width, GD_ERR_ARG,
+             "gd_guidance_divergence: window outside the image");
+  GD_REQUIRE(d.kind > GD_FIELD_AVERAGE || (d.source && d.select), GD_ERR_ARG,
+             "gd_guidance_divergence: cloning fields need a source and a selection");
+  GD_REQUIRE(d.kind != GD_FIELD_WEIGHTED || d.weights, GD_ERR_ARG,
+             "gd_guidance_divergence: weighted fields need weights");
+  k_guidance_div<<<blocks((long long)h * w), 256, 0, st>>>(div, FieldView{d}, row0, col0, h, w);
   GD_CHECK_LAUNCH();
   return GD_OK;
 }

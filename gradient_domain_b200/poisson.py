@@ -18,6 +18,7 @@ solution to rounding level.
 
 from __future__ import annotations
 
+import ctypes as C
 import time
 from dataclasses import dataclass
 
@@ -85,27 +86,19 @@ def _reports(results, method: str, seconds: float) -> list[SolverReport]:
                          _lib.STATUS_NAMES.get(r.status, str(r.status))) for r in results]
 
 
-def solve_dirichlet(field: GuidanceField, boundary, method: str = "mgcg",
-                    tolerance: float = 1e-8, max_iterations: int = 2000):
-    """Integrate ``field`` on a rectangle whose one-pixel ring is fixed to ``boundary``.
-
-    Returns the image (same shape as ``boundary``, equal to it on the ring)
-    and one :class:`SolverReport` per channel.
-    """
-    bnd, gray = _as_channels(np.asarray(boundary, dtype=float))
+def _dirichlet_from_div(div: torch.Tensor, bnd: np.ndarray, bnd_d: torch.Tensor, gray: bool,
+                        method: str, tolerance: float, max_iterations: int):
+    """Dirichlet solve on a rectangle from the per-channel divergence ``div``
+    (c, h, w) on the device and the boundary image (host ``bnd`` (h, w, c) and
+    its channels on the device ``bnd_d`` (c, h, w))."""
     h, w, c = bnd.shape
-    result = bnd.copy()
-    if h <= 2 or w <= 2:
-        return (result[..., 0] if gray else result), [
-            SolverReport(method, 0, 0.0, 0.0, True) for _ in range(c)]
-    dev = _lib.device()
-    div = _field_divergence(field, c, dev)
-    bnd_d = _to_chw(bnd, dev)
+    dev = div.device
     f = torch.empty((c, h - 2, w - 2), dtype=torch.float64, device=dev)
     for k in range(c):
         _lib.check(_lib.lib().gd_fold_dirichlet(_lib.ptr(f[k]), _lib.ptr(div[k]),
                                                 _lib.ptr(bnd_d[k]), h, w, 1.0,
                                                 _lib.stream_handle()), "gd_fold_dirichlet")
+    result = bnd.copy()
     if method not in ("mgcg", "mgcg_fp64"):
         reports = []
         folded = f.cpu().numpy()
@@ -126,10 +119,56 @@ def solve_dirichlet(field: GuidanceField, boundary, method: str = "mgcg",
     return (result[..., 0] if gray else result), _reports(results, method, elapsed)
 
 
+def solve_dirichlet(field: GuidanceField, boundary, method: str = "mgcg",
+                    tolerance: float = 1e-8, max_iterations: int = 2000):
+    """Integrate ``field`` on a rectangle whose one-pixel ring is fixed to ``boundary``.
+
+    Returns the image (same shape as ``boundary``, equal to it on the ring)
+    and one :class:`SolverReport` per channel.
+    """
+    bnd, gray = _as_channels(np.asarray(boundary, dtype=float))
+    h, w, c = bnd.shape
+    if h <= 2 or w <= 2:
+        return (bnd.copy()[..., 0] if gray else bnd.copy()), [
+            SolverReport(method, 0, 0.0, 0.0, True) for _ in range(c)]
+    dev = _lib.device()
+    div = _field_divergence(field, c, dev)
+    return _dirichlet_from_div(div, bnd, _to_chw(bnd, dev), gray, method, tolerance,
+                               max_iterations)
+
+
 def _interior(mask: np.ndarray) -> np.ndarray:
     inner = np.zeros(mask.shape, dtype=bool)
     inner[1:-1, 1:-1] = np.asarray(mask, dtype=bool)[1:-1, 1:-1]
     return inner
+
+
+def _window(interior: np.ndarray):
+    """Bounding box of the unknowns plus a one-pixel ring: (r0, r1, c0, c1)."""
+    rows = np.flatnonzero(interior.any(axis=1))
+    cols = np.flatnonzero(interior.any(axis=0))
+    return rows[0] - 1, rows[-1] + 2, cols[0] - 1, cols[-1] + 2
+
+
+def _masked_from_div(div: torch.Tensor, img_win: torch.Tensor, unk: torch.Tensor,
+                     tolerance: float, max_iterations: int, precision: str):
+    """Masked solve on a window from the per-channel divergence ``div`` (c, h, w),
+    the known image ``img_win`` (c, h, w) and the unknown mask ``unk`` (h, w),
+    all on the device; returns the solutions (c, h, w) and the solver results."""
+    c, hc, wc = div.shape
+    f = torch.empty_like(div)
+    for k in range(c):
+        _lib.check(_lib.lib().gd_masked_rhs(_lib.ptr(f[k]), _lib.ptr(div[k]),
+                                            _lib.ptr(img_win[k]), _lib.ptr(unk), hc, wc, -1.0,
+                                            _lib.stream_handle()), "gd_masked_rhs")
+    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations)
+    plan = cached_plan(tuple(Instance(hc, wc, "masked") for _ in range(c)), params)
+    for k in range(c):
+        plan.set_mask(k, unk)
+    x = torch.zeros_like(f)
+    started = time.perf_counter()
+    results = plan.solve(list(f), list(x), scale=1.0)
+    return x, results, time.perf_counter() - started
 
 
 def solve_masked(field: GuidanceField, image, mask, tolerance: float = DIRECT_TOLERANCE,
@@ -145,31 +184,15 @@ def solve_masked(field: GuidanceField, image, mask, tolerance: float = DIRECT_TO
     interior = _interior(mask)
     if not interior.any():
         return img.copy(), []
-    h, w, c = chans.shape
-    rows = np.nonzero(interior.any(axis=1))[0]
-    cols = np.nonzero(interior.any(axis=0))[0]
-    r0, r1 = rows[0] - 1, rows[-1] + 2
-    c0, c1 = cols[0] - 1, cols[-1] + 2
+    c = chans.shape[2]
+    r0, r1, c0, c1 = _window(interior)
     win = (slice(r0, r1), slice(c0, c1))
-    hc, wc = r1 - r0, c1 - c0
     dev = _lib.device()
     sub = GuidanceField(np.asarray(field.gx)[win], np.asarray(field.gy)[win])
     div = _field_divergence(sub, c, dev)
     img_d = _to_chw(chans[win], dev)
     unk = torch.as_tensor(np.ascontiguousarray(interior[win]).astype(np.uint8)).to(dev)
-    f = torch.empty((c, hc, wc), dtype=torch.float64, device=dev)
-    for k in range(c):
-        _lib.check(_lib.lib().gd_masked_rhs(_lib.ptr(f[k]), _lib.ptr(div[k]), _lib.ptr(img_d[k]),
-                                            _lib.ptr(unk), hc, wc, -1.0, _lib.stream_handle()),
-                   "gd_masked_rhs")
-    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations)
-    plan = cached_plan(tuple(Instance(hc, wc, "masked") for _ in range(c)), params)
-    for k in range(c):
-        plan.set_mask(k, unk)
-    x = torch.zeros_like(f)
-    started = time.perf_counter()
-    results = plan.solve(list(f), list(x), scale=1.0)
-    elapsed = time.perf_counter() - started
+    x, results, elapsed = _masked_from_div(div, img_d, unk, tolerance, max_iterations, precision)
     sol = x.permute(1, 2, 0).cpu().numpy()
     out = chans.copy()
     inner_win = interior[win]
@@ -178,16 +201,81 @@ def solve_masked(field: GuidanceField, image, mask, tolerance: float = DIRECT_TO
     return (out[..., 0] if gray else out), _reports(results, "mgcg (masked)", elapsed)
 
 
-def _place(source, mask, target_shape, offset):
+# ---------------------------------------------------------------------------
+# The editing entry points build their guidance fields on the device: the
+# images are uploaded once in their interleaved (h, w, c) layout and one
+# kernel per channel forms the field and its divergence on the solve window
+# (gd_guidance_divergence); only the result comes back.
+
+class _DeviceImages:
+    """The images of one edit on the device, interleaved (h, w, c) FP64."""
+
+    def __init__(self, target: np.ndarray, dev):
+        self.gray = target.ndim == 2
+        t = target[..., None] if self.gray else target
+        self.h, self.w, self.c = t.shape
+        self.target = torch.as_tensor(np.ascontiguousarray(t, dtype=np.float64)).to(dev)
+        self.keep = []  # device buffers referenced by descriptors
+
+    def desc(self, kind: int, channel: int, source=None, select=None, weights=None,
+             illumination=(0.0, 0.0, 0.0)) -> _lib.FieldDesc:
+        return _lib.FieldDesc(kind, self.h, self.w, self.c, channel, 0, _lib.ptr(self.target),
+                              _lib.ptr(source) if source is not None else None,
+                              _lib.ptr(select) if select is not None else None,
+                              _lib.ptr(weights) if weights is not None else None,
+                              float(illumination[0]), float(illumination[1]),
+                              float(illumination[2]))
+
+    def divergence(self, descs, r0: int, c0: int, hh: int, ww: int) -> torch.Tensor:
+        div = torch.empty((len(descs), hh, ww), dtype=torch.float64, device=self.target.device)
+        for k, d in enumerate(descs):
+            _lib.check(_lib.lib().gd_guidance_divergence(_lib.ptr(div[k]), C.byref(d), r0, c0,
+                                                         hh, ww, _lib.stream_handle()),
+                       "gd_guidance_divergence")
+        return div
+
+    def channels(self, r0: int, r1: int, c0: int, c1: int) -> torch.Tensor:
+        """(c, h, w) contiguous copy of a window of the target."""
+        return self.target[r0:r1, c0:c1, :].permute(2, 0, 1).contiguous()
+
+
+def _edit_masked(imgs: _DeviceImages, descs, mask: np.ndarray, tolerance: float,
+                 label: str = "mgcg (masked)"):
+    interior = _interior(mask)
+    host = imgs.target
+    if not interior.any():
+        out = host.cpu().numpy()
+        return (out[..., 0] if imgs.gray else out), []
+    r0, r1, c0, c1 = _window(interior)
+    div = imgs.divergence(descs, r0, c0, r1 - r0, c1 - c0)
+    img_win = imgs.channels(r0, r1, c0, c1)
+    unk = torch.as_tensor(np.ascontiguousarray(interior[r0:r1, c0:c1]).astype(np.uint8)).to(
+        host.device)
+    x, results, elapsed = _masked_from_div(div, img_win, unk, tolerance, 2000, "mixed")
+    out = host.clone()
+    win = out[r0:r1, c0:c1, :]
+    win.copy_(torch.where(unk.bool()[..., None], x.permute(1, 2, 0), win))
+    res = out.cpu().numpy()
+    return (res[..., 0] if imgs.gray else res), _reports(results, label, elapsed)
+
+
+def _edit_rectangle(imgs: _DeviceImages, descs, r0: int, r1: int, c0: int, c1: int,
+                    method: str, tolerance: float):
+    div = imgs.divergence(descs, r0, c0, r1 - r0, c1 - c0)
+    bnd_d = imgs.channels(r0, r1, c0, c1)
+    bnd = bnd_d.permute(1, 2, 0).cpu().numpy()
+    return _dirichlet_from_div(div, bnd, bnd_d, False, method, tolerance, 2000)
+
+
+_CLONE_KINDS = {"import": _lib.GD_FIELD_IMPORT, "mixed": _lib.GD_FIELD_MIXED,
+                "average": _lib.GD_FIELD_AVERAGE}
+
+
+def _check_place(source_shape, target_shape, offset):
     row, column = offset
-    height, width = source.shape[:2]
+    height, width = source_shape[:2]
     if row < 0 or column < 0 or row + height > target_shape[0] or column + width > target_shape[1]:
         raise ValueError("the source patch does not fit the target at this offset")
-    canvas = np.zeros(target_shape, dtype=float)
-    canvas[row:row + height, column:column + width] = source
-    placed = np.zeros(target_shape[:2], dtype=bool)
-    placed[row:row + height, column:column + width] = mask
-    return canvas, placed
 
 
 def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
@@ -199,62 +287,74 @@ def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
     masked domain otherwise runs at the direct-solver level 1e-12 and the
     rectangle at 1e-8, as in the reference.  Raises ``ValueError`` for an
     unknown ``mode`` or ``domain``, or a patch that does not fit
-    (poisson.py:310-335).
+    (poisson.py:310-335).  The placement, both gradient fields, their
+    combination and the right-hand side are formed on the device.
     """
     target = np.asarray(target, dtype=float)
     source = np.asarray(source, dtype=float)
     if source.ndim != target.ndim:
         raise ValueError("source and target must have the same number of dimensions")
-    placed, placed_mask = _place(source, mask, target.shape, offset)
-    source_field = GuidanceField.of(placed)
-    target_field = GuidanceField.of(target)
-    if mode == "import":
-        inside = source_field
-    elif mode == "mixed":
-        inside = source_field.mix_by_magnitude(target_field)
-    elif mode == "average":
-        inside = GuidanceField(0.5 * (source_field.gx + target_field.gx),
-                               0.5 * (source_field.gy + target_field.gy))
-    else:
+    _check_place(source.shape, target.shape, offset)
+    if mode not in _CLONE_KINDS:
         raise ValueError(f"unknown mode {mode!r}")
-    field = inside.select(placed_mask, target_field)
-    if domain == "mask":
-        if tolerance is None:
-            return solve_masked(field, target, placed_mask)
-        return solve_masked(field, target, placed_mask, tolerance=tolerance)
-    if domain != "rectangle":
+    if domain not in ("mask", "rectangle"):
         raise ValueError(f"unknown domain {domain!r}")
+    row, column = offset
+    height, width = source.shape[:2]
+    placed_mask = np.zeros(target.shape[:2], dtype=bool)
+    placed_mask[row:row + height, column:column + width] = mask
+    dev = _lib.device()
+    imgs = _DeviceImages(target, dev)
+    canvas = torch.zeros_like(imgs.target)
+    src = source[..., None] if source.ndim == 2 else source
+    canvas[row:row + height, column:column + width, :] = torch.as_tensor(
+        np.ascontiguousarray(src)).to(dev)
+    sel = torch.as_tensor(placed_mask.astype(np.uint8)).to(dev)
+    descs = [imgs.desc(_CLONE_KINDS[mode], ch, source=canvas, select=sel) for ch in range(imgs.c)]
+    if domain == "mask":
+        return _edit_masked(imgs, descs, placed_mask,
+                            DIRECT_TOLERANCE if tolerance is None else tolerance)
     rows, columns = np.nonzero(placed_mask)
     top = max(int(rows.min()) - margin, 0)
     bottom = min(int(rows.max()) + margin + 1, target.shape[0])
     left = max(int(columns.min()) - margin, 0)
     right = min(int(columns.max()) + margin + 1, target.shape[1])
-    window = (slice(top, bottom), slice(left, right))
-    patch, reports = solve_dirichlet(GuidanceField(field.gx[window], field.gy[window]),
-                                     target[window], method=method,
-                                     tolerance=1e-8 if tolerance is None else tolerance)
     result = target.copy()
-    result[window] = patch
+    if bottom - top <= 2 or right - left <= 2:
+        return result, [SolverReport(method, 0, 0.0, 0.0, True) for _ in range(imgs.c)]
+    patch, reports = _edit_rectangle(imgs, descs, top, bottom, left, right, method,
+                                     1e-8 if tolerance is None else tolerance)
+    result[top:bottom, left:right] = patch[..., 0] if imgs.gray else patch
     return result, reports
 
 
 def texture_flatten(image, edges, method: str = "mgcg", mask=None):
-    """Keep gradients only on ``edges`` (weights in [0, 1]) and re-integrate."""
+    """Keep gradients only on ``edges`` (weights in [0, 1]) and re-integrate.
+
+    The weighted gradient field is formed on the device."""
     image = np.asarray(image, dtype=float)
-    weights = np.asarray(edges, dtype=float)
-    if image.ndim == 3:
-        weights = weights[..., None]
-    field = GuidanceField.of(image).scaled(weights)
+    weights = np.ascontiguousarray(np.asarray(edges, dtype=float))
+    dev = _lib.device()
+    imgs = _DeviceImages(image, dev)
+    wts = torch.as_tensor(weights).to(dev)
+    descs = [imgs.desc(_lib.GD_FIELD_WEIGHTED, ch, weights=wts) for ch in range(imgs.c)]
     if mask is not None:
-        return solve_masked(field, image, mask)
-    return solve_dirichlet(field, image, method=method)
+        return _edit_masked(imgs, descs, np.asarray(mask, dtype=bool), DIRECT_TOLERANCE)
+    h, w = image.shape[:2]
+    if h <= 2 or w <= 2:
+        return image.copy(), [SolverReport(method, 0, 0.0, 0.0, True) for _ in range(imgs.c)]
+    out, reports = _edit_rectangle(imgs, descs, 0, h, 0, w, method, 1e-8)
+    return (out[..., 0] if imgs.gray else out), reports
 
 
 def illumination_change(image, mask, alpha: float = 0.2, beta: float = 0.2,
                         epsilon: float = 1e-4):
-    """Compress local dynamic range inside ``mask`` (gradient remap alpha^b g^-b)."""
+    """Compress local dynamic range inside ``mask`` (gradient remap alpha^b g^-b).
+
+    The remapped field is formed on the device."""
     image = np.asarray(image, dtype=float)
-    field = GuidanceField.of(image)
-    magnitude = np.sqrt(field.gx ** 2 + field.gy ** 2)
-    factor = (alpha ** beta) * np.maximum(magnitude, epsilon) ** (-beta)
-    return solve_masked(field.scaled(factor), image, mask)
+    dev = _lib.device()
+    imgs = _DeviceImages(image, dev)
+    descs = [imgs.desc(_lib.GD_FIELD_ILLUMINATION, ch,
+                       illumination=(alpha ** beta, beta, epsilon)) for ch in range(imgs.c)]
+    return _edit_masked(imgs, descs, np.asarray(mask, dtype=bool), DIRECT_TOLERANCE)

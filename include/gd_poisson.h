@@ -235,6 +235,37 @@ int gd_divergence(double *div_dev, const double *gx_dev, const double *gy_dev, i
 int gd_fold_dirichlet(double *f_dev, const double *div_dev, const double *boundary_dev,
                       int32_t h, int32_t w, double scale, cudaStream_t stream);
 
+/* Guidance fields of the editing entry points, built on the device from the
+ * images themselves (poisson.py:52-92 and the field set-up of seamless_clone,
+ * texture_flatten, illumination_change, poisson.py:306-431). */
+enum gd_field_kind {
+  GD_FIELD_IMPORT = 0,       /* source gradient inside `select`, target outside     */
+  GD_FIELD_MIXED = 1,        /* inside: the larger of source / target per component */
+  GD_FIELD_AVERAGE = 2,      /* inside: the mean of source and target gradients     */
+  GD_FIELD_WEIGHTED = 3,     /* target gradient times per-pixel `weights`           */
+  GD_FIELD_ILLUMINATION = 4  /* target gradient times alpha^beta max(|g|,eps)^-beta */
+};
+
+typedef struct gd_field_desc {
+  int32_t kind;                 /* enum gd_field_kind */
+  int32_t height, width;        /* image size */
+  int32_t channels, channel;    /* interleaved (height, width, channels) images; channel used */
+  int32_t pad;
+  const double *target;         /* the image whose gradient is the base field */
+  const double *source;         /* cloning: source placed on a target-sized canvas */
+  const uint8_t *select;        /* cloning: height x width, non-zero where the source field applies */
+  const double *weights;        /* weighted: height x width */
+  double alpha_pow_beta, beta, epsilon;  /* illumination parameters (alpha^beta precomputed) */
+} gd_field_desc;
+
+/* div (h x w, row pitch w) = divergence of the field over the interior cells
+ * of the window whose corner is image cell (row0, col0); the window's outer
+ * ring is written 0.  Replaces GuidanceField construction + operators.divergence
+ * as seamless_clone / texture_flatten / illumination_change use them; feed the
+ * result to gd_masked_rhs or gd_fold_dirichlet. */
+int gd_guidance_divergence(double *div_dev, const gd_field_desc *field, int32_t row0,
+                           int32_t col0, int32_t h, int32_t w, cudaStream_t stream);
+
 /* Masked system on the whole h x w image: f <- scale * (div - sum of known
  * neighbour values) at unknowns, 0 elsewhere (poisson.py:216-224). */
 int gd_masked_rhs(double *f_dev, const double *div_dev, const double *image_dev,

@@ -285,6 +285,72 @@ def test_async_solve_and_pipelined_batch():
         assert all(r.converged for r in gd.solve_neumann_batch.last_results)
 
 
+def _device_field_div(target, kind, window, source=None, select=None, weights=None,
+                      illumination=(0.0, 0.0, 0.0)):
+    import ctypes as C
+    t = target[..., None] if target.ndim == 2 else target
+    h, w, c = t.shape
+    tgt = torch.as_tensor(np.ascontiguousarray(t)).cuda()
+    src = (torch.as_tensor(np.ascontiguousarray(source[..., None] if source.ndim == 2
+                                                else source)).cuda()
+           if source is not None else None)
+    sel = torch.as_tensor(select.astype(np.uint8)).cuda() if select is not None else None
+    wts = torch.as_tensor(np.ascontiguousarray(weights)).cuda() if weights is not None else None
+    r0, r1, c0, c1 = window
+    out = []
+    for ch in range(c):
+        d = _lib.FieldDesc(kind, h, w, c, ch, 0, _lib.ptr(tgt),
+                           _lib.ptr(src) if src is not None else None,
+                           _lib.ptr(sel) if sel is not None else None,
+                           _lib.ptr(wts) if wts is not None else None, *illumination)
+        div = torch.empty((r1 - r0, c1 - c0), dtype=torch.float64, device="cuda")
+        _lib.check(_lib.lib().gd_guidance_divergence(_lib.ptr(div), C.byref(d), r0, c0,
+                                                     r1 - r0, c1 - c0, _lib.stream_handle()),
+                   "gd_guidance_divergence")
+        out.append(div.cpu().numpy())
+    return out
+
+
+def test_device_guidance_fields_match_numpy_fields():
+    """gd_guidance_divergence forms the editing fields and their divergence on the
+    device: bitwise the NumPy result for cloning and weighted fields, to rounding
+    for the illumination remap (its power function may differ in the last bit)."""
+    from oracle import poisson as op
+    rng = np.random.default_rng(31)
+    target = rng.random((70, 90, 3))
+    source = rng.random((40, 50, 3))
+    yy, xx = np.mgrid[0:40, 0:50]
+    mask = (yy - 20.0) ** 2 / 300 + (xx - 25.0) ** 2 / 500 < 1.0
+    offset = (12, 21)
+    window = (5, 66, 8, 85)
+    win = (slice(window[0], window[1]), slice(window[2], window[3]))
+    inner = (slice(1, -1), slice(1, -1))
+    kinds = {"import": _lib.GD_FIELD_IMPORT, "mixed": _lib.GD_FIELD_MIXED,
+             "average": _lib.GD_FIELD_AVERAGE}
+    for mode, kind in kinds.items():
+        field, placed, tgt = op.clone_field(source, target, mask, offset, mode)
+        canvas, _ = op.place(source, mask, target.shape, offset)
+        got = _device_field_div(target, kind, window, source=canvas, select=placed)
+        for ch in range(3):
+            want = ops.divergence(field.gx[win][..., ch], field.gy[win][..., ch])
+            assert np.array_equal(got[ch][inner], want[inner]), mode
+    weights = (rng.random((70, 90)) > 0.6).astype(float) * rng.random((70, 90))
+    g = op.GuidanceField.of(target).scaled(weights[..., None])
+    got = _device_field_div(target, _lib.GD_FIELD_WEIGHTED, window, weights=weights)
+    for ch in range(3):
+        want = ops.divergence(g.gx[win][..., ch], g.gy[win][..., ch])
+        assert np.array_equal(got[ch][inner], want[inner])
+    alpha, beta, eps = 0.2, 0.3, 1e-4
+    f = op.GuidanceField.of(target)
+    factor = (alpha ** beta) * np.maximum(np.sqrt(f.gx ** 2 + f.gy ** 2), eps) ** (-beta)
+    g = f.scaled(factor)
+    got = _device_field_div(target, _lib.GD_FIELD_ILLUMINATION, window,
+                            illumination=(alpha ** beta, beta, eps))
+    for ch in range(3):
+        want = ops.divergence(g.gx[win][..., ch], g.gy[win][..., ch])
+        assert np.abs(got[ch][inner] - want[inner]).max() <= 1e-14 * np.abs(want).max()
+
+
 def test_masked_and_dirichlet_applications_match_golden(golden):
     field = gd.GuidanceField.of(golden["app_src"])
     got, reps = gd.solve_masked(field, golden["app_img"], golden["app_disc"])
