@@ -28,7 +28,8 @@ EXPORTS = (
     "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
-    "gd_masked_rhs", "gd_guidance_divergence",
+    "gd_masked_rhs", "gd_guidance_divergence", "gd_tm_scratch_bytes", "gd_tm_log_luminance",
+    "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose",
 )
 
 
@@ -53,7 +54,7 @@ class Report(C.Structure):
 
 class FieldDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("height", C.c_int32), ("width", C.c_int32),
-                ("channels", C.c_int32), ("channel", C.c_int32), ("pad", C.c_int32),
+                ("channels", C.c_int32), ("channel", C.c_int32), ("edges", C.c_int32),
                 ("target", C.c_void_p), ("source", C.c_void_p), ("select", C.c_void_p),
                 ("weights", C.c_void_p), ("alpha_pow_beta", C.c_double), ("beta", C.c_double),
                 ("epsilon", C.c_double)]
@@ -115,6 +116,12 @@ def _declare(lib: C.CDLL) -> None:
         "gd_masked_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
         "gd_guidance_divergence": (C.c_int, [_vp, C.POINTER(FieldDesc), _i32, _i32, _i32, _i32,
                                              _vp]),
+        "gd_tm_scratch_bytes": (_sz, []),
+        "gd_tm_log_luminance": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+        "gd_tm_downsample": (C.c_int, [_vp, _vp, _i32, _i32, _vp]),
+        "gd_tm_level_factor": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _f64, _f64, _f64,
+                                         _f64, _vp, _vp]),
+        "gd_tm_compose": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _f64, _f64, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

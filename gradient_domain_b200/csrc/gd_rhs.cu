@@ -149,24 +149,29 @@ struct FieldView {
   }
 };
 
-// Divergence (operators.py:53-83, interior formula) of the field over the
-// interior cells of a window whose corner is image cell (row0, col0); the
-// window's outer ring is written 0 (no consumer reads it).
+// Divergence (operators.py:53-83) of the field over a window whose corner is
+// image cell (row0, col0).  Interior cells take the backward differences; the
+// window's outer ring is written 0 (no consumer of a window reads it) or, with
+// `edges`, follows operators.py's edge rules for the window as a whole image.
 __global__ void k_guidance_div(double *__restrict__ out, FieldView fv, int row0, int col0, int h,
                                int w) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= (long long)h * w) return;
   const int i = (int)(k / w), j = (int)(k % w);
-  if (i == 0 || j == 0 || i == h - 1 || j == w - 1) {
+  const int y = row0 + i, x = col0 + j;
+  const bool ring = i == 0 || j == 0 || i == h - 1 || j == w - 1;
+  if (ring && !fv.d.edges) {
     out[k] = 0.0;
     return;
   }
-  const int y = row0 + i, x = col0 + j;
-  double gx, gy, gxl, gyl, unused;
+  double gx, gy, gxl = 0.0, gyl = 0.0, unused;
   fv.field(y, x, gx, gy);
-  fv.field(y, x - 1, gxl, unused);
-  fv.field(y - 1, x, unused, gyl);
-  out[k] = __dadd_rn(__dsub_rn(gx, gxl), __dsub_rn(gy, gyl));
+  if (j > 0) fv.field(y, x - 1, gxl, unused);
+  if (i > 0) fv.field(y - 1, x, unused, gyl);
+  double dx = 0.0, dy = 0.0;
+  if (w > 1) dx = j == 0 ? gx : j == w - 1 ? -gxl : __dsub_rn(gx, gxl);
+  if (h > 1) dy = i == 0 ? gy : i == h - 1 ? -gyl : __dsub_rn(gy, gyl);
+  out[k] = __dadd_rn(dx, dy);
 }
 
 inline unsigned blocks(long long work) { return (unsigned)((work + 255) / 256); }
@@ -206,8 +211,8 @@ extern "C" int gd_fold_dirichlet(double *f, const double *div, const double *bnd
 
 extern "C" int gd_guidance_divergence(double *div, const gd_field_desc *field, int32_t row0,
                                       int32_t col0, int32_t h, int32_t w, cudaStream_t st) {
-  GD_REQUIRE(div && field && field->target && h > 2 && w > 2, GD_ERR_ARG,
-             "gd_guidance_divergence: bad arguments");
+  GD_REQUIRE(div && field && field->target && h > 0 && w > 0 && (field->edges || (h > 2 && w > 2)),
+             GD_ERR_ARG, "gd_guidance_divergence: bad arguments");
   const gd_field_desc &d = *field;
   GD_REQUIRE(d.kind >= GD_FIELD_IMPORT && d.kind <= GD_FIELD_ILLUMINATION, GD_ERR_ARG,
              "gd_guidance_divergence: unknown field kind %d", d.kind);

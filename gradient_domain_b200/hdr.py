@@ -1,24 +1,30 @@
-"""Gradient-domain HDR tone mapping on the GPU Neumann solver.
+"""Gradient-domain HDR tone mapping on the GPU.
 
 Same interface as gradient-domain/src/gradient_domain/hdr.py: ``ToneMapConfig``
-(:37-70), ``attenuation_field`` (:107-134) and ``tone_map`` (:137-185).  The
-Poisson integration (the ``solve_neumann`` call at hdr.py:175) runs in the
-B200 Neumann MGPCG; the attenuation pyramid and the final exposure/saturation
-steps are the reference's array expressions, evaluated on the host.
+(:37-70), ``attenuation_field`` (:107-134) and ``tone_map`` (:137-185).
+``tone_map`` runs on the device from the uploaded radiance to the display
+image: log-luminance, the attenuation pyramid (binomial downsampling, central
+gradients, per-level factors propagated coarse to fine), the attenuated field
+and its divergence, the Neumann MGPCG, and the exposure / saturation /
+percentile normalisation (gd_tonemap.cu, gd_rhs.cu); only the image and the
+factor come back.
 """
 
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
+import torch
 
-from .operators import divergence, gradient
-from .solvers import solve_neumann
+from . import _lib
+from .plan import Instance, SolveParams, cached_plan
 
 __all__ = ["ToneMapConfig", "attenuation_field", "tone_map"]
 
 LUMA = np.array([0.2126, 0.7152, 0.0722])
+NEUMANN_TOLERANCE = 1e-14  # the exact-solver level of solve_neumann
 
 
 @dataclass
@@ -32,70 +38,76 @@ class ToneMapConfig:
     epsilon: float = 1e-4
 
 
-_BINOMIAL = np.array([1.0, 4.0, 6.0, 4.0, 1.0]) / 16.0
+def _scratch(dev) -> torch.Tensor:
+    return torch.empty(int(_lib.lib().gd_tm_scratch_bytes()), dtype=torch.uint8, device=dev)
 
 
-def _downsample(image: np.ndarray) -> np.ndarray:
-    """Separable 5-tap binomial blur with edge replication, then keep every other sample."""
-    width = image.shape[1]
-    p = np.pad(image, ((0, 0), (2, 2)), mode="edge")
-    blurred = sum(k * p[:, i:i + width] for i, k in enumerate(_BINOMIAL))
-    height = image.shape[0]
-    p = np.pad(blurred, ((2, 2), (0, 0)), mode="edge")
-    blurred = sum(k * p[i:i + height, :] for i, k in enumerate(_BINOMIAL))
-    return blurred[::2, ::2]
-
-
-def _upsample(image: np.ndarray, shape) -> np.ndarray:
-    """Bilinear resampling onto a finer grid spanning the same extent."""
-    ry = np.linspace(0, image.shape[0] - 1, shape[0])
-    rx = np.linspace(0, image.shape[1] - 1, shape[1])
-    y0, x0 = np.floor(ry).astype(int), np.floor(rx).astype(int)
-    y1 = np.minimum(y0 + 1, image.shape[0] - 1)
-    x1 = np.minimum(x0 + 1, image.shape[1] - 1)
-    wy, wx = (ry - y0)[:, None], (rx - x0)[None, :]
-    top = image[y0][:, x0] * (1 - wx) + image[y0][:, x1] * wx
-    bottom = image[y1][:, x0] * (1 - wx) + image[y1][:, x1] * wx
-    return top * (1 - wy) + bottom * wy
-
-
-def _central_gradient(image: np.ndarray, spacing: float):
-    p = np.pad(image, 1, mode="edge")
-    return ((p[1:-1, 2:] - p[1:-1, :-2]) / (2.0 * spacing),
-            (p[2:, 1:-1] - p[:-2, 1:-1]) / (2.0 * spacing))
+def _attenuation_dev(logl: torch.Tensor, config: ToneMapConfig,
+                     scratch: torch.Tensor) -> torch.Tensor:
+    """The multiscale attenuation factor of a device log-luminance (h, w)."""
+    lib, st = _lib.lib(), _lib.stream_handle()
+    pyramid = [logl]
+    while len(pyramid) < config.levels and min(pyramid[-1].shape) > 16:
+        h, w = pyramid[-1].shape
+        out = torch.empty(((h + 1) // 2, (w + 1) // 2), dtype=torch.float64, device=logl.device)
+        _lib.check(lib.gd_tm_downsample(_lib.ptr(out), _lib.ptr(pyramid[-1]), h, w, st),
+                   "gd_tm_downsample")
+        pyramid.append(out)
+    factor = None
+    for level in reversed(range(len(pyramid))):
+        a = pyramid[level]
+        h, w = a.shape
+        f = torch.empty_like(a)
+        ch, cw = factor.shape if factor is not None else (0, 0)
+        _lib.check(lib.gd_tm_level_factor(_lib.ptr(f), _lib.ptr(a),
+                                          _lib.ptr(factor) if factor is not None else None,
+                                          h, w, ch, cw, 2.0 ** level, float(config.alpha),
+                                          float(config.beta), float(config.epsilon),
+                                          _lib.ptr(scratch), st), "gd_tm_level_factor")
+        factor = f
+    return factor
 
 
 def attenuation_field(log_luminance, config: ToneMapConfig) -> np.ndarray:
     """Multiscale gradient attenuation factor, propagated coarse to fine."""
-    pyramid = [np.asarray(log_luminance, dtype=float)]
-    while len(pyramid) < config.levels and min(pyramid[-1].shape) > 16:
-        pyramid.append(_downsample(pyramid[-1]))
-    factor = None
-    for level in reversed(range(len(pyramid))):
-        gx, gy = _central_gradient(pyramid[level], 2.0 ** level)
-        magnitude = np.sqrt(gx * gx + gy * gy)
-        scale = config.alpha * max(float(magnitude.mean()), config.epsilon)
-        floored = np.maximum(magnitude, config.epsilon)
-        local = (scale / floored) * (floored / scale) ** config.beta
-        factor = local if factor is None else _upsample(factor, local.shape) * local
-    return factor
+    dev = _lib.device()
+    logl = torch.as_tensor(np.ascontiguousarray(log_luminance, dtype=np.float64)).to(dev)
+    return _attenuation_dev(logl, config, _scratch(dev)).cpu().numpy()
 
 
 def tone_map(radiance, config: ToneMapConfig | None = None):
     """Compress a linear HDR radiance map (h, w, 3) to display values in [0, 1].
 
-    Raises ``ValueError`` if the input is not a three-channel image.
+    Returns the image and the attenuation factor that was applied.  Raises
+    ``ValueError`` if the input is not a three-channel image.
     """
     config = config or ToneMapConfig()
     radiance = np.asarray(radiance, dtype=float)
     if radiance.ndim != 3 or radiance.shape[2] != 3:
         raise ValueError("tone mapping expects a three-channel radiance map")
-    luminance = np.maximum(radiance @ LUMA, np.finfo(float).tiny)
-    log_luminance = np.log(luminance)
-    factor = attenuation_field(log_luminance, config)
-    gx, gy = gradient(log_luminance)
-    compressed = solve_neumann(divergence(gx * factor, gy * factor))
-    result = np.exp(compressed - compressed.max())
-    image = ((radiance / luminance[..., None]) ** config.saturation) * result[..., None]
-    peak = float(np.percentile(image, 99.5))
-    return np.clip(image / max(peak, 1e-12), 0.0, 1.0), factor
+    h, w, _ = radiance.shape
+    dev = _lib.device()
+    lib, st = _lib.lib(), _lib.stream_handle()
+    rad = torch.as_tensor(np.ascontiguousarray(radiance)).to(dev)
+    logl = torch.empty((h, w), dtype=torch.float64, device=dev)
+    lum = torch.empty_like(logl)
+    _lib.check(lib.gd_tm_log_luminance(_lib.ptr(logl), _lib.ptr(lum), _lib.ptr(rad), h, w, st),
+               "gd_tm_log_luminance")
+    scratch = _scratch(dev)
+    factor = _attenuation_dev(logl, config, scratch)
+    # forward-difference field of the log-luminance times the factor, and its
+    # divergence over the whole image (hdr.py:171-175)
+    div = torch.empty_like(logl)
+    desc = _lib.FieldDesc(_lib.GD_FIELD_WEIGHTED, h, w, 1, 0, 1, _lib.ptr(logl), None, None,
+                          _lib.ptr(factor), 0.0, 0.0, 0.0)
+    _lib.check(lib.gd_guidance_divergence(_lib.ptr(div), C.byref(desc), 0, 0, h, w, st),
+               "gd_guidance_divergence")
+    plan = cached_plan((Instance(h, w, "neumann", True),), SolveParams(tolerance=NEUMANN_TOLERANCE))
+    compressed = torch.zeros_like(div)
+    plan.solve([div], [compressed], scale=-1.0)
+    image = torch.empty_like(rad)
+    out = torch.empty_like(rad)
+    _lib.check(lib.gd_tm_compose(_lib.ptr(out), _lib.ptr(image), _lib.ptr(rad), _lib.ptr(lum),
+                                 _lib.ptr(compressed), h, w, float(config.saturation), 99.5,
+                                 _lib.ptr(scratch), st), "gd_tm_compose")
+    return out.cpu().numpy(), factor.cpu().numpy()

@@ -22,7 +22,33 @@ from __future__ import annotations
 
 import numpy as np
 
-from .hdr import ToneMapConfig, attenuation_field
+
+
+def _downsample(image):
+    """5-tap binomial blur with edge replication, every other sample."""
+    k = np.array([1.0, 4.0, 6.0, 4.0, 1.0]) / 16.0
+    p = np.pad(image, ((0, 0), (2, 2)), mode="edge")
+    b = sum(kk * p[:, i:i + image.shape[1]] for i, kk in enumerate(k))
+    p = np.pad(b, ((2, 2), (0, 0)), mode="edge")
+    b = sum(kk * p[i:i + image.shape[0], :] for i, kk in enumerate(k))
+    return b[::2, ::2]
+
+
+def _attenuation(log_r, alpha=0.1, beta=0.85, levels=1, eps=1e-4):
+    """Host copy of the attenuation factor used to shape the synthetic field
+    (one pyramid level by default, as the tone-mapping workload uses)."""
+    pyr = [log_r]
+    while len(pyr) < levels and min(pyr[-1].shape) > 16:
+        pyr.append(_downsample(pyr[-1]))
+    if len(pyr) != 1:
+        raise NotImplementedError("the synthetic workload uses a single level")
+    p = np.pad(log_r, 1, mode="edge")
+    gx = (p[1:-1, 2:] - p[1:-1, :-2]) / 2.0
+    gy = (p[2:, 1:-1] - p[:-2, 1:-1]) / 2.0
+    m = np.sqrt(gx * gx + gy * gy)
+    scale = alpha * max(float(m.mean()), eps)
+    fl = np.maximum(m, eps)
+    return (scale / fl) * (fl / scale) ** beta
 
 
 def blob_image(shape, count, rng, sigma=(10.0, 120.0), noise=0.05):
@@ -71,12 +97,11 @@ def tonemap_rhs(size=4096, seed=1, channels=3):
     rng = np.random.default_rng(seed)
     scale = size / 1024.0
     out = np.empty((channels, size, size))
-    cfg = ToneMapConfig(alpha=0.1, beta=0.85, levels=1)
     for c in range(channels):
         mod = 0.05 + blob_image((size, size), 64, rng, sigma=(10.0 * scale, 120.0 * scale),
                                 noise=0.0)
         log_r = 2.5 * rng.standard_normal((size, size)) + np.log(mod)
-        factor = attenuation_field(log_r, cfg)
+        factor = _attenuation(log_r)
         gx, gy = forward_gradient(log_r)
         out[c] = divergence(gx * factor, gy * factor)
     return out

@@ -144,6 +144,31 @@ int gd_solve_finish(gd_plan plan, gd_report *reports);
 int gd_plan_apply_vcycle(gd_plan plan, int32_t instance, const double *r_dev,
                          double *z_dev, int32_t pitch, cudaStream_t stream);
 
+/* Tone mapping around the Neumann solve (hdr.py:73-185), all FP64 row-major;
+ * `scratch` is gd_tm_scratch_bytes() of device memory owned by the caller.
+ *   gd_tm_log_luminance: lum = max(radiance . (0.2126, 0.7152, 0.0722), tiny),
+ *     logl = log(lum); radiance is (h, w, 3) interleaved          (hdr.py:168-170)
+ *   gd_tm_downsample: binomial blur + every other sample, out ceil(h/2) x ceil(w/2)
+ *                                                                   (hdr.py:73-80)
+ *   gd_tm_level_factor: the attenuation factor of one pyramid level (spacing
+ *     2^level), times the bilinear upsampling of the coarser level's factor
+ *     (coarse = NULL on the coarsest level)                     (hdr.py:83-134)
+ *   gd_tm_compose: out = clip(image / percentile(image, q), 0, 1) with
+ *     image = (radiance / lum)^saturation * exp(c - max c); `image` is an
+ *     (h, w, 3) buffer of the caller                            (hdr.py:178-185) */
+size_t gd_tm_scratch_bytes(void);
+int gd_tm_log_luminance(double *logl_dev, double *lum_dev, const double *radiance_dev,
+                        int32_t h, int32_t w, cudaStream_t stream);
+int gd_tm_downsample(double *out_dev, const double *in_dev, int32_t h, int32_t w,
+                     cudaStream_t stream);
+int gd_tm_level_factor(double *factor_dev, const double *level_dev, const double *coarse_dev,
+                       int32_t h, int32_t w, int32_t coarse_h, int32_t coarse_w, double spacing,
+                       double alpha, double beta, double epsilon, void *scratch_dev,
+                       cudaStream_t stream);
+int gd_tm_compose(double *out_dev, double *image_dev, const double *radiance_dev,
+                  const double *lum_dev, const double *compressed_dev, int32_t h, int32_t w,
+                  double saturation, double percentile, void *scratch_dev, cudaStream_t stream);
+
 /* Kernel kinds reported by gd_plan_kernel_times. */
 enum gd_kernel_kind {
   GD_K_DOWN0 = 0,   /* level-0 pre-smooth + residual + restriction      */
@@ -250,7 +275,8 @@ typedef struct gd_field_desc {
   int32_t kind;                 /* enum gd_field_kind */
   int32_t height, width;        /* image size */
   int32_t channels, channel;    /* interleaved (height, width, channels) images; channel used */
-  int32_t pad;
+  int32_t edges;                /* non-zero: the window's outer ring follows operators.py's
+                                   edge rules (for a window that is the whole image) */
   const double *target;         /* the image whose gradient is the base field */
   const double *source;         /* cloning: source placed on a target-sized canvas */
   const uint8_t *select;        /* cloning: height x width, non-zero where the source field applies */
@@ -260,7 +286,8 @@ typedef struct gd_field_desc {
 
 /* div (h x w, row pitch w) = divergence of the field over the interior cells
  * of the window whose corner is image cell (row0, col0); the window's outer
- * ring is written 0.  Replaces GuidanceField construction + operators.divergence
+ * ring is written 0, or with `edges` follows the edge rules of
+ * operators.divergence (tone mapping integrates the whole image).  Replaces GuidanceField construction + operators.divergence
  * as seamless_clone / texture_flatten / illumination_change use them; feed the
  * result to gd_masked_rhs or gd_fold_dirichlet. */
 int gd_guidance_divergence(double *div_dev, const gd_field_desc *field, int32_t row0,

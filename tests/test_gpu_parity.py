@@ -394,6 +394,25 @@ def test_tone_map_matches_golden(golden):
         gd.tone_map(np.ones((16, 16)))
 
 
+@pytest.mark.parametrize("shape,levels", [((300, 257), 8), ((97, 130), 3), ((40, 33), 8)])
+def test_tone_map_matches_oracle(shape, levels):
+    """The device tone map (pyramid, field, Neumann solve, exposure and the exact
+    radix-selected percentile) against the oracle's NumPy/DCT pipeline; the
+    radiance repeats values so the percentile meets ties."""
+    from oracle import hdr as oh
+    rng = np.random.default_rng(sum(shape))
+    rad = np.exp(2.0 * rng.standard_normal(shape + (3,)))
+    rad[: shape[0] // 3] = np.round(rad[: shape[0] // 3], 1) + 0.1
+    cfg = gd.ToneMapConfig(levels=levels)
+    got, fgot = gd.tone_map(rad, cfg)
+    want, fwant = oh.tone_map(rad, oh.ToneMapConfig(levels=levels))
+    np.testing.assert_allclose(fgot, fwant, rtol=1e-12)
+    assert np.abs(got - want).max() < 1e-8
+    np.testing.assert_allclose(gd.attenuation_field(np.log(rad[..., 0]), cfg),
+                               oh.attenuation_field(np.log(rad[..., 0]),
+                                                    oh.ToneMapConfig(levels=levels)), rtol=1e-12)
+
+
 def test_operators_match_golden(golden):
     gx, gy = gd.gradient(golden["op_u"])
     np.testing.assert_array_equal(gx, golden["op_gx"])
