@@ -331,6 +331,34 @@ def ours(args) -> None:
                 "b200_mixed_mpix_s": size * size / t_ours / 1e6,
                 "speedup_over_port": t_port / t_ours}
 
+    # the exact DCT Neumann solver (solvers.py:224-262 on the device) on the same workload
+    dct = None
+    if rank == 0:
+        from gradient_domain_b200.solvers import DctPlan
+        dplan = DctPlan(size, size)
+        ud = torch.empty_like(f)
+        for _ in range(2):
+            for c in range(n_ch):
+                dplan.solve(f[c], ud[c])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            for c in range(n_ch):
+                dplan.solve(f[c], ud[c])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_dct = e0.elapsed_time(e1) / args.steps
+        dct = {"ms_per_step": ms_dct, "mpix_s": cells / (ms_dct / 1e3) / 1e6,
+               "note": "exact transform solve (the reference's solve_neumann algorithm), "
+                       "cuFFT FFTs with this library's permutation / twiddle / eigenvalue kernels"}
+        if not args.no_cpu:
+            from oracle import solvers as osolvers
+            ref0 = osolvers.solve_neumann(rhs_np[0], workers=os.cpu_count())
+            # laplacian(u) = b here; the MGPCG plan solves A x = -b, the same zero-mean u
+            dct["rel_l2_err_vs_fp64_oracle_channel0"] = float(
+                np.linalg.norm(ud[0].cpu().numpy() - ref0) / np.linalg.norm(ref0))
+        del dplan
+
     # end to end through the public API, pinned host buffers, copies timed
     host_in = torch.as_tensor(rhs_np).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
@@ -390,6 +418,7 @@ def ours(args) -> None:
         "gpu_launches": int(launches),
         "iterations": its, "relative_residual": resid, "converged": converged,
         "port_equivalent_fp64": port,
+        "dct_neumann": dct,
         "fp64_mgpcg": {"value": value64, "ms_per_step": ms64,
                        "iterations": [r.iterations for r in r64],
                        "mixed_over_fp64": value / value64},

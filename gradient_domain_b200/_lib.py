@@ -29,7 +29,8 @@ EXPORTS = (
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
     "gd_masked_rhs", "gd_guidance_divergence", "gd_tm_scratch_bytes", "gd_tm_log_luminance",
-    "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose",
+    "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose", "gd_dct_plan_create",
+    "gd_dct_workspace_bytes", "gd_dct_plan_bind", "gd_dct_solve_neumann", "gd_dct_plan_destroy",
 )
 
 
@@ -117,6 +118,11 @@ def _declare(lib: C.CDLL) -> None:
         "gd_guidance_divergence": (C.c_int, [_vp, C.POINTER(FieldDesc), _i32, _i32, _i32, _i32,
                                              _vp]),
         "gd_tm_scratch_bytes": (_sz, []),
+        "gd_dct_plan_create": (C.c_int, [_i32, _i32, C.POINTER(C.c_void_p)]),
+        "gd_dct_workspace_bytes": (_sz, [_vp]),
+        "gd_dct_plan_bind": (C.c_int, [_vp, _vp, _sz]),
+        "gd_dct_solve_neumann": (C.c_int, [_vp, _vp, _vp, _i32, _vp]),
+        "gd_dct_plan_destroy": (None, [_vp]),
         "gd_tm_log_luminance": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_tm_downsample": (C.c_int, [_vp, _vp, _i32, _i32, _vp]),
         "gd_tm_level_factor": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _f64, _f64, _f64,

@@ -19,6 +19,11 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgd_poisson.so")
 
+# cuFFT runs the FFTs of the DCT Neumann solver (gd_dct.cu)
+LINK = ["-lcufft", "-Xlinker", "-rpath," + os.path.join(
+    os.path.dirname(os.path.dirname(os.path.realpath(os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")))),
+    "lib64")]
+
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -54,7 +59,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         return LIB
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *NVCC_FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"),
-           "-o", tmp, *sources()]
+           "-o", tmp, *sources(), *LINK]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

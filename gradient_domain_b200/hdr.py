@@ -5,9 +5,9 @@ Same interface as gradient-domain/src/gradient_domain/hdr.py: ``ToneMapConfig``
 ``tone_map`` runs on the device from the uploaded radiance to the display
 image: log-luminance, the attenuation pyramid (binomial downsampling, central
 gradients, per-level factors propagated coarse to fine), the attenuated field
-and its divergence, the Neumann MGPCG, and the exposure / saturation /
-percentile normalisation (gd_tonemap.cu, gd_rhs.cu); only the image and the
-factor come back.
+and its divergence, the Neumann solve (the reference's exact DCT algorithm,
+gd_dct.cu), and the exposure / saturation / percentile normalisation
+(gd_tonemap.cu, gd_rhs.cu); only the image and the factor come back.
 """
 
 from __future__ import annotations
@@ -102,9 +102,14 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
                           _lib.ptr(factor), 0.0, 0.0, 0.0)
     _lib.check(lib.gd_guidance_divergence(_lib.ptr(div), C.byref(desc), 0, 0, h, w, st),
                "gd_guidance_divergence")
-    plan = cached_plan((Instance(h, w, "neumann", True),), SolveParams(tolerance=NEUMANN_TOLERANCE))
     compressed = torch.zeros_like(div)
-    plan.solve([div], [compressed], scale=-1.0)
+    if h >= 2 and w >= 2:  # the reference's exact transform solve (solvers.py:224-262)
+        from .solvers import _dct_plan
+        _dct_plan(h, w).solve(div, compressed)
+    else:
+        plan = cached_plan((Instance(h, w, "neumann", True),),
+                           SolveParams(tolerance=NEUMANN_TOLERANCE))
+        plan.solve([div], [compressed], scale=-1.0)
     image = torch.empty_like(rad)
     out = torch.empty_like(rad)
     _lib.check(lib.gd_tm_compose(_lib.ptr(out), _lib.ptr(image), _lib.ptr(rad), _lib.ptr(lum),

@@ -31,6 +31,7 @@ Every method runs on the device; there is no CPU path.
 
 from __future__ import annotations
 
+import ctypes as C
 import threading
 import time
 from collections import OrderedDict
@@ -210,19 +211,83 @@ def solve_system(b, method: str = "mgcg", spacing: float = 1.0, tolerance: float
 NEUMANN_EXACT_TOLERANCE = 1e-14
 
 
+class DctPlan:
+    """cuFFT-based DCT Neumann solver for one grid shape (gd_dct_* of the C ABI)."""
+
+    def __init__(self, h: int, w: int):
+        self.shape = (h, w)
+        self.device = _lib.device()
+        lib = _lib.lib()
+        handle = C.c_void_p()
+        _lib.check(lib.gd_dct_plan_create(h, w, C.byref(handle)), "gd_dct_plan_create")
+        self._handle = handle
+        nbytes = int(lib.gd_dct_workspace_bytes(handle))
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        _lib.check(lib.gd_dct_plan_bind(handle, _lib.ptr(self.workspace), nbytes),
+                   "gd_dct_plan_bind")
+
+    def solve(self, b: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
+        """u = zero-mean solution of laplacian(u) = b (FP64 device tensors, one row pitch)."""
+        for t in (b, u):
+            if (t.dtype != torch.float64 or t.device != self.device or tuple(t.shape) != self.shape
+                    or t.stride(1) != 1):
+                raise ValueError(f"expected {self.shape} float64 tensors on {self.device}")
+        if b.stride(0) != u.stride(0) or b.data_ptr() == u.data_ptr():
+            raise ValueError("b and u must share a row pitch and may not alias")
+        _lib.check(_lib.lib().gd_dct_solve_neumann(self._handle, _lib.ptr(b), _lib.ptr(u),
+                                                   u.stride(0), _lib.stream_handle()),
+                   "gd_dct_solve_neumann")
+        return u
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            try:
+                torch.cuda.current_stream(self.device).synchronize()
+                _lib.lib().gd_dct_plan_destroy(self._handle)
+            except Exception:
+                pass
+            self._handle = None
+
+
+_DCT_PLANS: OrderedDict = OrderedDict()
+
+
+def _dct_plan(h: int, w: int) -> DctPlan:
+    key = (h, w, torch.cuda.current_device())
+    with _PIPELINE_LOCK:
+        plan = _DCT_PLANS.pop(key, None)
+        if plan is None:
+            plan = DctPlan(h, w)
+        _DCT_PLANS[key] = plan
+        while len(_DCT_PLANS) > 8:
+            _DCT_PLANS.popitem(last=False)
+    return plan
+
+
 def solve_neumann(b, tolerance: float = NEUMANN_EXACT_TOLERANCE,
-                  max_iterations: int = 2000) -> np.ndarray:
+                  max_iterations: int = 2000, method: str = "mgcg") -> np.ndarray:
     """Zero-mean solution of ``laplacian(u) = b`` with homogeneous Neumann boundaries.
 
-    Replaces the DCT solve of solvers.py:224-262 with the B200 MGPCG on the
-    edge-replicated operator.  As there, any constant component of ``b`` is
-    discarded and the returned solution has zero mean.  The default tolerance
+    ``method="mgcg"`` (default) replaces the DCT solve of solvers.py:224-262
+    with the B200 MGPCG on the edge-replicated operator; the default tolerance
     drives the true relative residual to 1e-14, so that even the smoothest
     error mode is reduced to the rounding level of the exact transform solve.
+    ``method="dct"`` runs the reference's own algorithm (forward DCT-II,
+    division by the eigenvalues, inverse) on the device with cuFFT.  Either
+    way any constant component of ``b`` is discarded and the solution has
+    zero mean.
     """
     b = np.asarray(b, dtype=float)
     if b.ndim != 2:
         raise ValueError("solve_neumann expects a 2-D right-hand side")
+    if method == "dct":
+        if min(b.shape) < 2:
+            raise ValueError("the DCT solver needs at least 2 x 2 cells")
+        dev = _lib.device()
+        bd = _dev_array(b, dev)
+        return _dct_plan(*b.shape).solve(bd, torch.empty_like(bd)).cpu().numpy()
+    if method != "mgcg":
+        raise KeyError(f"unknown Neumann method {method!r}; choose 'mgcg' or 'dct'")
     params = SolveParams(tolerance=tolerance, max_iterations=max_iterations)
     u, _ = _plan_solve(b, 1.0, "neumann", params, zero_mean=True)
     return u

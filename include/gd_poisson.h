@@ -144,6 +144,22 @@ int gd_solve_finish(gd_plan plan, gd_report *reports);
 int gd_plan_apply_vcycle(gd_plan plan, int32_t instance, const double *r_dev,
                          double *z_dev, int32_t pitch, cudaStream_t stream);
 
+/* Exact Neumann solve by the discrete cosine transform, the algorithm of
+ * solvers.py:224-262 (replaces scipy dctn / idctn with cuFFT-based DCT-II
+ * kernels): u = zero-mean solution of laplacian(u) = b with edge-replicated
+ * (Neumann) boundaries, any constant component of b dropped.  Grids of at
+ * least 2 x 2.  The plan holds cuFFT plans made without work-area allocation;
+ * the caller binds a 256-byte aligned workspace of gd_dct_workspace_bytes
+ * (buffers and the cuFFT work area) before solving.  b and u have row pitch
+ * `pitch` (elements) and may not alias. */
+typedef struct gd_dct_plan_s *gd_dct_plan;
+int gd_dct_plan_create(int32_t h, int32_t w, gd_dct_plan *out);
+size_t gd_dct_workspace_bytes(gd_dct_plan plan);
+int gd_dct_plan_bind(gd_dct_plan plan, void *workspace_dev, size_t bytes);
+int gd_dct_solve_neumann(gd_dct_plan plan, const double *b_dev, double *u_dev, int32_t pitch,
+                         cudaStream_t stream);
+void gd_dct_plan_destroy(gd_dct_plan plan);
+
 /* Tone mapping around the Neumann solve (hdr.py:73-185), all FP64 row-major;
  * `scratch` is gd_tm_scratch_bytes() of device memory owned by the caller.
  *   gd_tm_log_luminance: lum = max(radiance . (0.2126, 0.7152, 0.0722), tiny),

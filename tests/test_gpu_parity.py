@@ -78,6 +78,23 @@ def test_solve_neumann_matches_golden(golden, key):
     assert abs(float(got.mean())) < 1e-12
 
 
+@pytest.mark.parametrize("shape", [(2, 2), (3, 5), (64, 64), (97, 130), (257, 2), (1024, 768)])
+def test_dct_neumann_matches_oracle(shape):
+    """The cuFFT DCT solver against the oracle's scipy DCT solve."""
+    rng = np.random.default_rng(shape[0] * 7 + shape[1])
+    b = rng.standard_normal(shape)
+    got = gd.solve_neumann(b, method="dct")
+    want = osolvers.solve_neumann(b)
+    assert _rel(got, want) <= 1e-12
+    assert abs(got.mean()) <= 1e-12 * np.abs(got).max()
+
+
+@pytest.mark.parametrize("key", ["neu32x40", "neu97x131", "neu64x64"])
+def test_dct_neumann_matches_golden(golden, key):
+    got = gd.solve_neumann(golden[key + "_b"], method="dct")
+    assert _rel(got, golden[key + "_u"]) <= 1e-12
+
+
 def test_neumann_exact_on_reference_pins():
     # gradient-domain/tests/test_solvers.py:90-101
     rng = np.random.default_rng(8)
