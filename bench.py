@@ -126,10 +126,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from gradient_domain_b200 import replicas
+    return replicas.rank_env()
 
 
 def cpu_baseline_tonemap(rhs: np.ndarray, budget_s: float = 20.0) -> dict:
@@ -183,19 +181,19 @@ def reference_arm(args) -> None:
 
 def ours(args) -> None:
     import torch
-    import torch.distributed as dist
 
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    from gradient_domain_b200 import workloads
+    from gradient_domain_b200 import replicas, workloads
     from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
     from gradient_domain_b200.solvers import solve_neumann_batch
 
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    replicas.init(world)
+
     dev = torch.device("cuda", local)
     size = args.size
-    rhs_np = workloads.tonemap_rhs(size, seed=1 + rank, channels=args.channels)
+    rhs_np = workloads.tonemap_rhs(size, seed=replicas.replica_seed(1, rank),
+                                   channels=args.channels)
     n_ch = rhs_np.shape[0]
     cells = n_ch * size * size
     f = torch.as_tensor(rhs_np).to(dev)
@@ -210,15 +208,10 @@ def ours(args) -> None:
         return p.solve(list(f), list(x), scale=-1.0)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(world)
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(v, world, dev)
 
     for _ in range(args.warmup):
         results = step(plan)
@@ -258,7 +251,7 @@ def ours(args) -> None:
     ms_prof = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     ktimes = plan.kernel_times()
     plan.set_profiling(False)
-    value = cells * world / (ms / 1e3) / 1e6
+    value = replicas.aggregate_rate(cells, world, ms / 1e3) / 1e6
     its = [r.iterations for r in results]
     resid = max(r.relative_residual for r in results)
     converged = all(r.converged for r in results)
@@ -290,7 +283,7 @@ def ours(args) -> None:
     e1.record(stream)
     torch.cuda.synchronize()
     ms64 = max_over_ranks(e0.elapsed_time(e1) / k64)
-    value64 = cells * world / (ms64 / 1e3) / 1e6
+    value64 = replicas.aggregate_rate(cells, world, ms64 / 1e3) / 1e6
     del plan64
 
     # the literal GPU port of the reference mgcg (vertex-centred V-cycle, one kernel per
@@ -373,7 +366,7 @@ def ours(args) -> None:
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) / args.steps
     ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall * 1e3))
-    e2e_value = cells * world / (ms_e2e / 1e3) / 1e6
+    e2e_value = replicas.aggregate_rate(cells, world, ms_e2e / 1e3) / 1e6
 
     # roofline of the dominant kernel (live CUDA-event durations)
     hbm, peak_kind = peaks()
@@ -436,18 +429,16 @@ def ours(args) -> None:
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 def _timed_steps(step, steps, warmup, world, dev):
     """Warm up, then device-time exactly `steps` calls of step() (max over ranks)."""
     import torch
-    import torch.distributed as dist
+    from gradient_domain_b200 import replicas
     for _ in range(warmup):
         out = step()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(world)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -456,28 +447,22 @@ def _timed_steps(step, steps, warmup, world, dev):
         out = step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms, out
+    return replicas.max_over_ranks(e0.elapsed_time(e1) / steps, world, dev), out
 
 
 def composite(args) -> None:
     """Masked seamless compositing, 2048 x 2048 x 3, star-polygon selection, tolerance 1e-8."""
     import torch
-    import torch.distributed as dist
+    from gradient_domain_b200 import replicas
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    replicas.init(world)
     import gradient_domain_b200 as gd
     from gradient_domain_b200 import workloads
     from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
     dev = torch.device("cuda", local)
     size = args.size if args.size != 4096 else 2048
-    src, tgt, mask = workloads.composite_case(size, seed=2 + rank)
+    src, tgt, mask = workloads.composite_case(size, seed=replicas.replica_seed(2, rank))
     f_np, unk_np, win = workloads.masked_system(src, tgt, mask)
     n_ch, hb, wb = f_np.shape
     unknowns = int(unk_np.sum())
@@ -501,7 +486,7 @@ def composite(args) -> None:
     ms_prof, _ = _timed_steps(step, args.steps, 0, world, dev)
     kt = plan.kernel_times()
     plan.set_profiling(False)
-    value = unknowns * n_ch * world / (ms / 1e3) / 1e6
+    value = replicas.aggregate_rate(unknowns * n_ch, world, ms / 1e3) / 1e6
     # end to end: the public seamless_clone from host arrays (field, RHS and copies included)
     t0 = time.perf_counter()
     e2e_steps = max(1, args.steps // 2)
@@ -544,22 +529,20 @@ def composite(args) -> None:
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 def batch(args) -> None:
     """256 uneven images (1 or 3 channels; Neumann blobs or masked polygons) in one plan."""
     import torch
-    import torch.distributed as dist
+    from gradient_domain_b200 import replicas
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    replicas.init(world)
     from gradient_domain_b200 import workloads
     from gradient_domain_b200.plan import Instance, PoissonPlan, SolveParams
     dev = torch.device("cuda", local)
-    items = workloads.batch_instances(args.count, seed=3 + rank)
+    items = workloads.batch_instances(args.count, seed=replicas.replica_seed(3, rank))
     insts, fs, xs, masks = [], [], [], []
     for it in items:
         c, h, w = it["f"].shape
@@ -583,7 +566,7 @@ def batch(args) -> None:
         return plan.solve(fs, xs, scale=1.0)
 
     ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
-    value = cells * world / (ms / 1e3) / 1e6
+    value = replicas.aggregate_rate(cells, world, ms / 1e3) / 1e6
     its = [r.iterations for r in res]
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
@@ -600,8 +583,7 @@ def batch(args) -> None:
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 def main():
