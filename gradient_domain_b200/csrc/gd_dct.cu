@@ -27,7 +27,7 @@ struct gd_dct_plan_s {
   cufftHandle fr = 0, fc = 0, ir = 0, ic = 0;  // forward / inverse, along rows (w) / columns (h)
   bool made[4] = {false, false, false, false};
   size_t work = 0;                             // largest cuFFT work area
-  size_t o_r1 = 0, o_r2 = 0, o_cx = 0, o_wk = 0, total = 0;
+  size_t o_r1 = 0, o_r2 = 0, o_cx = 0, o_wk = 0, o_tab = 0, total = 0;
   char *ws = nullptr;
 };
 
@@ -53,8 +53,31 @@ __device__ __forceinline__ double dct_scale(int k, int n) {
   return k == 0 ? sqrt(1.0 / (double)n) : sqrt(2.0 / (double)n);
 }
 
+// Per-plan tables, computed once at bind: twiddles (cos, sin)(pi k / 2n) for
+// both lengths and the eigenvalue terms 2 cos(pi i / n).
+struct DctTables {
+  double2 *tw_w, *tw_h;  // w and h entries
+  double *eig_w, *eig_h;
+};
+
+__global__ void k_dct_tables(DctTables t, int h, int w) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double s, c;
+  if (k < w) {
+    sincospi((double)k / (2.0 * (double)w), &s, &c);
+    t.tw_w[k] = make_double2(c, s);
+    t.eig_w[k] = 2.0 * cos(M_PI * (double)k / (double)w);
+  }
+  if (k < h) {
+    sincospi((double)k / (2.0 * (double)h), &s, &c);
+    t.tw_h[k] = make_double2(c, s);
+    t.eig_h[k] = 2.0 * cos(M_PI * (double)k / (double)h);
+  }
+}
+
 // Orthonormal DCT coefficient k of row r from the half spectrum V (n/2 + 1 per row).
-__device__ __forceinline__ double dct_coef(const cufftDoubleComplex *V, int r, int k, int n) {
+__device__ __forceinline__ double dct_coef(const cufftDoubleComplex *V, const double2 *tw, int r,
+                                           int k, int n) {
   const int nh = n / 2 + 1;
   cufftDoubleComplex z;
   if (k < nh) {
@@ -63,31 +86,37 @@ __device__ __forceinline__ double dct_coef(const cufftDoubleComplex *V, int r, i
     z = V[(long long)r * nh + (n - k)];
     z.y = -z.y;
   }
-  double s, c;
-  sincospi((double)k / (2.0 * (double)n), &s, &c);
-  return (z.x * c + z.y * s) * dct_scale(k, n);
+  const double2 t = tw[k];
+  return (z.x * t.x + z.y * t.y) * dct_scale(k, n);
 }
 
-// out (n x rows) = transpose of the row coefficients (rows x n), via a shared tile.
+// Position of element r in the even/odd reordering of a length-n sequence.
+__device__ __forceinline__ int dct_pos(int r, int n) {
+  return (r & 1) ? n - 1 - (r >> 1) : (r >> 1);
+}
+
+// out (n x rows) = transpose of the row coefficients (rows x n), via a shared
+// tile, each output row already in the even/odd order of the next transform.
 __global__ void k_dct_twiddle_t(double *__restrict__ out, const cufftDoubleComplex *__restrict__ V,
-                                int rows, int n) {
+                                const double2 *__restrict__ tw, int rows, int n) {
   __shared__ double tile[kT][kT + 1];
   const int r0 = blockIdx.y * kT, k0 = blockIdx.x * kT;
   for (int dy = threadIdx.y; dy < kT; dy += blockDim.y) {
     const int r = r0 + dy, k = k0 + threadIdx.x;
-    if (r < rows && k < n) tile[dy][threadIdx.x] = dct_coef(V, r, k, n);
+    if (r < rows && k < n) tile[dy][threadIdx.x] = dct_coef(V, tw, r, k, n);
   }
   __syncthreads();
   for (int dy = threadIdx.y; dy < kT; dy += blockDim.y) {
     const int k = k0 + dy, r = r0 + threadIdx.x;
-    if (k < n && r < rows) out[(long long)k * rows + r] = tile[threadIdx.x][dy];
+    if (k < n && r < rows) out[(long long)k * rows + dct_pos(r, rows)] = tile[threadIdx.x][dy];
   }
 }
 
 // Second axis: row j of the transposed layout holds column j of the image;
 // coefficient (i, j) divided by the eigenvalue, the constant mode set to zero.
 __global__ void k_dct_twiddle_div(double *__restrict__ out,
-                                  const cufftDoubleComplex *__restrict__ V, int w, int h) {
+                                  const cufftDoubleComplex *__restrict__ V, DctTables t, int w,
+                                  int h) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (long long)w * h) return;
   const int j = (int)(q / h), i = (int)(q % h);
@@ -95,15 +124,14 @@ __global__ void k_dct_twiddle_div(double *__restrict__ out,
     out[q] = 0.0;
     return;
   }
-  const double lam = 2.0 * cos(M_PI * (double)i / (double)h) +
-                     2.0 * cos(M_PI * (double)j / (double)w) - 4.0;
-  out[q] = dct_coef(V, j, i, h) / lam;
+  const double lam = t.eig_h[i] + t.eig_w[j] - 4.0;
+  out[q] = dct_coef(V, t.tw_h, j, i, h) / lam;
 }
 
 // Inverse, first step: W_k = exp(i pi k / 2n) (X_k - i X_{n-k}) for k <= n/2,
 // X the unscaled coefficients of row r.
 __global__ void k_idct_pretwiddle(cufftDoubleComplex *__restrict__ W, const double *__restrict__ Xo,
-                                  int rows, int n) {
+                                  const double2 *__restrict__ tw, int rows, int n) {
   const int nh = n / 2 + 1;
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= (long long)rows * nh) return;
@@ -111,8 +139,7 @@ __global__ void k_idct_pretwiddle(cufftDoubleComplex *__restrict__ W, const doub
   const double *row = Xo + (long long)r * n;
   const double a = row[k] / dct_scale(k, n);
   const double b = k == 0 ? 0.0 : row[n - k] / dct_scale(n - k, n);
-  double s, c;
-  sincospi((double)k / (2.0 * (double)n), &s, &c);
+  const double c = tw[k].x, s = tw[k].y;
   // (c + i s)(a - i b) = (c a + s b) + i (s a - c b)
   W[q].x = c * a + s * b;
   W[q].y = s * a - c * b;
@@ -211,12 +238,26 @@ extern "C" int gd_dct_plan_create(int32_t h, int32_t w, gd_dct_plan *out) {
   o = a256(o + nc * sizeof(cufftDoubleComplex));
   p->o_wk = o;
   o = a256(o + std::max<size_t>(p->work, 256));
+  p->o_tab = o;
+  o = a256(o + (size_t)(h + w) * (sizeof(double2) + sizeof(double)));
   p->total = o;
   *out = p;
   return GD_OK;
 }
 
 extern "C" size_t gd_dct_workspace_bytes(gd_dct_plan p) { return p ? p->total : 0; }
+
+namespace {
+DctTables dct_tables(gd_dct_plan p) {
+  DctTables t;
+  char *b = p->ws + p->o_tab;
+  t.tw_w = reinterpret_cast<double2 *>(b);
+  t.tw_h = t.tw_w + p->w;
+  t.eig_w = reinterpret_cast<double *>(t.tw_h + p->h);
+  t.eig_h = t.eig_w + p->w;
+  return t;
+}
+}  // namespace
 
 extern "C" int gd_dct_plan_bind(gd_dct_plan p, void *ws, size_t bytes) {
   GD_REQUIRE(p && ws, GD_ERR_ARG, "gd_dct_plan_bind: bad arguments");
@@ -230,6 +271,11 @@ extern "C" int gd_dct_plan_bind(gd_dct_plan p, void *ws, size_t bytes) {
   for (cufftHandle hd : hs)
     GD_REQUIRE(cufftSetWorkArea(hd, wk) == CUFFT_SUCCESS, GD_ERR_CUDA,
                "gd_dct_plan_bind: cufftSetWorkArea failed");
+  const int n = std::max(p->h, p->w);
+  k_dct_tables<<<nblocks(n, 256), 256>>>(dct_tables(p), p->h, p->w);
+  GD_CHECK_LAUNCH();
+  // the tables must be complete before a solve on any stream (set-up, once per plan)
+  GD_CHECK_CUDA(cudaStreamSynchronize(nullptr));
   return GD_OK;
 }
 
@@ -247,21 +293,24 @@ extern "C" int gd_dct_solve_neumann(gd_dct_plan p, const double *b, double *u, i
     GD_REQUIRE(cufftSetStream(hd, st) == CUFFT_SUCCESS, GD_ERR_CUDA,
                "gd_dct_solve_neumann: cufftSetStream failed");
   const dim3 tb(kT, 8);
-  // forward along rows (length w), then the transposed columns (length h)
+  const DctTables t = dct_tables(p);
+  // forward along rows (length w), then the transposed columns (length h); the
+  // transposing twiddle writes the columns already reordered for their FFT
   k_dct_permute<<<nblocks(n, 256), 256, 0, st>>>(r1, b, h, w, pitch);
   GD_REQUIRE(cufftExecD2Z(p->fr, r1, cx) == CUFFT_SUCCESS, GD_ERR_CUDA,
              "gd_dct_solve_neumann: forward row FFT failed");
-  k_dct_twiddle_t<<<dim3(nblocks(w, kT), nblocks(h, kT)), tb, 0, st>>>(r2, cx, h, w);
-  k_dct_permute<<<nblocks(n, 256), 256, 0, st>>>(r1, r2, w, h, h);
-  GD_REQUIRE(cufftExecD2Z(p->fc, r1, cx) == CUFFT_SUCCESS, GD_ERR_CUDA,
+  k_dct_twiddle_t<<<dim3(nblocks(w, kT), nblocks(h, kT)), tb, 0, st>>>(r2, cx, t.tw_w, h, w);
+  GD_REQUIRE(cufftExecD2Z(p->fc, r2, cx) == CUFFT_SUCCESS, GD_ERR_CUDA,
              "gd_dct_solve_neumann: forward column FFT failed");
-  k_dct_twiddle_div<<<nblocks(n, 256), 256, 0, st>>>(r2, cx, w, h);
+  k_dct_twiddle_div<<<nblocks(n, 256), 256, 0, st>>>(r2, cx, t, w, h);
   // inverse along the transposed columns (length h), transpose back, rows (length w)
-  k_idct_pretwiddle<<<nblocks((long long)w * (h / 2 + 1), 256), 256, 0, st>>>(cx, r2, w, h);
+  k_idct_pretwiddle<<<nblocks((long long)w * (h / 2 + 1), 256), 256, 0, st>>>(cx, r2, t.tw_h, w,
+                                                                              h);
   GD_REQUIRE(cufftExecZ2D(p->ir, cx, r1) == CUFFT_SUCCESS, GD_ERR_CUDA,
              "gd_dct_solve_neumann: inverse column FFT failed");
   k_idct_unpermute_t<<<dim3(nblocks(h, kT), nblocks(w, kT)), tb, 0, st>>>(r2, r1, w, h);
-  k_idct_pretwiddle<<<nblocks((long long)h * (w / 2 + 1), 256), 256, 0, st>>>(cx, r2, h, w);
+  k_idct_pretwiddle<<<nblocks((long long)h * (w / 2 + 1), 256), 256, 0, st>>>(cx, r2, t.tw_w, h,
+                                                                              w);
   GD_REQUIRE(cufftExecZ2D(p->ic, cx, r1) == CUFFT_SUCCESS, GD_ERR_CUDA,
              "gd_dct_solve_neumann: inverse row FFT failed");
   k_idct_unpermute<<<nblocks(n, 256), 256, 0, st>>>(u, pitch, r1, h, w);
