@@ -28,7 +28,11 @@ constexpr int kBThreads = 1024;    // bottom kernel
 constexpr int kLastWarps = kFThreads / 32;
 
 enum : int { BC_DIR = 0, BC_NEU = 1, BC_MASK = 2 };
-enum : int { FLAG_RU = 1 };
+// FLAG_RU: an FP64 refresh is due (set by cgupdate, cleared by the residual).
+// FLAG_DZERO: the correction d restarts from zero (set when a solve starts and
+// at every refresh, cleared by the next cgupdate, which then writes d = alpha p
+// without reading the stale d, so nobody has to write zeros into it).
+enum : int { FLAG_RU = 1, FLAG_DZERO = 2 };
 
 struct LevelInfo {
   int ny, nx, pitch, inst;

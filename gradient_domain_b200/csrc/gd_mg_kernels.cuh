@@ -303,13 +303,17 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
 // Elementwise level-0 kernels over 64 x 128 tiles (the Krylov kernels with
 // halos are in gd_stream.cuh).
 
-// x += d, d = 0 for instances with a pending FP64 refresh.  A thread owns one
+// x += d for instances with a pending FP64 refresh (d then restarts from zero
+// through FLAG_DZERO instead of being cleared here).  A thread owns one
 // column of the 64 x 128 tile, so every warp access is 32 consecutive
 // elements; the independent rows are unrolled for several loads in flight.
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
-  if (!(a.st[tl.inst].flags & FLAG_RU)) return;
+  // nothing to fold without a refresh, or when d restarted since the last one
+  // (a breakdown can request a refresh before any cgupdate wrote d)
+  const int flags = a.st[tl.inst].flags;
+  if (!(flags & FLAG_RU) || (flags & FLAG_DZERO)) return;
   // descriptor fields in registers: the stores below could alias the descriptor
   const InstInfo &Ig = a.inst[tl.inst];
   const int ny = Ig.ny, nx = Ig.nx, pitch = Ig.pitch;
@@ -333,10 +337,7 @@ __global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int y = yb + k;
-      if (y < y1) {
-        X[(long long)y * upitch + x] = xv[k] + (double)dv[k];
-        d[(long long)y * pitch + x] = T(0);
-      }
+      if (y < y1) X[(long long)y * upitch + x] = xv[k] + (double)dv[k];
     }
   }
 }

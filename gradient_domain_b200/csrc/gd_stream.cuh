@@ -886,7 +886,7 @@ template <typename T, bool INT>
 __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInfo &L,
                                                 const ClassTable<T> &tab, int lane, int x0,
                                                 int y0, int y1, T alpha, const T *p, T *d, T *r,
-                                                unsigned char *smem) {
+                                                bool dzero, unsigned char *smem) {
   const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
   const Ring<T> rp(reinterpret_cast<T *>(smem));
   const Ring<T> rd(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
@@ -898,7 +898,7 @@ __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInf
   auto issue = [&](int q) {
     const int y = y0 - 1 + q;
     rp.issue(q, p, L, y, x0);
-    rd.issue(q, d, L, y, x0);
+    if (!dzero) rd.issue(q, d, L, y, x0);
     rr.issue(q, r, L, y, x0);
     if (edge_lane) ep.issue(q, p, L, y, xe);
     __pipeline_commit();
@@ -912,7 +912,7 @@ __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInf
     const V4<T> pp = rp.read(step);
     dcur = dnext;
     rcur = rnext;
-    dnext = rd.read(step);
+    dnext = dzero ? zero4<T>() : rd.read(step);
     rnext = rr.read(step);
     edge_next = edge_lane ? ep.read(step) : T(0);
     issue(step + kRing - 1);
@@ -947,7 +947,7 @@ __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInf
         st4(r + g, rv);
       } else {
         for (int j = 0; j < 4 && x0 + j < L.nx; ++j) {
-          d[g + j] += alpha * cu.v[j];
+          d[g + j] = (dzero ? T(0) : d[g + j]) + alpha * cu.v[j];
           const T rn = r[g + j] - alpha * ap.v[j];
           r[g + j] = rn;
           part += (double)rn * (double)rn;
@@ -982,11 +982,12 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
       const T *p = a.arena + p_offset(I, a.st[tl.inst].pcur);
       T *d = a.arena + I.d_off;
       T *r = a.arena + I.r_off;
+      const bool dzero = a.st[tl.inst].flags & FLAG_DZERO;
       extern __shared__ __align__(16) unsigned char smem[];
       if (strip_interior(L, y0, y1 - 1, xl, xl + 127))
-        part = cgupdate_rows<T, true>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, smem);
+        part = cgupdate_rows<T, true>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, dzero, smem);
       else
-        part = cgupdate_rows<T, false>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, smem);
+        part = cgupdate_rows<T, false>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, dzero, smem);
     }
   }
   part = block_sum<kThreads>(part);
@@ -1001,6 +1002,7 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
     if ((threadIdx.x & 31) == 0) {
       S.rr = rr;
       S.iters += 1;
+      S.flags &= ~FLAG_DZERO;  // every CTA of this launch has read it
       if (rr <= a.delta2 * S.rr_ref || rr <= a.tol2 * S.ff || S.iters >= a.max_iter ||
           !isfinite(rr))
         S.flags |= FLAG_RU;
@@ -1036,7 +1038,6 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
     const long long upitch = Ig.upitch;
     const double scale = Ig.scale;
     T *const r = a.arena + Ig.r_off;
-    T *const dz = a.arena + Ig.d_off;
     const LevelInfo L = a.lv[Ig.level0];
     const int lane = threadIdx.x & 31;
     const int col = tl.tx * kFTX + threadIdx.x;
@@ -1111,7 +1112,6 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
         r[(long long)y * L.pitch + col] = T(0);
         if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
       }
-      if (INIT && in_col) dz[(long long)y * L.pitch + col] = T(0);
       xu = xc;
       xc = xd;
     }
@@ -1164,7 +1164,7 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
         } else if (S.status == GD_ACTIVE && S.iters >= a.max_iter) {
           S.status = GD_MAX_ITERATIONS;
         }
-        S.flags = 0;
+        S.flags = FLAG_DZERO;  // the correction restarts after every refresh
       }
     }
     if (lane == 0 && S.status == GD_ACTIVE) ++active;
