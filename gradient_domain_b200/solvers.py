@@ -294,7 +294,8 @@ def solve_neumann(b, tolerance: float = NEUMANN_EXACT_TOLERANCE,
 
 
 def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_iterations: int = 2000,
-                        precision: str = "mixed", out: torch.Tensor | None = None):
+                        precision: str = "mixed", out: torch.Tensor | None = None,
+                        method: str = "mgcg"):
     """:func:`solve_neumann` for a stack of right-hand sides ``(n, h, w)`` in one batched solve.
 
     ``b`` may be a NumPy array or a (preferably pinned) CPU torch tensor; with
@@ -303,9 +304,28 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
     through the same kernel launches (they are instances of one plan), except
     when ``b`` and ``out`` are both pinned FP64 tensors: then each problem has
     its own plan and stream, so host-device copies overlap the solves (the
-    results are bitwise the same either way).
+    results are bitwise the same either way).  ``method="dct"`` solves each
+    right-hand side with the exact transform solver instead.
     """
     dev = _lib.device()
+    if method == "dct":
+        f = (b.to(device=dev, dtype=torch.float64) if isinstance(b, torch.Tensor)
+             else torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64)).to(dev))
+        if f.dim() != 3 or min(f.shape[1:]) < 2:
+            raise ValueError("solve_neumann_batch expects an (n, h, w) stack with h, w >= 2")
+        f = f.contiguous()
+        plan = _dct_plan(f.shape[1], f.shape[2])
+        x = torch.empty_like(f)
+        for k in range(f.shape[0]):
+            plan.solve(f[k], x[k])
+        solve_neumann_batch.last_results = []
+        if out is not None:
+            out.copy_(x, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            return out
+        return x.cpu().numpy()
+    if method != "mgcg":
+        raise KeyError(f"unknown Neumann method {method!r}; choose 'mgcg' or 'dct'")
     if (isinstance(b, torch.Tensor) and isinstance(out, torch.Tensor) and b.dim() == 3
             and b.shape[0] > 1 and b.dtype == torch.float64 and out.dtype == torch.float64
             and b.device.type == "cpu" and out.device.type == "cpu" and b.is_pinned()

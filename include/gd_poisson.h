@@ -128,7 +128,9 @@ int gd_solve(gd_plan plan, const double *const *f_dev, double *const *x_dev,
              const int32_t *pitch, const double *scale, cudaStream_t stream,
              gd_report *reports);
 
-/* gd_solve in two halves, so that copies and other work can overlap a solve.
+/* gd_solve in two halves, so that copies and other work can overlap a solve
+ * (no counterpart in the reference, whose solves are synchronous Python calls,
+ * solvers.py:171-221).
  * gd_solve_async enqueues the solve on `stream` and, once the plan has been
  * solved before (its whole solve is then one CUDA graph with a device-side
  * loop), returns without waiting; a plan's first solve and profiled solves

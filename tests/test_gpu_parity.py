@@ -89,6 +89,16 @@ def test_dct_neumann_matches_oracle(shape):
     assert abs(got.mean()) <= 1e-12 * np.abs(got).max()
 
 
+def test_dct_neumann_batch_matches_single():
+    rng = np.random.default_rng(41)
+    stack = rng.standard_normal((3, 50, 70))
+    got = gd.solve_neumann_batch(stack, method="dct")
+    for k in range(3):
+        assert np.array_equal(got[k], gd.solve_neumann(stack[k], method="dct"))
+    with pytest.raises(KeyError):
+        gd.solve_neumann_batch(stack, method="fft")
+
+
 @pytest.mark.parametrize("key", ["neu32x40", "neu97x131", "neu64x64"])
 def test_dct_neumann_matches_golden(golden, key):
     got = gd.solve_neumann(golden[key + "_b"], method="dct")
