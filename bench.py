@@ -45,9 +45,8 @@ BYTES_PER_CELL_MIXED = {
     "up0": 4 + 4 + 1 + 4, "up": 4 + 4 + 1 + 4,      # read b, w, coarse e; write u
     "pupdate": 4 + 4 + 4,                   # read z, p; write p
     "cgupdate": 12 + 8,                     # read p, d, r; write d, r
-    "resid": 8 + 8 + 4,                     # read x, f; write r (refresh iterations)
-    "fold": 8 + 4 + 8 + 4,                  # read x, d; write x, d (refresh iterations)
-    "init": 8 + 8 + 8 + 16,                 # read f twice, x; write r, d, p, z
+    "resid": 8 + 4 + 8 + 8 + 4,             # read x, d, f; write x + d, r (refresh iterations)
+    "init": 8 + 8 + 8 + 4,                  # read f twice, x; write r
     "mean": 8 + 16,                         # read x; read+write x
 }
 
@@ -57,7 +56,7 @@ def bytes_per_cell(kind: str, fp64: bool) -> float:
     if not fp64:
         return b
     fp32_part = {"down0": 9, "down": 9, "up0": 13, "up": 13, "pupdate": 12, "cgupdate": 20,
-                 "resid": 4, "fold": 8, "init": 16, "mean": 0}.get(kind, 0)
+                 "resid": 8, "init": 4, "mean": 0}.get(kind, 0)
     return b + fp32_part
 
 

@@ -37,10 +37,10 @@ struct gd_plan_s {
   int fine_base = 0, fine_count = 0, depth = 0;
   std::vector<int> down_base, down_count, up_base, up_count;     // strip maps per level
   std::vector<int> tdown_base, tdown_count, tup_base, tup_count;  // tile maps per level
-  size_t arena_elems = 0, code_bytes = 0, dense_elems = 0;
+  size_t arena_elems = 0, code_bytes = 0, dense_elems = 0, xs_elems = 0;
   int max_partials = 1;
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
-         o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, o_trip = 0, total = 0;
+         o_xs = 0, o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, o_trip = 0, total = 0;
   size_t bottom_smem = 0;
   char *ws = nullptr;
   bool prepared = false;
@@ -201,6 +201,10 @@ struct Runner {
                          (int)st::pupdate_smem<T>());
     cudaFuncSetAttribute(st::k_cgupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)st::cgupdate_smem<T>());
+    cudaFuncSetAttribute(st::k_refresh_s<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)st::refresh_smem<T>());
+    cudaFuncSetAttribute(st::k_refresh_s<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)st::refresh_smem<T>());
   }
 
   static Args<T> args(gd_plan p) {
@@ -209,6 +213,7 @@ struct Runner {
     a.inst = reinterpret_cast<const InstInfo *>(p->ws + p->o_inst);
     a.st = reinterpret_cast<InstState *>(p->ws + p->o_st);
     a.arena = reinterpret_cast<T *>(p->ws + p->o_arena);
+    a.xs = reinterpret_cast<double *>(p->ws + p->o_xs);
     a.codes = reinterpret_cast<const unsigned char *>(p->ws + p->o_codes);
     a.dense = reinterpret_cast<const double *>(p->ws + p->o_dense);
     a.part0 = reinterpret_cast<double *>(p->ws + p->o_p0);
@@ -277,11 +282,8 @@ struct Runner {
     prof_begin(p, GD_K_CGUPDATE, c, st);
     st::k_cgupdate_s<T><<<p->fine_count, st::kThreads, st::cgupdate_smem<T>(), st>>>(f);
     prof_end(p, st);
-    prof_begin(p, GD_K_FOLD, c, st);
-    k_fold<T><<<p->fine_count, kFThreads, 0, st>>>(f);
-    prof_end(p, st);
     prof_begin(p, GD_K_RESID, c, st);
-    st::k_resid_s<T, false><<<p->fine_count, st::kThreads, st::resid_smem<T>(), st>>>(f);
+    st::k_refresh_s<T, false><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(f);
     prof_end(p, st);
   }
 
@@ -400,7 +402,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     cursor = align_up(cursor + elems, align_el);
     return (long long)off;
   };
-  size_t arena = 0, codes = 0, dense = 0;
+  size_t arena = 0, codes = 0, dense = 0, xs = 0;
   std::vector<int> bottoms(p->n);
   for (int i = 0; i < p->n; ++i) {
     const gd_grid_desc &g = grids[i];
@@ -416,6 +418,8 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     I.d_off = take(arena, cells0);
     I.z_off = take(arena, cells0);
     I.q_off = take(arena, cells0);
+    I.xs_off = (long long)xs;
+    xs = align_up(xs + cells0, kArrayAlign / sizeof(double));
     I.level0 = (int)p->lv.size();
     int ny = I.ny, nx = I.nx, level = 0;
     int bottom = -1;
@@ -571,6 +575,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   p->arena_elems = arena;
   p->code_bytes = std::max<size_t>(codes, kArrayAlign);
   p->dense_elems = std::max<size_t>(dense, 32);
+  p->xs_elems = xs;
   // workspace
   size_t o = 0;
   auto sect = [&](size_t bytes) {
@@ -585,6 +590,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   p->o_arena = sect(p->arena_elems * es);
   p->o_codes = sect(p->code_bytes);
   p->o_dense = sect(p->dense_elems * sizeof(double));
+  p->o_xs = sect(p->xs_elems * sizeof(double));
   p->o_p0 = sect(p->max_partials * sizeof(double));
   p->o_p1 = sect(p->max_partials * sizeof(double));
   p->o_cnt = sect(16 * sizeof(unsigned));
@@ -628,7 +634,7 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);
   else Runner<float>::dispatch_attrs(p->prm.pre_sweeps);
   p->h_st_bytes = sizeof(InstState) * n;
-  p->h_nact = static_cast<int *>(pinned_get(sizeof(int)));
+  p->h_nact = static_cast<int *>(pinned_get(2 * sizeof(int)));  // active count, error word
   p->h_st = static_cast<InstState *>(pinned_get(p->h_st_bytes));
   p->h_inst_bytes = sizeof(InstInfo) * n;
   p->h_inst = static_cast<InstInfo *>(pinned_get(p->h_inst_bytes));
@@ -652,7 +658,7 @@ extern "C" void gd_plan_destroy(gd_plan p) {
   if (p->gexec) cudaGraphExecDestroy(p->gexec);
   if (p->done_ev) cudaEventDestroy(p->done_ev);
   capture_stream_put(p->cap_device, p->cap);
-  pinned_put(p->h_nact, sizeof(int));
+  pinned_put(p->h_nact, 2 * sizeof(int));
   pinned_put(p->h_st, p->h_st_bytes);
   pinned_put(p->h_inst, p->h_inst_bytes);
   delete p;
@@ -738,15 +744,7 @@ template <typename T>
 void launch_init(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
   k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  st::k_resid_s<T, true><<<p->fine_count, st::kThreads, st::resid_smem<T>(), st>>>(fine);
-  prof_end(p, st);
-}
-
-template <typename T>
-void launch_mean(gd_plan p, const Args<T> &fine, cudaStream_t st) {
-  prof_begin(p, GD_K_MEAN, p->fine_cells, st);
-  k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  st::k_refresh_s<T, true><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(fine);
   prof_end(p, st);
 }
 
@@ -754,6 +752,17 @@ bool plan_any_mean(gd_plan p) {
   for (int i = 0; i < p->n; ++i)
     if (p->inst[i].zero_mean) return true;
   return false;
+}
+
+// After the loop: the mean of zero-mean instances, then the solution into the
+// caller's buffer (mean subtracted; copied from the plan's copy where the last
+// refresh left it there).
+template <typename T>
+void launch_finish(gd_plan p, const Args<T> &fine, cudaStream_t st) {
+  prof_begin(p, GD_K_MEAN, p->fine_cells, st);
+  if (plan_any_mean(p)) k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  prof_end(p, st);
 }
 
 int loop_cap(gd_plan p) {
@@ -802,7 +811,7 @@ int build_solve_graph(gd_plan p, const Args<T> &a, const Args<T> &fine) {
     if ((e = cudaStreamUpdateCaptureDependencies(cs, &wn, 1, cudaStreamSetCaptureDependencies)) !=
         cudaSuccess)
       break;
-    if (plan_any_mean(p)) launch_mean(p, fine, cs);
+    launch_finish(p, fine, cs);
     e = cudaGetLastError();
   } while (0);
   cudaGraph_t g = nullptr;
@@ -869,13 +878,13 @@ int enqueue_solve(gd_plan p, cudaStream_t st) {
       GD_CHECK_CUDA(cudaStreamSynchronize(st));
       prof_collect(p);
     }
-    if (plan_any_mean(p)) {
-      launch_mean(p, fine, st);
-      GD_CHECK_LAUNCH();
-    }
+    launch_finish(p, fine, st);
+    GD_CHECK_LAUNCH();
   }
   GD_CHECK_CUDA(cudaMemcpyAsync(p->h_st, p->ws + p->o_st, sizeof(InstState) * p->n,
                                 cudaMemcpyDeviceToHost, st));
+  GD_CHECK_CUDA(cudaMemcpyAsync(p->h_nact + 1, p->ws + p->o_cnt + kErrWord * sizeof(unsigned),
+                                sizeof(int), cudaMemcpyDeviceToHost, st));
   if (!p->done_ev) GD_CHECK_CUDA(cudaEventCreateWithFlags(&p->done_ev, cudaEventDisableTiming));
   GD_CHECK_CUDA(cudaEventRecord(p->done_ev, st));
   ++p->solves;
@@ -889,6 +898,9 @@ int collect_reports(gd_plan p, gd_report *reports) {
   GD_CHECK_CUDA(cudaEventSynchronize(p->done_ev));
   p->pending = false;
   prof_collect(p);
+  GD_REQUIRE(p->h_nact[1] == 0, GD_ERR_CUDA,
+             "solve: a kernel's bounded wait for its bulk copies gave up (error word %#x); "
+             "the solution is not valid", (unsigned)p->h_nact[1]);
   for (int i = 0; i < p->n; ++i) {
     const InstState &S = p->h_st[i];
     gd_report &R = reports[i];

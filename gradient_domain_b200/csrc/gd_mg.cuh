@@ -33,6 +33,9 @@ enum : int { BC_DIR = 0, BC_NEU = 1, BC_MASK = 2 };
 // at every refresh, cleared by the next cgupdate, which then writes d = alpha p
 // without reading the stale d, so nobody has to write zeros into it).
 enum : int { FLAG_RU = 1, FLAG_DZERO = 2 };
+// Slot of the plan's counter array that holds the device error word: bits set
+// by a kernel whose bounded wait gave up, cleared when a solve starts.
+constexpr int kErrWord = 15;
 
 struct LevelInfo {
   int ny, nx, pitch, inst;
@@ -54,6 +57,7 @@ struct InstInfo {
   int ny, nx, pitch, bc;
   int level0, bottom, coarsest, nlevels;
   long long r_off, p_off, d_off, z_off, q_off;  // p is double-buffered: p_off / q_off
+  long long xs_off;  // the plan's own FP64 copy of the solution (element offset, row pitch `pitch`)
   int fine_begin, fine_end;  // tile range in the fine map
   int up0_begin, up0_end;    // tile range in the level-0 up map (empty if bottom is level 0)
   int zero_mean, pad;
@@ -68,7 +72,8 @@ struct InstInfo {
 struct InstState {
   double rz, beta, pAp, alpha, rr, rr_ref, ff, rr_true, mean, fmean, rr_prev;
   int status, iters, flags, first;
-  int pcur, pad;  // which of the two p buffers holds the current direction
+  int pcur;  // which of the two p buffers holds the current direction
+  int xcur;  // where the current solution is: 0 the caller's x, 1 the plan's copy
 };
 
 struct Tile {
@@ -83,6 +88,7 @@ struct Args {
   const InstInfo *inst;
   InstState *st;
   T *arena;
+  double *xs;  // the plan's FP64 solution copies
   const unsigned char *codes;
   const double *dense;
   double *part0;

@@ -307,41 +307,6 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
 // through FLAG_DZERO instead of being cleared here).  A thread owns one
 // column of the 64 x 128 tile, so every warp access is 32 consecutive
 // elements; the independent rows are unrolled for several loads in flight.
-template <typename T>
-__global__ void __launch_bounds__(kFThreads) k_fold(Args<T> a) {
-  const Tile tl = a.tiles[blockIdx.x];
-  // nothing to fold without a refresh, or when d restarted since the last one
-  // (a breakdown can request a refresh before any cgupdate wrote d)
-  const int flags = a.st[tl.inst].flags;
-  if (!(flags & FLAG_RU) || (flags & FLAG_DZERO)) return;
-  // descriptor fields in registers: the stores below could alias the descriptor
-  const InstInfo &Ig = a.inst[tl.inst];
-  const int ny = Ig.ny, nx = Ig.nx, pitch = Ig.pitch;
-  const long long upitch = Ig.upitch;
-  double *const X = Ig.x;
-  T *const d = a.arena + Ig.d_off;
-  const int x = tl.tx * kFTX + threadIdx.x;
-  const int y0 = tl.ty * kFTY;
-  if (x >= nx) return;
-  const int y1 = min(y0 + kFTY, ny);
-  // eight rows at a time: every load of a chunk is issued before its stores
-  for (int yb = y0; yb < y1; yb += 8) {
-    double xv[8];
-    T dv[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int y = yb + k;
-      xv[k] = y < y1 ? X[(long long)y * upitch + x] : 0.0;
-      dv[k] = y < y1 ? d[(long long)y * pitch + x] : T(0);
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int y = yb + k;
-      if (y < y1) X[(long long)y * upitch + x] = xv[k] + (double)dv[k];
-    }
-  }
-}
-
 // Sum of column x over rows y0 .. y1 - 1 of an FP64 array, eight independent
 // loads in flight per thread and a fixed summation tree.
 __device__ __forceinline__ double column_sum(const double *A, long long pitch, int y0, int y1,
@@ -365,6 +330,7 @@ __device__ __forceinline__ double column_sum(const double *A, long long pitch, i
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_fmean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.counter[kErrWord] = 0u;  // a solve starts
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
   if (I.zero_mean) {
@@ -389,8 +355,11 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
   if (I.zero_mean) {
+    const bool own = a.st[tl.inst].xcur != 0;
+    const double *X = own ? a.xs + I.xs_off : I.x;
+    const long long pitch = own ? (long long)I.pitch : I.upitch;
     const int Y0 = tl.ty * kFTY, gx = tl.tx * kFTX + threadIdx.x;
-    if (gx < I.nx) part = column_sum(I.x, I.upitch, Y0, min(Y0 + kFTY, I.ny), gx);
+    if (gx < I.nx) part = column_sum(X, pitch, Y0, min(Y0 + kFTY, I.ny), gx);
   }
   part = block_sum<kFThreads>(part);
   if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
@@ -404,22 +373,27 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   }
 }
 
+// The solution into the caller's buffer: x - mean for zero-mean instances, a
+// copy when the last refresh left the solution in the plan's own copy.
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const InstInfo &Ig = a.inst[tl.inst];
-  if (!Ig.zero_mean) return;
+  const bool own = a.st[tl.inst].xcur != 0;
+  if (!Ig.zero_mean && !own) return;
   const int ny = Ig.ny, nx = Ig.nx;
   const long long upitch = Ig.upitch;
   double *const X = Ig.x;
-  const double m = a.st[tl.inst].mean;
+  const double *const src = own ? a.xs + Ig.xs_off : X;
+  const long long spitch = own ? (long long)Ig.pitch : upitch;
+  const double m = Ig.zero_mean ? a.st[tl.inst].mean : 0.0;
   const int Y0 = tl.ty * kFTY, gx = tl.tx * kFTX + threadIdx.x;
   if (gx >= nx) return;
   const int y1 = min(Y0 + kFTY, ny);
   for (int yb = Y0; yb < y1; yb += 8) {
     double v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = yb + k < y1 ? X[(long long)(yb + k) * upitch + gx] : 0.0;
+    for (int k = 0; k < 8; ++k) v[k] = yb + k < y1 ? src[(long long)(yb + k) * spitch + gx] : 0.0;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
       if (yb + k < y1) X[(long long)(yb + k) * upitch + gx] = v[k] - m;

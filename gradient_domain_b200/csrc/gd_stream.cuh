@@ -18,6 +18,7 @@
 
 #include <cuda_pipeline.h>
 
+#include "gd_bulk.cuh"
 #include "gd_mg_kernels.cuh"
 
 namespace gd {
@@ -1010,117 +1011,385 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
   }
 }
 
-// FP64 residual r = scale (f - fmean) - A x of the refreshed (or, with INIT,
-// the initial) iterate, its norm, and the convergence decision per instance.
-// x and f are the caller's FP64 arrays (any row pitch).  A thread owns one
-// column of the 64 x 128 tile and walks its rows with x rows y - 1, y, y + 1 in
-// registers; horizontal neighbours come from shuffles, and lanes 0 and 31 take
-// the column just outside their warp.  Every warp access is 32 consecutive
-// elements.  The rows arrive through per-thread cp.async rings in shared
-// memory (x one row ahead, f, and the edge column of lanes 0 and 31),
-// kResidRing - 1 rows in flight per thread without holding registers.
-constexpr int kResidRing = 8;
+// FP64 refresh: x' = x + d (the FP32 correction folded into the FP64
+// solution), r = scale (f - fmean) - A x', the residual norm and the
+// convergence decision per instance, in one pass.  With INIT: the residual of
+// the caller's initial x, nothing to fold.
+//
+// The solution alternates between the caller's buffer and the plan's own FP64
+// copy (InstState::xcur names the current one): the pass reads the current
+// copy and d and writes x' into the other one, so the halo rows and edge
+// columns that neighbouring warps read are never rewritten while it runs.
+// When d restarted since the last refresh (FLAG_DZERO) there is nothing to
+// fold and the current copy stays where it is.
+//
+// A warp covers 128 columns (four per lane) and kKrylovRows rows of the
+// 64 x 128 fine tile, plus one halo row above and below; horizontal
+// neighbours come from shuffles and lanes 0 and 31 take the column just
+// outside the warp.  Rows arrive through a ring of kRefRing slots in shared
+// memory: slot q holds x, d and the classes of row y0 - 1 + q, and f and the
+// edge column of the row before it, the row completed at step q.  On
+// rectangle strips whose 128 columns are inside the grid and whose caller
+// rows are 16-byte aligned (almost all strips), lane 0 fills a slot with
+// three bulk copies (x, f, d row segments) completed on the slot's mbarrier;
+// elsewhere every lane copies its own four columns with cp.async, element by
+// element at the ragged right end and on unaligned caller rows.  The edge
+// columns always travel by cp.async (lanes 0 and 31).
+constexpr int kRefRing = 4;
 
 template <typename T>
-constexpr size_t resid_smem() { return (size_t)3 * kResidRing * kThreads * sizeof(double); }
+struct RefSmem {
+  // per-thread cp.async ring
+  static constexpr int DCH = (int)(4 * sizeof(T) / 16);  // 16-byte chunks of d per lane and row
+  static constexpr int CH = 4 + DCH;                       // chunks: x 0-1, f 2-3, d 4..
+  static constexpr size_t main = (size_t)kRefRing * CH * kThreads * 16;
+  static constexpr size_t edge = (size_t)kRefRing * kWarps * 2 * 16;  // x and d, per side
+  static constexpr size_t code = (size_t)kRefRing * kThreads * 4;
+  static constexpr size_t ecode = (size_t)kRefRing * kWarps * 2 * 4;
+  static constexpr size_t general = main + edge + code + ecode;
+  // bulk ring: per warp and slot the x, f and d row segments, then the
+  // barriers, then the edge ring laid out as above
+  static constexpr size_t SB = 2048 + 128 * sizeof(T);
+  static constexpr size_t rows = (size_t)kWarps * kRefRing * SB;
+  static constexpr size_t bars = (size_t)kWarps * kRefRing * 8;
+  static constexpr size_t bulk = rows + bars + edge;
+  static constexpr size_t bytes = general > bulk ? general : bulk;
+};
+
+template <typename T>
+constexpr size_t refresh_smem() { return RefSmem<T>::bytes; }
+
+static_assert(kFTX == 4 * kLanes && kFTY == kWarps * kKrylovRows,
+              "the refresh maps one warp to 128 columns and kKrylovRows rows of a fine tile");
+
+// x[x0 .. x0 + 3] of one FP64 row into two 16-byte chunks; `nv` (0..4) of the
+// four columns are inside the grid, the others are zero-filled.  `row` is any
+// valid address when nv is 0.
+__device__ __forceinline__ void copy_row4(unsigned char *c0, unsigned char *c1, const double *row,
+                                          int nv) {
+  if (nv == 4 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+    __pipeline_memcpy_async(c0, row, 16);
+    __pipeline_memcpy_async(c1, row + 2, 16);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      __pipeline_memcpy_async((j < 2 ? c0 : c1) + 8 * (j & 1), j < nv ? row + j : row, 8,
+                              j < nv ? 0 : 8);
+  }
+}
+
+__device__ __forceinline__ void read_row4(double (&v)[4], const unsigned char *c0,
+                                          const unsigned char *c1) {
+  const double2 a = *reinterpret_cast<const double2 *>(c0);
+  const double2 b = *reinterpret_cast<const double2 *>(c1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// What one warp of the refresh works on, resolved once per launch.
+template <typename T>
+struct RefWarp {
+  const double *src;  // the current solution copy
+  long long spitch;
+  double *dst;        // the other copy (written when folding)
+  long long dpitch;
+  double *X;          // the caller's buffer (INIT zeroes it where there is no unknown)
+  long long upitch;
+  const double *F;
+  const T *D;
+  T *R;
+  const unsigned char *codes;
+  int ny, nx, pitch, x0, nv, y0, y1, ecol;
+  bool masked, ecol_in;
+  double scale, fmean, omw;
+};
+
+// One warp's rows.  FAST: a rectangle strip whose 128 columns are all inside
+// the grid, on 16-byte aligned caller rows; lane 0 moves whole row segments
+// with bulk copies, rows outside the grid are not copied and read as zeros,
+// and no cell needs a class test.  Both paths do the same arithmetic in the
+// same order.
+template <typename T, bool INIT, bool FOLD, bool FAST>
+__device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char *smem,
+                                              unsigned *err, double &part, double &part_f) {
+  using SM = RefSmem<T>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool edge_lane = lane == 0 || lane == 31;
+  const int side = lane == 31;
+  const bool masked = !FAST && w.masked;
+  const int x0 = w.x0, nv = FAST ? 4 : w.nv, y0 = w.y0, y1 = w.y1, ny = w.ny;
+  const int col0 = x0 - 4 * lane;
+  double dgc[4];  // diagonal of the lane's columns away from the top and bottom rows
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    dgc[j] = 4.0 - (double)((x0 + j == 0) + (x0 + j == w.nx - 1)) * w.omw;
+  // per-thread ring (general strips)
+  auto chunk = [&](int s, int k) {
+    return smem + ((size_t)(s * SM::CH + k) * kThreads + threadIdx.x) * 16;
+  };
+  auto cslot = [&](int s) {
+    return reinterpret_cast<unsigned *>(smem + SM::main + SM::edge) + s * kThreads + threadIdx.x;
+  };
+  auto ecslot = [&](int s) {
+    return reinterpret_cast<unsigned *>(smem + SM::main + SM::edge + SM::code) +
+           (s * kWarps + warp) * 2 + side;
+  };
+  // bulk ring (FAST strips)
+  unsigned char *const brow = smem + (size_t)warp * kRefRing * SM::SB;
+  uint64_t *const bar = reinterpret_cast<uint64_t *>(smem + SM::rows) + warp * kRefRing;
+  auto eslot = [&](int s) {
+    return smem + (FAST ? SM::rows + SM::bars : SM::main) +
+           ((size_t)(s * kWarps + warp) * 2 + side) * 16;
+  };
+  if constexpr (FAST) {
+    if (lane == 0)
+      for (int s = 0; s < kRefRing; ++s) bulk::init(bar + s, 1);
+    bulk::init_fence();
+    __syncwarp();
+  }
+  // step q: x, d, classes of row y0 - 1 + q; f and the edge column of the row before
+  auto issue = [&](int q) {
+    const int s = q & (kRefRing - 1);
+    const int yy = y0 - 1 + q;
+    const bool rok = yy >= 0 && yy < ny && nv > 0;
+    const int p = yy - 1;
+    const bool pin = p >= y0 && p < y1;
+    const bool pok = pin && nv > 0;
+    if constexpr (FAST) {
+      if (lane == 0) {
+        unsigned char *slot = brow + s * SM::SB;
+        const unsigned xb = 128 * sizeof(double), db = FOLD ? 128 * sizeof(T) : 0;
+        bulk::arrive_expect(bar + s, (rok ? xb + db : 0u) + (pok ? xb : 0u));
+        if (rok) {
+          bulk::copy(slot, w.src + yy * w.spitch + col0, xb, bar + s);
+          if (FOLD) bulk::copy(slot + 2 * xb, w.D + (long long)yy * w.pitch + col0, db, bar + s);
+        }
+        if (pok) bulk::copy(slot + xb, w.F + p * w.upitch + col0, xb, bar + s);
+      }
+    } else {
+      copy_row4(chunk(s, 0), chunk(s, 1), rok ? w.src + yy * w.spitch + x0 : w.src,
+                rok ? nv : 0);
+      if constexpr (FOLD) {
+        const T *dr = rok ? w.D + (long long)yy * w.pitch + x0 : w.D;
+#pragma unroll
+        for (int k = 0; k < SM::DCH; ++k)
+          __pipeline_memcpy_async(chunk(s, 4 + k), dr + (rok ? k * (16 / sizeof(T)) : 0), 16,
+                                  rok ? 0 : 16);
+      }
+      if (masked)
+        __pipeline_memcpy_async(cslot(s), w.codes + (rok ? (long long)yy * w.pitch + x0 : 0), 4,
+                                rok ? 0 : 4);
+      copy_row4(chunk(s, 2), chunk(s, 3), pok ? w.F + p * w.upitch + x0 : w.F, pok ? nv : 0);
+    }
+    if (edge_lane) {
+      const bool eok = pin && w.ecol_in;
+      __pipeline_memcpy_async(eslot(s), eok ? w.src + p * w.spitch + w.ecol : w.src, 8,
+                              eok ? 0 : 8);
+      if constexpr (FOLD)
+        __pipeline_memcpy_async(eslot(s) + 8, eok ? w.D + (long long)p * w.pitch + w.ecol : w.D,
+                                sizeof(T), eok ? 0 : sizeof(T));
+      if (masked) {
+        // the aligned word holding the edge column: byte 3 left of lane 0, byte 0 right of lane 31
+        const int wc = lane == 0 ? x0 - 4 : x0 + 4;
+        __pipeline_memcpy_async(ecslot(s), w.codes + (eok ? (long long)p * w.pitch + wc : 0), 4,
+                                eok ? 0 : 4);
+      }
+    }
+  };
+  const int nsteps = y1 - y0 + 2;
+#pragma unroll
+  for (int q = 0; q < kRefRing - 1; ++q) {
+    if (q < nsteps) issue(q);
+    __pipeline_commit();
+  }
+  double xu[4] = {0.0, 0.0, 0.0, 0.0}, xc[4] = {0.0, 0.0, 0.0, 0.0};
+  unsigned cc = 0u;  // classes of the row in xc (masked)
+  for (int q = 0; q < nsteps; ++q) {
+    const int s = q & (kRefRing - 1);
+    const int yy = y0 - 1 + q;
+    const bool rok = yy >= 0 && yy < ny;
+    double xd[4], fv[4];
+    T dv[4] = {T(0), T(0), T(0), T(0)};
+    if constexpr (FAST) {
+      bulk::wait(bar + s, (unsigned)(q / kRefRing) & 1u, err);
+      __pipeline_wait_prior(kRefRing - 2);
+      const unsigned char *slot = brow + s * SM::SB;
+      const bool pok = yy - 1 >= y0;
+      if (rok) {
+        read_row4(xd, slot + lane * 32, slot + lane * 32 + 16);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) xd[j] = 0.0;
+      }
+      if (pok) {
+        read_row4(fv, slot + 1024 + lane * 32, slot + 1024 + lane * 32 + 16);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) fv[j] = 0.0;
+      }
+      if (FOLD && rok) {
+        const V4<T> t = ld4(reinterpret_cast<const T *>(slot + 2048) + 4 * lane);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dv[j] = t.v[j];
+      }
+    } else {
+      __pipeline_wait_prior(kRefRing - 2);
+      read_row4(xd, chunk(s, 0), chunk(s, 1));
+      read_row4(fv, chunk(s, 2), chunk(s, 3));
+      if constexpr (FOLD) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 t = *reinterpret_cast<const float4 *>(chunk(s, 4));
+          dv[0] = t.x; dv[1] = t.y; dv[2] = t.z; dv[3] = t.w;
+        } else {
+          const double2 t0 = *reinterpret_cast<const double2 *>(chunk(s, 4));
+          const double2 t1 = *reinterpret_cast<const double2 *>(chunk(s, 5));
+          dv[0] = t0.x; dv[1] = t0.y; dv[2] = t1.x; dv[3] = t1.y;
+        }
+      }
+    }
+    const unsigned cw = masked ? *cslot(s) : 0u;
+    double ex = 0.0, ed = 0.0;
+    unsigned ecw = 0u;
+    if (edge_lane) {
+      ex = *reinterpret_cast<const double *>(eslot(s));
+      if constexpr (FOLD) ed = (double)*reinterpret_cast<const T *>(eslot(s) + 8);
+      if (masked) ecw = *ecslot(s);
+    }
+    if (q + kRefRing - 1 < nsteps) {
+      if constexpr (FAST) {
+        __syncwarp();  // every lane has read the slot refilled now (step q - 1's)
+        if (lane == 0) bulk::proxy_fence();
+      }
+      issue(q + kRefRing - 1);
+    }
+    __pipeline_commit();
+    // x' of row yy, zero where there is no unknown
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool on = FAST || (rok && j < nv && (!masked || ((cw >> (8 * j)) & 0xffu) != 0u));
+      xd[j] = on ? xd[j] + (double)dv[j] : 0.0;
+    }
+    if (q >= 2) {  // row p = yy - 1 has x' above, at and below it
+      const int p = yy - 1;
+      bool eon = true;
+      if (!FAST && edge_lane) {
+        eon = w.ecol_in;
+        if (masked) eon = eon && ((lane == 0 ? (ecw >> 24) : ecw) & 0xffu) != 0u;
+      }
+      const double ev = eon ? ex + ed : 0.0;
+      double left = shfl_up1(xc[3]), right = shfl_dn1(xc[0]);
+      if (lane == 0) left = ev;
+      if (lane == 31) right = ev;
+      const double rowd = (double)((p == 0) + (p == ny - 1)) * w.omw;
+      double res[4], fq[4];
+      bool on[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        double dg = dgc[j] - rowd;
+        on[j] = FAST || j < nv;
+        if (masked) {
+          const int c = (int)((cc >> (8 * j)) & 0xffu);
+          on[j] = on[j] && c != 0;
+          dg = 4.0 - (double)(c - 1) * w.omw;
+        }
+        const double lf = j == 0 ? left : xc[j - 1];
+        const double rt = j == 3 ? right : xc[j + 1];
+        fq[j] = on[j] ? w.scale * (fv[j] - w.fmean) : 0.0;
+        res[j] = on[j] ? fq[j] - (dg * xc[j] - ((xu[j] + xd[j]) + (lf + rt))) : 0.0;
+      }
+      part += (res[0] * res[0] + res[1] * res[1]) + (res[2] * res[2] + res[3] * res[3]);
+      if (INIT) part_f += (fq[0] * fq[0] + fq[1] * fq[1]) + (fq[2] * fq[2] + fq[3] * fq[3]);
+      V4<T> rv;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rv.v[j] = (T)res[j];
+      if (FAST || nv > 0) st4(w.R + (long long)p * w.pitch + x0, rv);
+      if constexpr (FOLD) {
+        double *drow = w.dst + p * w.dpitch + x0;
+        if (FAST || (nv == 4 && (reinterpret_cast<uintptr_t>(drow) & 15) == 0)) {
+          *reinterpret_cast<double2 *>(drow) = make_double2(xc[0], xc[1]);
+          *reinterpret_cast<double2 *>(drow + 2) = make_double2(xc[2], xc[3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (j < nv) drow[j] = xc[j];
+        }
+      }
+      if (INIT && masked) {  // the caller's x is zero where there is no unknown
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nv && !on[j]) w.X[p * w.upitch + x0 + j] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      xu[j] = xc[j];
+      xc[j] = xd[j];
+    }
+    cc = cw;
+  }
+  __pipeline_wait_prior(0);  // no copy may land after the shared memory is released
+}
 
 template <typename T, bool INIT>
-__global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
-  const bool work = INIT || (a.st[tl.inst].flags & FLAG_RU);
+  const int flags = a.st[tl.inst].flags;
+  const bool work = INIT || (flags & FLAG_RU);
   double part = 0.0, part_f = 0.0;
   extern __shared__ __align__(16) unsigned char smem[];
   if (work) {
     // descriptor fields in registers: the stores below could alias the descriptor
     const InstInfo &Ig = a.inst[tl.inst];
-    double *const X = Ig.x;
-    const double *const Fu = Ig.f;
-    const long long upitch = Ig.upitch;
-    const double scale = Ig.scale;
-    T *const r = a.arena + Ig.r_off;
     const LevelInfo L = a.lv[Ig.level0];
-    const int lane = threadIdx.x & 31;
-    const int col = tl.tx * kFTX + threadIdx.x;
-    const int y0 = tl.ty * kFTY;
-    const int y1 = min(y0 + kFTY, L.ny);
-    const bool masked = L.code_off >= 0;
-    const bool in_col = col < L.nx;
-    const double fmean = a.st[tl.inst].fmean;
-    const double omw = 1.0 - (double)L.wall;
-    auto klass = [&](int y, int x) -> int {
-      if (y < 0 || y >= L.ny || x < 0 || x >= L.nx) return 0;
-      if (masked) return a.codes[L.code_off + (long long)y * L.pitch + x];
-      return rect_class(y, x, L.ny, L.nx);
-    };
-    // x at (y, x) where the cell has an unknown, else zero
-    auto xv = [&](int y, int x) -> double {
-      return klass(y, x) ? X[(long long)y * upitch + x] : 0.0;
-    };
-    // rings: slot q holds x of row y0 + 1 + q, f of row y0 + q and the edge
-    // column of row y0 + q (lane 0: col - 1, lane 31: col + 1)
-    double *const rx = reinterpret_cast<double *>(smem) + threadIdx.x;
-    double *const rf = rx + kResidRing * kThreads;
-    double *const re = rf + kResidRing * kThreads;
-    const int ecol = lane == 0 ? col - 1 : col + 1;
-    const bool edge_lane = lane == 0 || lane == 31;
-    auto issue = [&](int q) {
-      const int sl = (q & (kResidRing - 1)) * kThreads;
-      const int yx = y0 + 1 + q, yf = y0 + q;
-      const bool okx = in_col && yx < L.ny;
-      const bool okf = in_col && yf < y1;
-      __pipeline_memcpy_async(rx + sl, okx ? X + (long long)yx * upitch + col : X, 8,
-                              okx ? 0 : 8);
-      __pipeline_memcpy_async(rf + sl, okf ? Fu + (long long)yf * upitch + col : Fu, 8,
-                              okf ? 0 : 8);
-      if (edge_lane) {
-        const bool oke = yf < y1 && ecol >= 0 && ecol < L.nx;
-        __pipeline_memcpy_async(re + sl, oke ? X + (long long)yf * upitch + ecol : X, 8,
-                                oke ? 0 : 8);
+    const bool own = !INIT && a.st[tl.inst].xcur != 0;
+    double *const XS = a.xs + Ig.xs_off;
+    RefWarp<T> w;
+    w.X = Ig.x;
+    w.upitch = Ig.upitch;
+    w.src = own ? XS : w.X;
+    w.spitch = own ? (long long)L.pitch : w.upitch;
+    w.dst = own ? w.X : XS;
+    w.dpitch = own ? w.upitch : (long long)L.pitch;
+    w.F = Ig.f;
+    w.D = a.arena + Ig.d_off;
+    w.R = a.arena + Ig.r_off;
+    w.masked = L.code_off >= 0;
+    w.codes = a.codes + (w.masked ? L.code_off : 0);
+    w.ny = L.ny;
+    w.nx = L.nx;
+    w.pitch = L.pitch;
+    w.scale = Ig.scale;
+    w.fmean = a.st[tl.inst].fmean;
+    w.omw = 1.0 - (double)L.wall;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col0 = tl.tx * kFTX;
+    w.x0 = col0 + 4 * lane;
+    w.nv = max(0, min(4, w.nx - w.x0));
+    w.y0 = tl.ty * kFTY + warp * kKrylovRows;
+    w.y1 = min(w.y0 + kKrylovRows, w.ny);
+    w.ecol = lane == 0 ? w.x0 - 1 : w.x0 + 4;
+    w.ecol_in = w.ecol >= 0 && w.ecol < w.nx;
+    unsigned *const err = a.counter + kErrWord;
+    if (w.y0 < w.ny) {
+      const bool fast = !w.masked && col0 + kFTX <= w.nx &&
+                        ((reinterpret_cast<uintptr_t>(w.X) | reinterpret_cast<uintptr_t>(w.F)) &
+                         15) == 0 &&
+                        (w.upitch & 1) == 0;
+      if constexpr (INIT) {
+        if (fast) refresh_strip<T, true, false, true>(w, smem, err, part, part_f);
+        else refresh_strip<T, true, false, false>(w, smem, err, part, part_f);
+      } else if (!(flags & FLAG_DZERO)) {
+        if (fast) refresh_strip<T, false, true, true>(w, smem, err, part, part_f);
+        else refresh_strip<T, false, true, false>(w, smem, err, part, part_f);
+      } else {
+        if (fast) refresh_strip<T, false, false, true>(w, smem, err, part, part_f);
+        else refresh_strip<T, false, false, false>(w, smem, err, part, part_f);
       }
-    };
-    double xu = xv(y0 - 1, col), xc = xv(y0, col);
-    for (int q = 0; q < kResidRing - 1; ++q) {
-      issue(q);
-      __pipeline_commit();
     }
-    for (int y = y0; y < y1; ++y) {
-      const int q = y - y0;
-      __pipeline_wait_prior(kResidRing - 2);
-      const int sl = (q & (kResidRing - 1)) * kThreads;
-      double xd = rx[sl];
-      const double fraw = rf[sl];
-      const double eraw = edge_lane ? re[sl] : 0.0;
-      issue(q + kResidRing - 1);
-      __pipeline_commit();
-      double ev = eraw;
-      if (masked) {  // values of cells without an unknown read as zero
-        if (!klass(y + 1, col)) xd = 0.0;
-        if (edge_lane && !klass(y, ecol)) ev = 0.0;
-      }
-      double left = shfl_up1(xc), right = shfl_dn1(xc);
-      if (lane == 0) left = ev;
-      if (lane == 31) right = ev;
-      const int c = in_col ? klass(y, col) : 0;
-      if (c) {
-        const double dg = 4.0 - (double)(c - 1) * omw;
-        const double f = scale * (fraw - fmean);
-        const double r64 = f - (dg * xc - (xu + xd + left + right));
-        r[(long long)y * L.pitch + col] = (T)r64;
-        part += r64 * r64;
-        if (INIT) part_f += f * f;
-      } else if (in_col) {
-        r[(long long)y * L.pitch + col] = T(0);
-        if (INIT && masked) X[(long long)y * upitch + col] = 0.0;
-      }
-      xu = xc;
-      xc = xd;
+    part = block_sum<kThreads>(part);
+    if (INIT) {
+      __syncthreads();
+      part_f = block_sum<kThreads>(part_f);
     }
-    __pipeline_wait_prior(0);  // no copy may land after the shared memory is released
-  }
-  part = block_sum<kThreads>(part);
-  if (INIT) {
-    __syncthreads();
-    part_f = block_sum<kThreads>(part_f);
   }
   if (threadIdx.x == 0) {
     a.part0[blockIdx.x] = part;
@@ -1145,7 +1414,10 @@ __global__ void __launch_bounds__(kThreads) k_resid_s(Args<T> a) {
           S.rz = 0.0;
           S.beta = 0.0;
           S.pcur = 0;
+          S.xcur = 0;
           S.status = GD_ACTIVE;
+        } else if (!(S.flags & FLAG_DZERO)) {
+          S.xcur ^= 1;  // x + d went to the other copy
         }
         // A refresh that barely lowers the true residual (less than 3x), once
         // it is already below 1e-6 of ||f||, means the FP64 rounding floor is

@@ -240,6 +240,52 @@ def test_batch_equals_alone():
         assert torch.equal(xa, xb[k])
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_caller_buffers_of_any_alignment_and_pitch(precision):
+    """Right-hand sides and solutions may be views with an odd row pitch that
+    start off a 16-byte boundary (the refresh then copies element by element):
+    the same bits as contiguous buffers, over repeated solves of one plan (the
+    solution alternates between the caller's buffer and the plan's copy), and
+    zeros where a masked instance has no unknown even from a non-zero start."""
+    rng = np.random.default_rng(31)
+    active = np.zeros((61, 203), bool)
+    active[5:50, 7:190] = True
+    active[20:30, 60:90] = False
+    shapes = [(61, 203, "neumann"), (90, 131, "dirichlet"), (61, 203, "masked")]
+    rhs = [rng.standard_normal(s[:2]) for s in shapes]
+    start = [np.zeros(s[:2]) for s in shapes]
+    start[2] = np.where(active, 0.0, 7.0)  # garbage outside the mask
+
+    def run(offset, extra):
+        plan = PoissonPlan([Instance(h, w, b, b == "neumann") for h, w, b in shapes],
+                           SolveParams(precision=precision, tolerance=1e-10))
+        plan.set_mask(2, torch.as_tensor(active.astype(np.uint8)).cuda())
+        out = []
+        for _ in range(3):
+            fv, xv = [], []
+            for k, (h, w, _) in enumerate(shapes):
+                fb = torch.zeros((h, w + extra), dtype=torch.float64, device="cuda")
+                xb = torch.zeros_like(fb)
+                fb[:, offset:offset + w] = torch.as_tensor(rhs[k])
+                xb[:, offset:offset + w] = torch.as_tensor(start[k])
+                fv.append(fb[:, offset:offset + w])
+                xv.append(xb[:, offset:offset + w])
+            res = plan.solve(fv, xv, scale=-1.0)
+            out.append(([t.clone() for t in xv], [(r.iterations, r.status) for r in res]))
+        return out
+
+    dense = run(0, 0)
+    for offset, extra in ((1, 3), (3, 4)):
+        for (xa, sa), (xb, sb) in zip(run(offset, extra), dense):
+            assert sa == sb and all(s == _lib.GD_CONVERGED for _, s in sa)
+            for a, b in zip(xa, xb):
+                assert torch.equal(a, b)
+    for xs, _ in dense:
+        assert torch.all(xs[2][torch.as_tensor(~active).cuda()] == 0)
+        ref = osolvers.solve_neumann(rhs[0])
+        assert _rel(xs[0].cpu().numpy(), ref) < 1e-6
+
+
 def test_zero_and_nonfinite_rhs_are_reported_not_raised():
     plan = PoissonPlan([Instance(40, 40, "dirichlet"), Instance(40, 40, "dirichlet")],
                        SolveParams())
