@@ -50,7 +50,8 @@ class Params(C.Structure):
 
 class Report(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("status", C.c_int32),
-                ("relative_residual", C.c_double), ("initial_norm", C.c_double)]
+                ("relative_residual", C.c_double), ("initial_norm", C.c_double),
+                ("refreshes", C.c_int32), ("reserved", C.c_int32)]
 
 
 class FieldDesc(C.Structure):

@@ -271,8 +271,10 @@ struct Runner {
     }
   }
 
+  // One Krylov iteration; `refresh` false leaves out the FP64 refresh, which
+  // the solve graph launches behind a conditional node instead.
   template <int S>
-  static void iteration(gd_plan p, const Args<T> &a, cudaStream_t st) {
+  static void iteration(gd_plan p, const Args<T> &a, cudaStream_t st, bool refresh) {
     vcycle<S>(p, a, st);
     const Args<T> f = at_tiles(a, p->fine_base);
     const double c = p->fine_cells;
@@ -282,8 +284,13 @@ struct Runner {
     prof_begin(p, GD_K_CGUPDATE, c, st);
     st::k_cgupdate_s<T><<<p->fine_count, st::kThreads, st::cgupdate_smem<T>(), st>>>(f);
     prof_end(p, st);
-    prof_begin(p, GD_K_RESID, c, st);
-    st::k_refresh_s<T, false><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(f);
+    if (refresh) launch_refresh(p, a, st);
+  }
+
+  static void launch_refresh(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    prof_begin(p, GD_K_RESID, p->fine_cells, st);
+    st::k_refresh_s<T, false><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(
+        at_tiles(a, p->fine_base));
     prof_end(p, st);
   }
 
@@ -292,11 +299,12 @@ struct Runner {
     else if (s == 2) set_attrs<2>();
     else set_attrs<3>();
   }
-  static void dispatch_iteration(gd_plan p, const Args<T> &a, cudaStream_t st) {
+  static void dispatch_iteration(gd_plan p, const Args<T> &a, cudaStream_t st,
+                                 bool refresh = true) {
     const int s = p->prm.pre_sweeps;
-    if (s == 1) iteration<1>(p, a, st);
-    else if (s == 2) iteration<2>(p, a, st);
-    else iteration<3>(p, a, st);
+    if (s == 1) iteration<1>(p, a, st, refresh);
+    else if (s == 2) iteration<2>(p, a, st, refresh);
+    else iteration<3>(p, a, st, refresh);
   }
   static void dispatch_vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
     const int s = p->prm.pre_sweeps;
@@ -740,6 +748,16 @@ __global__ void k_loop_gate(cudaGraphConditionalHandle h, const int *n_active, i
   cudaGraphSetConditional(h, (*n_active > 0 && t < cap) ? 1u : 0u);
 }
 
+// Condition of the refresh node in the loop body: some instance asked for an
+// FP64 refresh (FLAG_RU).  Iterations without one launch no refresh kernel.
+__global__ void k_refresh_gate(cudaGraphConditionalHandle h, const InstState *st, int n) {
+  if (blockIdx.x != 0) return;
+  bool any = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) any = any || (st[i].flags & FLAG_RU);
+  any = __any_sync(0xffffffffu, any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
 template <typename T>
 void launch_init(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
@@ -770,10 +788,12 @@ int loop_cap(gd_plan p) {
 }
 
 // One graph per plan for a whole solve: the initial residual, a conditional
-// while node whose body is one Krylov iteration followed by k_loop_gate, and
-// the zero-mean projection.  The device decides when to stop, so a solve is a
-// single graph launch with no host round trip and no iteration past the last
-// active instance.
+// while node whose body is one Krylov iteration (V-cycle, p update, d / r
+// update, then the FP64 refresh behind an if node, launched only when some
+// instance asked for one) followed by k_loop_gate, and the zero-mean
+// projection.  The device decides when to stop, so a solve is a single graph
+// launch with no host round trip and no iteration past the last active
+// instance.
 template <typename T>
 int build_solve_graph(gd_plan p, const Args<T> &a, const Args<T> &fine) {
   if (!p->cap) {
@@ -817,16 +837,58 @@ int build_solve_graph(gd_plan p, const Args<T> &a, const Args<T> &fine) {
   cudaGraph_t g = nullptr;
   const cudaError_t ee = cudaStreamEndCapture(cs, &g);
   if (e == cudaSuccess) e = ee;
+  // loop body: an iteration without the refresh, the refresh behind an if
+  // node that k_refresh_gate sets, then the loop gate
+  cudaGraph_t refresh_body = nullptr;
   if (e == cudaSuccess) {
     e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      Runner<T>::dispatch_iteration(p, a, cs);
-      k_loop_gate<<<1, 32, 0, cs>>>(h, a.n_active, trips, 0, cap);
-      e = cudaGetLastError();
+      do {
+        Runner<T>::dispatch_iteration(p, a, cs, false);
+        cudaStreamCaptureStatus status;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        cudaGraphConditionalHandle hr{};
+        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &nd)) != cudaSuccess)
+          break;
+        if ((e = cudaGraphConditionalHandleCreate(&hr, cg, 0, cudaGraphCondAssignDefault)) !=
+            cudaSuccess)
+          break;
+        k_refresh_gate<<<1, 32, 0, cs>>>(hr, a.st, p->n);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &nd)) != cudaSuccess)
+          break;
+        cudaGraphNodeParams ip = {};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = hr;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        cudaGraphNode_t in;
+        if ((e = cudaGraphAddNode(&in, cg, deps, nd, &ip)) != cudaSuccess) break;
+        refresh_body = ip.conditional.phGraph_out[0];
+        if ((e = cudaStreamUpdateCaptureDependencies(cs, &in, 1,
+                                                     cudaStreamSetCaptureDependencies)) !=
+            cudaSuccess)
+          break;
+        k_loop_gate<<<1, 32, 0, cs>>>(h, a.n_active, trips, 0, cap);
+        e = cudaGetLastError();
+      } while (0);
       cudaGraph_t bg = nullptr;
       const cudaError_t eb = cudaStreamEndCapture(cs, &bg);
       if (e == cudaSuccess) e = eb;
+    }
+  }
+  if (e == cudaSuccess) {
+    e = cudaStreamBeginCaptureToGraph(cs, refresh_body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      Runner<T>::launch_refresh(p, a, cs);
+      e = cudaGetLastError();
+      cudaGraph_t rg = nullptr;
+      const cudaError_t er = cudaStreamEndCapture(cs, &rg);
+      if (e == cudaSuccess) e = er;
     }
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&p->gexec, g, 0);
@@ -908,6 +970,8 @@ int collect_reports(gd_plan p, gd_report *reports) {
     R.status = S.status == GD_ACTIVE ? GD_MAX_ITERATIONS : S.status;
     R.initial_norm = std::sqrt(S.ff);
     R.relative_residual = S.ff > 0.0 ? std::sqrt(S.rr_true / S.ff) : 0.0;
+    R.refreshes = S.refreshes;
+    R.reserved = 0;
   }
   return GD_OK;
 }

@@ -74,6 +74,8 @@ struct InstState {
   int status, iters, flags, first;
   int pcur;  // which of the two p buffers holds the current direction
   int xcur;  // where the current solution is: 0 the caller's x, 1 the plan's copy
+  int refreshes;  // FP64 refreshes after the initial residual
+  int pad;
 };
 
 struct Tile {

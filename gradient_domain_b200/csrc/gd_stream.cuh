@@ -1490,9 +1490,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
           S.beta = 0.0;
           S.pcur = 0;
           S.xcur = 0;
+          S.refreshes = 0;
           S.status = GD_ACTIVE;
-        } else if (!(S.flags & FLAG_DZERO)) {
-          S.xcur ^= 1;  // x + d went to the other copy
+        } else {
+          S.refreshes += 1;
+          if (!(S.flags & FLAG_DZERO)) S.xcur ^= 1;  // x + d went to the other copy
         }
         // A refresh that barely lowers the true residual (less than 3x), once
         // it is already below 1e-6 of ||f||, means the FP64 rounding floor is

@@ -64,6 +64,7 @@ class InstanceResult:
     status: int
     relative_residual: float
     initial_norm: float
+    refreshes: int = 0  # FP64 residual refreshes after the initial residual
 
     @property
     def converged(self) -> bool:
@@ -151,7 +152,7 @@ class PoissonPlan:
 
     def _results(self) -> list[InstanceResult]:
         return [InstanceResult(int(r.iterations), int(r.status), float(r.relative_residual),
-                               float(r.initial_norm)) for r in self._reports]
+                               float(r.initial_norm), int(r.refreshes)) for r in self._reports]
 
     def solve(self, rhs: list[torch.Tensor], x: list[torch.Tensor],
               scale: list[float] | float = 1.0) -> list[InstanceResult]:

@@ -84,6 +84,8 @@ typedef struct gd_report {
   int32_t status;            /* enum gd_status                            */
   double relative_residual;  /* true FP64 ||f - A x|| / ||f|| at exit      */
   double initial_norm;       /* ||f||                                      */
+  int32_t refreshes;         /* FP64 residual refreshes after the first    */
+  int32_t reserved;
 } gd_report;
 
 typedef struct gd_plan_s *gd_plan;

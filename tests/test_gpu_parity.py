@@ -313,12 +313,13 @@ def test_graph_solves_equal_direct_solves(precision):
     for _ in range(3):
         xs = [torch.zeros_like(r) for r in rhs]
         res = plan.solve(rhs, xs, scale=-1.0)
-        runs.append(([t.clone() for t in xs], [(r.iterations, r.status) for r in res]))
+        runs.append(([t.clone() for t in xs], [(r.iterations, r.status, r.refreshes) for r in res]))
     for xs, st in runs[1:]:
         assert st == runs[0][1]
         for a, b in zip(xs, runs[0][0]):
             assert torch.equal(a, b)
     assert all(r[1] == _lib.GD_CONVERGED for r in runs[0][1])
+    assert all(r[2] >= 1 for r in runs[0][1][:3])  # converged through an FP64 refresh
     assert runs[0][1][3][0] == 0
     capped = PoissonPlan([Instance(96, 80, "neumann", True), Instance(40, 40, "dirichlet")],
                          SolveParams(precision=precision, tolerance=1e-14, max_iterations=2))
