@@ -372,12 +372,21 @@ int choose_bottom(gd_plan p, int level0, int last, size_t es) {
   return last;
 }
 
-// Strip height for one level: the tallest of 64, 32, 16, 8 rows that still
-// gives `target` warps for this level, else 8 (taller strips amortise the
-// warm-up rows, shorter ones give small levels enough parallelism).
-int strip_rows(int ny, int nx, int ow, int target) {
+// Strip height of level l: the tallest of 64, 32, 16, 8 rows that still gives
+// `target` warps over the level-l strips of all instances (one launch), else 8.
+// Taller strips amortise the warm-up rows; shorter ones keep enough warps in
+// flight on small levels and in plans with few instances, where the strips'
+// per-warp row chain would otherwise set the launch time.
+int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int ow, int target) {
+  const long long tile_max = p->prm.tile_cells > 0 ? p->prm.tile_cells : kTileCells;
   for (int rb = 64; rb >= 8; rb >>= 1) {
-    const long long warps = (long long)ceil_div(nx, ow) * ceil_div(ny, rb);
+    long long warps = 0;
+    for (int i = 0; i < p->n; ++i) {
+      if (l >= bottoms[i]) continue;
+      const LevelInfo &L = p->lv[p->inst[i].level0 + l];
+      if (l >= 1 && (long long)L.ny * L.nx <= tile_max) continue;  // on the tile kernels
+      warps += (long long)ceil_div(L.nx, ow) * ceil_div(L.ny, rb);
+    }
     if (warps >= target) return rb;
   }
   return 8;
@@ -487,13 +496,11 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   }
   int down_ow = 0, up_ow = 0;
   strip_widths(p, &down_ow, &up_ow);
-  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 600;
-  for (int i = 0; i < p->n; ++i) {
-    const InstInfo &I = p->inst[i];
-    for (int l = 0; l < bottoms[i]; ++l) {
-      LevelInfo &L = p->lv[I.level0 + l];
-      L.rows_per_warp = strip_rows(L.ny, L.nx, std::min(down_ow, up_ow), target_warps);
-    }
+  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 1800;
+  for (int l = 0; l < p->depth; ++l) {
+    const int rb = strip_rows(p, bottoms, l, std::min(down_ow, up_ow), target_warps);
+    for (int i = 0; i < p->n; ++i)
+      if (l < bottoms[i]) p->lv[p->inst[i].level0 + l].rows_per_warp = rb;
   }
   p->fine_base = (int)p->tiles.size();
   for (int i = 0; i < p->n; ++i) {

@@ -36,7 +36,7 @@ class SolveParams:
     reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
     check_every: int = 4          # host poll interval of solves on direct launches
     use_graph: bool = True        # from a plan's second solve on: one graph, device-side loop
-    strip_target_warps: int = 600   # smoother strip height: warps wanted per level
+    strip_target_warps: int = 1800  # smoother strip height: warps per level launch (all instances)
     bottom_cells: int = 0         # largest level solved inside the one-CTA bottom (0 = 4096)
     tile_cells: int = 0           # largest coarse level on shared-memory tiles (0 = 262144)
 
