@@ -253,7 +253,13 @@ template <typename T>
 constexpr size_t ring_bytes() { return (size_t)kRing * kThreads * 4 * sizeof(T); }
 template <typename T>
 constexpr size_t level_smem() { return 2 * ring_bytes<T>() + (size_t)kRing * kThreads * 4; }
+template <typename T>
+constexpr size_t edge_bytes() { return (size_t)kRing * kThreads * sizeof(T); }
 
+template <typename T>
+constexpr size_t pupdate_smem() { return 2 * ring_bytes<T>() + 2 * edge_bytes<T>(); }
+template <typename T>
+constexpr size_t cgupdate_smem() { return 3 * ring_bytes<T>() + edge_bytes<T>(); }
 
 // Lanes whose output is exact for a dependency radius of R columns.
 template <int R>
@@ -743,127 +749,59 @@ __global__ void __launch_bounds__(kThreads) k_up_s(Args<T> a) {
 
 // ---------------------------------------------------------------------------
 // Krylov kernels on level 0: a warp covers 128 columns x kKrylovRows rows and
-// the CTA four such row bands.  Row segments arrive by bulk copies: lane 0 of
-// each warp fills a ring of kKrylovRing slots (one segment per streamed array
-// and row, completed on the slot's mbarrier); arena rows are 16-byte aligned
-// and padded to a multiple of four elements, so the segment at the right end
-// of a row copies up to the padding, which holds zeros.  The one column
-// outside the warp on each side travels by cp.async (lanes 0 and 31).
-constexpr int kKrylovRing = 4;
-
-template <typename T, int NA>
-struct KrylovSmem {
-  static constexpr size_t SEG = 128 * sizeof(T);  // one warp's row segment of one array
-  static constexpr size_t rows = (size_t)kWarps * kKrylovRing * NA * SEG;
-  static constexpr size_t bars = (size_t)kWarps * kKrylovRing * 8;
-  static constexpr size_t edges = (size_t)kRing * kThreads * sizeof(T);  // one EdgeRing
-};
+// the CTA four such row bands.  The one column outside the warp on each side
+// comes from a scalar load by lanes 0 and 31.
 
 template <typename T>
-constexpr size_t pupdate_smem() {
-  using K = KrylovSmem<T, 2>;
-  return K::rows + K::bars + 2 * K::edges;
+__device__ __forceinline__ T edge_value(const T *A, const LevelInfo &L, int y, int x) {
+  return (y >= 0 && y < L.ny && x >= 0 && x < L.nx) ? A[(long long)y * L.pitch + x] : T(0);
 }
-template <typename T>
-constexpr size_t cgupdate_smem() {
-  using K = KrylovSmem<T, 3>;
-  return K::rows + K::bars + K::edges;
-}
-
-// One warp's bulk ring over NA arrays of a level-0 instance.
-template <typename T, int NA>
-struct WarpRows {
-  using K = KrylovSmem<T, NA>;
-  unsigned char *rows;
-  uint64_t *bar;
-  unsigned seg;  // bytes per copied segment
-  int xl;        // first column of the warp
-  int pitch;
-  __device__ __forceinline__ WarpRows(unsigned char *smem, int warp, int xl_, int pitch_)
-      : rows(smem + (size_t)warp * kKrylovRing * NA * K::SEG),
-        bar(reinterpret_cast<uint64_t *>(smem + K::rows) + warp * kKrylovRing),
-        seg((unsigned)(min(128, pitch_ - xl_) * (int)sizeof(T))), xl(xl_), pitch(pitch_) {
-    if ((threadIdx.x & 31) == 0)
-      for (int s = 0; s < kKrylovRing; ++s) bulk::init(bar + s, 1);
-    bulk::init_fence();
-    __syncwarp();
-  }
-  __device__ __forceinline__ unsigned char *slot(int step, int k) const {
-    return rows + ((size_t)((step & (kKrylovRing - 1)) * NA + k)) * K::SEG;
-  }
-  // lane 0: copy row y of the arrays selected by `mask` into the slot of `step`
-  __device__ __forceinline__ void issue(int step, const T *const (&src)[NA], unsigned mask,
-                                        int y) const {
-    uint64_t *b = bar + (step & (kKrylovRing - 1));
-    bulk::arrive_expect(b, (unsigned)__popc(mask) * seg);
-#pragma unroll
-    for (int k = 0; k < NA; ++k)
-      if (mask & (1u << k)) bulk::copy(slot(step, k), src[k] + (long long)y * pitch + xl, seg, b);
-  }
-  __device__ __forceinline__ void wait(int step, unsigned *err) const {
-    bulk::wait(bar + (step & (kKrylovRing - 1)), (unsigned)(step / kKrylovRing) & 1u, err);
-  }
-  __device__ __forceinline__ V4<T> read(int step, int k, int lane) const {
-    return ld4(reinterpret_cast<const T *>(slot(step, k)) + 4 * lane);
-  }
-  // before lane 0 refills a slot: every lane has read it
-  __device__ __forceinline__ void release() const {
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) bulk::proxy_fence();
-  }
-};
 
 template <typename T, bool INT>
-__device__ __forceinline__ double pupdate_rows(const Args<T> &a, const LevelInfo &L,
-                                               const ClassTable<T> &tab, int lane, int xl,
-                                               int y0, int y1, T beta, const T *z, const T *p,
-                                               T *pn, unsigned char *smem) {
-  using K = KrylovSmem<T, 2>;
+__device__ __forceinline__ double pupdate_rows(const Args<T> &a, const InstInfo &I,
+                                               const LevelInfo &L, const ClassTable<T> &tab,
+                                               int lane, int x0, int y0, int y1, T beta,
+                                               const T *z, const T *p, T *pn,
+                                               unsigned char *smem) {
   const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
-  const int x0 = xl + 4 * lane;
-  const WarpRows<T, 2> wr(smem, threadIdx.x >> 5, xl, L.pitch);
-  const EdgeRing<T> ez(reinterpret_cast<T *>(smem + K::rows + K::bars));
-  const EdgeRing<T> ep(reinterpret_cast<T *>(smem + K::rows + K::bars + K::edges));
-  unsigned *const err = a.counter + kErrWord;
+  const Ring<T> rz(reinterpret_cast<T *>(smem));
+  const Ring<T> rp(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
+  const EdgeRing<T> ez(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4);
+  const EdgeRing<T> ep(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4 + kRing * kThreads);
   const int xe = lane == 0 ? x0 - 1 : x0 + 4;  // edge column of lanes 0 and 31
   const bool edge_lane = lane == 0 || lane == 31;
-  const bool lane_in = x0 < L.pitch;  // the lane's columns are in the copied segment
-  // The first direction is p = z: with beta == 0 the old buffer is not read
-  // (it need not be initialised).
-  const bool use_p = beta != T(0);
-  const T *const src[2] = {z, p};
-  const int nsteps = y1 - y0 + 2;  // rows y0 - 1 .. y1
+  const bool read_p = beta != T(0);
+  const int nsteps = y1 - y0 + 2;  // rows y0 - 1 .. y1; nothing past them is copied
   auto issue = [&](int q) {
     if (q < nsteps) {
       const int y = y0 - 1 + q;
-      const bool rok = y >= 0 && y < L.ny;
-      if (lane == 0) wr.issue(q, src, rok ? (use_p ? 3u : 1u) : 0u, y);
+      rz.issue(q, z, L, y, x0);
+      if (read_p) rp.issue(q, p, L, y, x0);
       if (edge_lane) {
         ez.issue(q, z, L, y, xe);
-        if (use_p) ep.issue(q, p, L, y, xe);
+        if (read_p) ep.issue(q, p, L, y, xe);
       }
     }
     __pipeline_commit();
   };
-  for (int q = 0; q < kKrylovRing - 1; ++q) issue(q);
+  for (int q = 0; q < kRing - 1; ++q) issue(q);
   int step = 0;
   T edge_next = T(0);
+  // The first direction is p = z: with beta == 0 the old buffer is not read
+  // (it need not be initialised), so the rings for p are left idle.
+  const bool use_p = beta != T(0);
   auto newp = [&]() {
-    wr.wait(step, err);
-    __pipeline_wait_prior(kKrylovRing - 2);
-    const int y = y0 - 1 + step;
-    const bool ok = y >= 0 && y < L.ny && lane_in;
-    V4<T> zz = ok ? wr.read(step, 0, lane) : zero4<T>();
+    __pipeline_wait_prior(kRing - 2);
+    V4<T> zz = rz.read(step);
     T e = edge_lane ? ez.read(step) : T(0);
     if (use_p) {
-      const V4<T> pp = ok ? wr.read(step, 1, lane) : zero4<T>();
+      const V4<T> pp = rp.read(step);
       if (edge_lane) e += beta * ep.read(step);
 #pragma unroll
       for (int j = 0; j < 4; ++j) zz.v[j] += beta * pp.v[j];
     }
     edge_next = e;
-    wr.release();
-    issue(step + kKrylovRing - 1);
+    issue(step + kRing - 1);
     ++step;
     return zz;
   };
@@ -910,6 +848,7 @@ __global__ void __launch_bounds__(kThreads) k_pupdate_s(Args<T> a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
     const int xl = tl.tx * kKrylovCols;
+    const int x0 = xl + 4 * lane;
     if (y0 < L.ny) {
       const int y1 = min(y0 + kKrylovRows, L.ny);
       const T beta = (T)a.st[tl.inst].beta;
@@ -919,9 +858,9 @@ __global__ void __launch_bounds__(kThreads) k_pupdate_s(Args<T> a) {
       T *pn = a.arena + p_offset(I, cur ^ 1);
       extern __shared__ __align__(16) unsigned char smem[];
       if (strip_interior(L, y0, y1 - 1, xl, xl + 127))
-        part = pupdate_rows<T, true>(a, L, tab, lane, xl, y0, y1, beta, z, p, pn, smem);
+        part = pupdate_rows<T, true>(a, I, L, tab, lane, x0, y0, y1, beta, z, p, pn, smem);
       else
-        part = pupdate_rows<T, false>(a, L, tab, lane, xl, y0, y1, beta, z, p, pn, smem);
+        part = pupdate_rows<T, false>(a, I, L, tab, lane, x0, y0, y1, beta, z, p, pn, smem);
     }
   }
   part = block_sum<kThreads>(part);
@@ -949,50 +888,44 @@ __global__ void __launch_bounds__(kThreads) k_pupdate_s(Args<T> a) {
 
 template <typename T, bool INT>
 __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInfo &L,
-                                                const ClassTable<T> &tab, int lane, int xl,
+                                                const ClassTable<T> &tab, int lane, int x0,
                                                 int y0, int y1, T alpha, const T *p, T *d, T *r,
                                                 bool dzero, unsigned char *smem) {
-  using K = KrylovSmem<T, 3>;
   const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
-  const int x0 = xl + 4 * lane;
-  const WarpRows<T, 3> wr(smem, threadIdx.x >> 5, xl, L.pitch);
-  const EdgeRing<T> ep(reinterpret_cast<T *>(smem + K::rows + K::bars));
-  unsigned *const err = a.counter + kErrWord;
+  const Ring<T> rp(reinterpret_cast<T *>(smem));
+  const Ring<T> rd(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
+  const Ring<T> rr(reinterpret_cast<T *>(smem) + 2 * kRing * kThreads * 4);
+  const EdgeRing<T> ep(reinterpret_cast<T *>(smem) + 3 * kRing * kThreads * 4);
   const int xe = lane == 0 ? x0 - 1 : x0 + 4;  // edge column of lanes 0 and 31
   const bool edge_lane = lane == 0 || lane == 31;
-  const bool lane_in = x0 < L.pitch;
-  const T *const src[3] = {p, d, r};
+  // p streams rows y0 - 1 .. y1; d and r the band's own rows y0 .. y1 - 1, used
+  // one step later (the slots of the two halo rows are never read); nothing past
+  // row y1 is copied
   const int nsteps = y1 - y0 + 2;
-  // p streams rows y0 - 1 .. y1; d and r rows y0 .. y1 - 1, used one step later
   auto issue = [&](int q) {
     if (q < nsteps) {
       const int y = y0 - 1 + q;
-      const bool rok = y >= 0 && y < L.ny;
       const bool own = y >= y0 && y < y1;
-      if (lane == 0)
-        wr.issue(q, src, (rok ? 1u : 0u) | (own && !dzero ? 2u : 0u) | (own ? 4u : 0u), y);
+      rp.issue(q, p, L, y, x0);
+      if (own && !dzero) rd.issue(q, d, L, y, x0);
+      if (own) rr.issue(q, r, L, y, x0);
       if (edge_lane) ep.issue(q, p, L, y, xe);
     }
     __pipeline_commit();
   };
-  for (int q = 0; q < kKrylovRing - 1; ++q) issue(q);
+  for (int q = 0; q < kRing - 1; ++q) issue(q);
   int step = 0;
   V4<T> dcur, rcur, dnext = zero4<T>(), rnext = zero4<T>();
   T edge_next = T(0);
   auto next = [&]() {
-    wr.wait(step, err);
-    __pipeline_wait_prior(kKrylovRing - 2);
-    const int y = y0 - 1 + step;
-    const bool ok = y >= 0 && y < L.ny && lane_in;
-    const bool own = y >= y0 && y < y1 && lane_in;
-    const V4<T> pp = ok ? wr.read(step, 0, lane) : zero4<T>();
+    __pipeline_wait_prior(kRing - 2);
+    const V4<T> pp = rp.read(step);
     dcur = dnext;
     rcur = rnext;
-    dnext = own && !dzero ? wr.read(step, 1, lane) : zero4<T>();
-    rnext = own ? wr.read(step, 2, lane) : zero4<T>();
+    dnext = dzero ? zero4<T>() : rd.read(step);
+    rnext = rr.read(step);
     edge_next = edge_lane ? ep.read(step) : T(0);
-    wr.release();
-    issue(step + kKrylovRing - 1);
+    issue(step + kRing - 1);
     ++step;
     return pp;
   };
@@ -1024,8 +957,8 @@ __device__ __forceinline__ double cgupdate_rows(const Args<T> &a, const LevelInf
         st4(r + g, rv);
       } else {
         for (int j = 0; j < 4 && x0 + j < L.nx; ++j) {
-          d[g + j] = dcur.v[j] + alpha * cu.v[j];
-          const T rn = rcur.v[j] - alpha * ap.v[j];
+          d[g + j] = (dzero ? T(0) : d[g + j]) + alpha * cu.v[j];
+          const T rn = r[g + j] - alpha * ap.v[j];
           r[g + j] = rn;
           part += (double)rn * (double)rn;
         }
@@ -1052,6 +985,7 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y0 = (tl.ty * kWarps + warp) * kKrylovRows;
     const int xl = tl.tx * kKrylovCols;
+    const int x0 = xl + 4 * lane;
     if (y0 < L.ny) {
       const int y1 = min(y0 + kKrylovRows, L.ny);
       const T alpha = (T)a.st[tl.inst].alpha;
@@ -1061,9 +995,9 @@ __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
       const bool dzero = a.st[tl.inst].flags & FLAG_DZERO;
       extern __shared__ __align__(16) unsigned char smem[];
       if (strip_interior(L, y0, y1 - 1, xl, xl + 127))
-        part = cgupdate_rows<T, true>(a, L, tab, lane, xl, y0, y1, alpha, p, d, r, dzero, smem);
+        part = cgupdate_rows<T, true>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, dzero, smem);
       else
-        part = cgupdate_rows<T, false>(a, L, tab, lane, xl, y0, y1, alpha, p, d, r, dzero, smem);
+        part = cgupdate_rows<T, false>(a, L, tab, lane, x0, y0, y1, alpha, p, d, r, dzero, smem);
     }
   }
   part = block_sum<kThreads>(part);
