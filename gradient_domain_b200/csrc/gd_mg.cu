@@ -340,17 +340,22 @@ int bottom_layout(gd_plan p, int first, int last, size_t es, bool write) {
     off = a16(off + cells * es);
     const size_t u = off;
     off = a16(off + cells * es);
+    const size_t r = off;
+    off = a16(off + cells * es);
     const size_t c = off;
     off = a16(off + cells);
     if (write) {
       L.sm_b = (int)b;
       L.sm_u = (int)u;
+      L.sm_r = (int)r;
       L.sm_c = (int)c;
       L.sm_px = (int)px;
     }
   }
+  // FP64 right-hand side of the dense solve, then the dense inverse
   const size_t d = off;
-  off = a16(off + (size_t)kCoarsestCells * sizeof(double));
+  off = a16(off + (size_t)kCoarsestCells * sizeof(double) +
+            (size_t)kCoarsestCells * kCoarsestCells * sizeof(double));
   if (write) {
     p->lv[last].sm_d = (int)d;
     for (int l = first; l <= last; ++l) p->lv[l].sm_end = (int)off;

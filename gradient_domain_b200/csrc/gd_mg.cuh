@@ -42,10 +42,11 @@ struct LevelInfo {
   int bc, level, coarse, is_bottom;
   float wall, pad0;
   int rows_per_warp;  // strip height of the down / up kernels on this level (even)
-  int pad2;
-  // bottom levels: byte offsets of the padded b, u and class arrays in the
-  // bottom kernel's shared memory, their row pitch (nx + 3), the FP64 right-
-  // hand side of the dense solve (coarsest level) and the end of the layout
+  // bottom levels: byte offsets of the padded b, u, residual and class arrays
+  // in the bottom kernel's shared memory, their row pitch (nx + 3), the FP64
+  // right-hand side of the dense solve (coarsest level; the dense inverse
+  // follows it at sm_d + kCoarsestCells doubles) and the end of the layout
+  int sm_r;
   int sm_b, sm_u, sm_c, sm_px, sm_d, sm_end;
   long long b_off, u_off;  // element offsets into the T arena
   long long w_off;         // pre-smoothed iterate written by down, read by up

@@ -19,6 +19,8 @@
 // instance, down to a dense FP64 solve.
 #pragma once
 
+#include <cuda_pipeline.h>
+
 #include "gd_mg.cuh"
 
 namespace gd {
@@ -98,9 +100,10 @@ __device__ __forceinline__ int mirror_fine(int f, int n, bool neumann) {
 // an odd-sized level reaches two cells past its edge).  A missing neighbour
 // then reads 0, as the operator defines, and Dirichlet / masked transfers read
 // zero ghosts, so no stencil needs a bounds check.  A warp works on whole rows
-// and its lanes on columns, so no index is divided.  The residual overwrites b
-// in place and the up pass reloads b from the arena, where the restriction also
-// writes it.
+// and its lanes on columns, so no index is divided.  The residual goes to its
+// own array, so b stays in shared memory for the up pass; only the top level's
+// b comes from (and its u goes back to) global memory.  The dense inverse of
+// the coarsest level is copied in by cp.async while the down pass runs.
 
 template <typename T>
 __device__ __forceinline__ void bot_sweep(T *u, const T *b, const unsigned char *c, int ny,
@@ -139,8 +142,17 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
   const int nb = I.coarsest - I.bottom + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = kBThreads / 32;
-  {  // zero every padded array (ghost rings stay zero for the whole launch)
-    const int bytes = a.lv[I.coarsest].sm_end;
+  const LevelInfo &Lq = a.lv[I.coarsest];
+  const int nq = Lq.ny * Lq.nx;
+  double *const inv_s = reinterpret_cast<double *>(smem + Lq.sm_d) + kCoarsestCells;
+  {  // the coarsest inverse travels while the levels above are worked on
+    const double *inv_g = a.dense + Lq.inv_off;
+    for (int k = threadIdx.x; k < nq * nq; k += kBThreads)
+      __pipeline_memcpy_async(inv_s + k, inv_g + k, sizeof(double));
+    __pipeline_commit();
+  }
+  {  // zero every padded array up to the inverse (ghost rings stay zero for the whole launch)
+    const int bytes = Lq.sm_d + kCoarsestCells * (int)sizeof(double);
     uint4 *z = reinterpret_cast<uint4 *>(smem);
     for (int k = threadIdx.x; k < bytes / 16; k += kBThreads) z[k] = make_uint4(0, 0, 0, 0);
   }
@@ -175,7 +187,8 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
     const LevelInfo &L = a.lv[I.bottom + q];
     const LevelInfo &C = a.lv[I.bottom + q + 1];
     T *u = reinterpret_cast<T *>(smem + L.sm_u);
-    T *b = reinterpret_cast<T *>(smem + L.sm_b);
+    const T *b = reinterpret_cast<const T *>(smem + L.sm_b);
+    T *res = reinterpret_cast<T *>(smem + L.sm_r);
     const unsigned char *c = smem + L.sm_c;
     const int px = L.sm_px;
     for (int s = 0; s < S1; ++s) {
@@ -188,13 +201,12 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
         const int i = row + x;
         const int cl = c[i];
         const T nbs = u[i - px] + u[i + px] + u[i - 1] + u[i + 1];
-        b[i] = cl ? b[i] - (tdiag[q][cl] * u[i] - nbs) : T(0);
+        res[i] = cl ? b[i] - (tdiag[q][cl] * u[i] - nbs) : T(0);
       }
     }
     __syncthreads();
     T *bc = reinterpret_cast<T *>(smem + C.sm_b);
     const unsigned char *cc = smem + C.sm_c;
-    T *Bg = a.arena + C.b_off;
     const bool neu = L.bc == BC_NEU;
     const int cpx = C.sm_px;
     for (int Iy = warp; Iy < C.ny; Iy += NW) {
@@ -212,12 +224,11 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
           for (int pp = 0; pp < 4; ++pp) {
             T rowv = T(0);
 #pragma unroll
-            for (int r = 0; r < 4; ++r) rowv += (T)rweight(r) * b[fy[pp] + fx[r]];
+            for (int r = 0; r < 4; ++r) rowv += (T)rweight(r) * res[fy[pp] + fx[r]];
             acc += (T)rweight(pp) * rowv;
           }
         }
         bc[ci] = acc;
-        Bg[(long long)Iy * C.pitch + Jx] = acc;
       }
     }
     __syncthreads();
@@ -233,8 +244,9 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
       const int y = k / L.nx, x = k - y * L.nx;
       bd[k] = (double)b[(y + 1) * px + 1 + x];
     }
+    __pipeline_wait_prior(0);
     __syncthreads();
-    const double *inv = a.dense + L.inv_off;
+    const double *inv = inv_s;
     for (int t = warp; t < n; t += NW) {
       double acc = 0.0;
       for (int j = lane; j < n; j += 32) acc += inv[(long long)t * n + j] * bd[j];
@@ -254,7 +266,6 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
     T *b = reinterpret_cast<T *>(smem + L.sm_b);
     const T *e = reinterpret_cast<const T *>(smem + C.sm_u);
     const unsigned char *c = smem + L.sm_c;
-    const T *Bg = a.arena + L.b_off;
     const bool neu = L.bc == BC_NEU;
     const int px = L.sm_px, cpx = C.sm_px;
     for (int y = warp; y < L.ny; y += NW) {
@@ -265,7 +276,6 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
       const int r1 = (cy + 1) * cpx + 1, r2 = (cy2 + 1) * cpx + 1;
       for (int x = lane; x < L.nx; x += 32) {
         const int i = row + x;
-        b[i] = Bg[(long long)y * L.pitch + x];
         if (!c[i]) continue;
         const int cx = x >> 1;
         int cx2 = (x & 1) ? cx + 1 : cx - 1;

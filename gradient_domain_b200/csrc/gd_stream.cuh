@@ -399,8 +399,10 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
       __pipeline_wait_prior(kRing - 2);
       Bw[wslot<U>(ph, 0)] = ring.read(step);
       if (!INT) Cw[wslot<U>(ph, 0)] = masked ? cring.read(step) : row_classes(L, nullptr, y, x0);
-      ring.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
-      if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      if (y + kRing - 1 <= y_last) {  // no copy of rows past the strip
+        ring.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
+        if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      }
       __pipeline_commit();
       // y_start is even, so the parity of y is the parity of ph
       if ((ph & 1) == 0)
@@ -504,7 +506,7 @@ __device__ __forceinline__ bool strip_interior(const LevelInfo &L, int y_lo, int
 }
 
 template <typename T, int S1>
-__global__ void __launch_bounds__(kThreads) k_down_s(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, 4) k_down_s(Args<T> a) {
   using G = DownGeom<T, S1>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -641,9 +643,11 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
       Bw[wslot<U>(ph, 0)] = rb.read(step);
       V4<T> u = rw.read(step);
       if (!INT) Cw[wslot<U>(ph, 0)] = masked ? cring.read(step) : row_classes(L, nullptr, y, x0);
-      rb.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
-      rw.issue(step + kRing - 1, Wp, L, y + kRing - 1, x0);
-      if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      if (y + kRing - 1 <= y_last) {  // no copy of rows past the strip
+        rb.issue(step + kRing - 1, B, L, y + kRing - 1, x0);
+        rw.issue(step + kRing - 1, Wp, L, y + kRing - 1, x0);
+        if (!INT && masked) cring.issue(step + kRing - 1, L, a.codes, y + kRing - 1, x0);
+      }
       __pipeline_commit();
       {  // prolongation of row y; the coarse window holds rows cy - 1, cy, cy + 1
         const int cy = y >> 1;
@@ -701,8 +705,9 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
   return part;
 }
 
+// Three CTAs per SM: above 170 registers only two fit, which was measured slower.
 template <typename T, int S1, int S2, bool LEVEL0>
-__global__ void __launch_bounds__(kThreads) k_up_s(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, 3) k_up_s(Args<T> a) {
   using G = UpGeom<T, S1, S2>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
