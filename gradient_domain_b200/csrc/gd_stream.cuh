@@ -506,7 +506,7 @@ __device__ __forceinline__ bool strip_interior(const LevelInfo &L, int y_lo, int
 }
 
 template <typename T, int S1>
-__global__ void __launch_bounds__(kThreads, 4) k_down_s(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_down_s(Args<T> a) {
   using G = DownGeom<T, S1>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -705,9 +705,10 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
   return part;
 }
 
-// Three CTAs per SM: above 170 registers only two fit, which was measured slower.
+// FP32: three CTAs per SM (above 170 registers only two fit, which was measured
+// slower); the FP64 form needs more registers than that and is left unbounded.
 template <typename T, int S1, int S2, bool LEVEL0>
-__global__ void __launch_bounds__(kThreads, 3) k_up_s(Args<T> a) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) k_up_s(Args<T> a) {
   using G = UpGeom<T, S1, S2>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
