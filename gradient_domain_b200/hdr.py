@@ -19,6 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._host import download, upload
 from .plan import Instance, SolveParams, cached_plan
 
 __all__ = ["ToneMapConfig", "attenuation_field", "tone_map"]
@@ -71,8 +72,8 @@ def _attenuation_dev(logl: torch.Tensor, config: ToneMapConfig,
 def attenuation_field(log_luminance, config: ToneMapConfig) -> np.ndarray:
     """Multiscale gradient attenuation factor, propagated coarse to fine."""
     dev = _lib.device()
-    logl = torch.as_tensor(np.ascontiguousarray(log_luminance, dtype=np.float64)).to(dev)
-    return _attenuation_dev(logl, config, _scratch(dev)).cpu().numpy()
+    logl = upload(log_luminance, dev, np.float64)
+    return download(_attenuation_dev(logl, config, _scratch(dev)))
 
 
 def tone_map(radiance, config: ToneMapConfig | None = None):
@@ -88,7 +89,7 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
     h, w, _ = radiance.shape
     dev = _lib.device()
     lib, st = _lib.lib(), _lib.stream_handle()
-    rad = torch.as_tensor(np.ascontiguousarray(radiance)).to(dev)
+    rad = upload(radiance, dev, np.float64)
     logl = torch.empty((h, w), dtype=torch.float64, device=dev)
     lum = torch.empty_like(logl)
     _lib.check(lib.gd_tm_log_luminance(_lib.ptr(logl), _lib.ptr(lum), _lib.ptr(rad), h, w, st),
@@ -115,4 +116,4 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
     _lib.check(lib.gd_tm_compose(_lib.ptr(out), _lib.ptr(image), _lib.ptr(rad), _lib.ptr(lum),
                                  _lib.ptr(compressed), h, w, float(config.saturation), 99.5,
                                  _lib.ptr(scratch), st), "gd_tm_compose")
-    return out.cpu().numpy(), factor.cpu().numpy()
+    return download(out), download(factor)

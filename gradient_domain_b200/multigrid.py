@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._host import download, upload
 
 
 @dataclass
@@ -92,7 +93,7 @@ class RefWorkspace:
 
 
 def _to_dev(a, dev) -> torch.Tensor:
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev).contiguous()
+    return upload(a, dev, np.float64)
 
 
 def v_cycle(u, b, spacing: float, options: MultigridOptions) -> np.ndarray:
@@ -103,7 +104,7 @@ def v_cycle(u, b, spacing: float, options: MultigridOptions) -> np.ndarray:
     if u_d.shape != b_d.shape or u_d.dim() != 2:
         raise ValueError("u and b must be 2-D arrays of the same shape")
     RefWorkspace(tuple(b_d.shape), options.coarsest_size, dev).vcycle(u_d, b_d, spacing, options)
-    return u_d.cpu().numpy()
+    return download(u_d)
 
 
 def solve(b, spacing: float = 1.0, options: MultigridOptions | None = None,
@@ -117,7 +118,7 @@ def solve(b, spacing: float = 1.0, options: MultigridOptions | None = None,
     ws = RefWorkspace(tuple(b_d.shape), options.coarsest_size, dev)
     scale = float(np.sqrt(ws.dot(b_d, b_d)))
     if scale == 0.0:
-        return u_d.cpu().numpy(), MultigridReport([0.0], 0, True)
+        return download(u_d), MultigridReport([0.0], 0, True)
     r_d = torch.empty_like(b_d)
 
     def rel_residual() -> float:
@@ -129,5 +130,5 @@ def solve(b, spacing: float = 1.0, options: MultigridOptions | None = None,
         ws.vcycle(u_d, b_d, spacing, options)
         history.append(rel_residual())
         if history[-1] < options.tolerance:
-            return u_d.cpu().numpy(), MultigridReport(history, cycle, True)
-    return u_d.cpu().numpy(), MultigridReport(history, options.max_cycles, False)
+            return download(u_d), MultigridReport(history, cycle, True)
+    return download(u_d), MultigridReport(history, options.max_cycles, False)

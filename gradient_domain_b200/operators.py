@@ -14,12 +14,13 @@ import scipy.sparse as sp
 import torch
 
 from . import _lib
+from ._host import download, upload
 
 __all__ = ["gradient", "divergence", "laplacian", "sparse_laplacian", "fold_boundary"]
 
 
 def _dev(a, dev) -> torch.Tensor:
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    return upload(a, dev, np.float64)
 
 
 def _channels_first(a: torch.Tensor) -> torch.Tensor:
@@ -27,8 +28,7 @@ def _channels_first(a: torch.Tensor) -> torch.Tensor:
 
 
 def _channels_last(a: torch.Tensor, ndim: int) -> np.ndarray:
-    out = a[0] if ndim == 2 else a.permute(1, 2, 0)
-    return out.cpu().numpy()
+    return download(a[0] if ndim == 2 else a.permute(1, 2, 0))
 
 
 def gradient_dev(u: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
@@ -115,4 +115,4 @@ def fold_boundary(right_hand_side, boundary, spacing: float = 1.0) -> np.ndarray
     out = torch.empty((h - 2, w - 2), dtype=torch.float64, device=dev)
     _lib.check(_lib.lib().gd_fold_dirichlet(_lib.ptr(out), _lib.ptr(div), _lib.ptr(_dev(bnd, dev)),
                                             h, w, 1.0, _lib.stream_handle()), "gd_fold_dirichlet")
-    return out.cpu().numpy()
+    return download(out)

@@ -26,6 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._host import download, upload
 from .operators import divergence_dev, gradient
 from .plan import Instance, SolveParams, cached_plan
 from .solvers import SolverReport, solve_system
@@ -68,8 +69,7 @@ def _as_channels(image: np.ndarray):
 
 
 def _to_chw(a: np.ndarray, dev) -> torch.Tensor:
-    a = np.asarray(a, dtype=np.float64)
-    t = torch.as_tensor(np.ascontiguousarray(a)).to(dev)
+    t = upload(a, dev, np.float64)
     return t.unsqueeze(0) if t.dim() == 2 else t.permute(2, 0, 1).contiguous()
 
 
@@ -101,7 +101,7 @@ def _dirichlet_from_div(div: torch.Tensor, bnd: np.ndarray, bnd_d: torch.Tensor,
     result = bnd.copy()
     if method not in ("mgcg", "mgcg_fp64"):
         reports = []
-        folded = f.cpu().numpy()
+        folded = download(f)
         for k in range(c):
             sol, rep = solve_system(folded[k], method=method, tolerance=tolerance,
                                     max_iterations=max_iterations)
@@ -115,7 +115,7 @@ def _dirichlet_from_div(div: torch.Tensor, bnd: np.ndarray, bnd_d: torch.Tensor,
     started = time.perf_counter()
     results = plan.solve(list(f), list(x), scale=-1.0)
     elapsed = time.perf_counter() - started
-    result[1:-1, 1:-1, :] = x.permute(1, 2, 0).cpu().numpy()
+    result[1:-1, 1:-1, :] = download(x.permute(1, 2, 0))
     return (result[..., 0] if gray else result), _reports(results, method, elapsed)
 
 
@@ -191,9 +191,9 @@ def solve_masked(field: GuidanceField, image, mask, tolerance: float = DIRECT_TO
     sub = GuidanceField(np.asarray(field.gx)[win], np.asarray(field.gy)[win])
     div = _field_divergence(sub, c, dev)
     img_d = _to_chw(chans[win], dev)
-    unk = torch.as_tensor(np.ascontiguousarray(interior[win]).astype(np.uint8)).to(dev)
+    unk = upload(interior[win], dev, np.uint8)
     x, results, elapsed = _masked_from_div(div, img_d, unk, tolerance, max_iterations, precision)
-    sol = x.permute(1, 2, 0).cpu().numpy()
+    sol = download(x.permute(1, 2, 0))
     out = chans.copy()
     inner_win = interior[win]
     out_win = out[win]
@@ -214,7 +214,7 @@ class _DeviceImages:
         self.gray = target.ndim == 2
         t = target[..., None] if self.gray else target
         self.h, self.w, self.c = t.shape
-        self.target = torch.as_tensor(np.ascontiguousarray(t, dtype=np.float64)).to(dev)
+        self.target = upload(t, dev, np.float64)
         self.keep = []  # device buffers referenced by descriptors
 
     def desc(self, kind: int, channel: int, source=None, select=None, weights=None,
@@ -244,18 +244,17 @@ def _edit_masked(imgs: _DeviceImages, descs, mask: np.ndarray, tolerance: float,
     interior = _interior(mask)
     host = imgs.target
     if not interior.any():
-        out = host.cpu().numpy()
+        out = download(host)
         return (out[..., 0] if imgs.gray else out), []
     r0, r1, c0, c1 = _window(interior)
     div = imgs.divergence(descs, r0, c0, r1 - r0, c1 - c0)
     img_win = imgs.channels(r0, r1, c0, c1)
-    unk = torch.as_tensor(np.ascontiguousarray(interior[r0:r1, c0:c1]).astype(np.uint8)).to(
-        host.device)
+    unk = upload(interior[r0:r1, c0:c1], host.device, np.uint8)
     x, results, elapsed = _masked_from_div(div, img_win, unk, tolerance, 2000, "mixed")
     out = host.clone()
     win = out[r0:r1, c0:c1, :]
     win.copy_(torch.where(unk.bool()[..., None], x.permute(1, 2, 0), win))
-    res = out.cpu().numpy()
+    res = download(out)
     return (res[..., 0] if imgs.gray else res), _reports(results, label, elapsed)
 
 
@@ -263,7 +262,7 @@ def _edit_rectangle(imgs: _DeviceImages, descs, r0: int, r1: int, c0: int, c1: i
                     method: str, tolerance: float):
     div = imgs.divergence(descs, r0, c0, r1 - r0, c1 - c0)
     bnd_d = imgs.channels(r0, r1, c0, c1)
-    bnd = bnd_d.permute(1, 2, 0).cpu().numpy()
+    bnd = download(bnd_d.permute(1, 2, 0))
     return _dirichlet_from_div(div, bnd, bnd_d, False, method, tolerance, 2000)
 
 
@@ -307,9 +306,8 @@ def seamless_clone(source, target, mask, offset=(0, 0), mode: str = "import",
     imgs = _DeviceImages(target, dev)
     canvas = torch.zeros_like(imgs.target)
     src = source[..., None] if source.ndim == 2 else source
-    canvas[row:row + height, column:column + width, :] = torch.as_tensor(
-        np.ascontiguousarray(src)).to(dev)
-    sel = torch.as_tensor(placed_mask.astype(np.uint8)).to(dev)
+    canvas[row:row + height, column:column + width, :] = upload(src, dev, np.float64)
+    sel = upload(placed_mask, dev, np.uint8)
     descs = [imgs.desc(_CLONE_KINDS[mode], ch, source=canvas, select=sel) for ch in range(imgs.c)]
     if domain == "mask":
         return _edit_masked(imgs, descs, placed_mask,
@@ -336,7 +334,7 @@ def texture_flatten(image, edges, method: str = "mgcg", mask=None):
     weights = np.ascontiguousarray(np.asarray(edges, dtype=float))
     dev = _lib.device()
     imgs = _DeviceImages(image, dev)
-    wts = torch.as_tensor(weights).to(dev)
+    wts = upload(weights, dev, np.float64)
     descs = [imgs.desc(_lib.GD_FIELD_WEIGHTED, ch, weights=wts) for ch in range(imgs.c)]
     if mask is not None:
         return _edit_masked(imgs, descs, np.asarray(mask, dtype=bool), DIRECT_TOLERANCE)

@@ -41,6 +41,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._host import download, upload
 from .multigrid import MultigridOptions, RefWorkspace
 from .plan import Instance, PoissonPlan, SolveParams, cached_plan
 
@@ -64,7 +65,7 @@ class SolverReport:
 
 
 def _dev_array(a, dev: torch.device) -> torch.Tensor:
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    return upload(a, dev, np.float64)
 
 
 def _plan_solve(b: np.ndarray, spacing: float, boundary: str, params: SolveParams,
@@ -75,7 +76,7 @@ def _plan_solve(b: np.ndarray, spacing: float, boundary: str, params: SolveParam
     f = _dev_array(b, dev)
     x = torch.zeros_like(f)
     (res,) = plan.solve([f], [x], scale=-(spacing * spacing))
-    return x.cpu().numpy(), res
+    return download(x), res
 
 
 def _solve_mgcg(b, spacing, tolerance, max_iterations):
@@ -131,12 +132,12 @@ def _ref_pcg(b, spacing, tolerance, max_iterations, precondition_kind: str):
         ws.axpby(u, p, alpha, 1.0)
         ws.axpby(r, q, -alpha, 1.0)
         if float(np.sqrt(ws.dot(r, r))) <= target:
-            return u.cpu().numpy(), it, True
+            return download(u), it, True
         z = precondition(r)
         rz_new = ws.dot(r, z)
         ws.axpby(p, z, 1.0, rz_new / rz)
         rz = rz_new
-    return u.cpu().numpy(), max_iterations, False
+    return download(u), max_iterations, False
 
 
 def _solve_cg(b, spacing, tolerance, max_iterations):
@@ -160,8 +161,8 @@ def _solve_multigrid(b, spacing, tolerance, max_iterations):
         ws.vcycle(u, b_d, spacing, opts)
         ws.residual(r, u, b_d, spacing)
         if float(np.sqrt(ws.dot(r, r))) / scale < tolerance:
-            return u.cpu().numpy(), cycle, True
-    return u.cpu().numpy(), max_iterations, False
+            return download(u), cycle, True
+    return download(u), max_iterations, False
 
 
 SOLVERS = {
@@ -285,7 +286,7 @@ def solve_neumann(b, tolerance: float = NEUMANN_EXACT_TOLERANCE,
             raise ValueError("the DCT solver needs at least 2 x 2 cells")
         dev = _lib.device()
         bd = _dev_array(b, dev)
-        return _dct_plan(*b.shape).solve(bd, torch.empty_like(bd)).cpu().numpy()
+        return download(_dct_plan(*b.shape).solve(bd, torch.empty_like(bd)))
     if method != "mgcg":
         raise KeyError(f"unknown Neumann method {method!r}; choose 'mgcg' or 'dct'")
     params = SolveParams(tolerance=tolerance, max_iterations=max_iterations)
@@ -310,7 +311,7 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
     dev = _lib.device()
     if method == "dct":
         f = (b.to(device=dev, dtype=torch.float64) if isinstance(b, torch.Tensor)
-             else torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64)).to(dev))
+             else upload(b, dev, np.float64))
         if f.dim() != 3 or min(f.shape[1:]) < 2:
             raise ValueError("solve_neumann_batch expects an (n, h, w) stack with h, w >= 2")
         f = f.contiguous()
@@ -323,7 +324,7 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
             out.copy_(x, non_blocking=True)
             torch.cuda.current_stream().synchronize()
             return out
-        return x.cpu().numpy()
+        return download(x)
     if method != "mgcg":
         raise KeyError(f"unknown Neumann method {method!r}; choose 'mgcg' or 'dct'")
     if (isinstance(b, torch.Tensor) and isinstance(out, torch.Tensor) and b.dim() == 3
@@ -337,7 +338,7 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
     if isinstance(b, torch.Tensor):
         f = b.to(device=dev, dtype=torch.float64, non_blocking=True)
     else:
-        f = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64)).to(dev)
+        f = upload(b, dev, np.float64)
     if f.dim() != 3:
         raise ValueError("solve_neumann_batch expects an (n, h, w) stack")
     n, h, w = f.shape
@@ -351,7 +352,7 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
         solve_neumann_batch.last_results = results
         return out
     solve_neumann_batch.last_results = results
-    return x.cpu().numpy()
+    return download(x)
 
 
 solve_neumann_batch.last_results = []
