@@ -489,7 +489,11 @@ def composite(args) -> None:
     kt = plan.kernel_times()
     plan.set_profiling(False)
     value = replicas.aggregate_rate(unknowns * n_ch, world, ms / 1e3) / 1e6
-    # end to end: the public seamless_clone from host arrays (field, RHS and copies included)
+    # end to end: the public seamless_clone from host arrays (field, RHS and copies included);
+    # the warm-up calls build the cached plan and its graph and fill the pinned-memory cache
+    for _ in range(args.warmup):
+        gd.seamless_clone(src, tgt, mask, (0, 0), domain="mask", tolerance=args.tol)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_steps = max(1, args.steps // 2)
     for _ in range(e2e_steps):

@@ -1,22 +1,68 @@
 """Host <-> device transfers of the NumPy entry points.
 
 The reference's functions take and return NumPy arrays, so every call moves
-its images across PCIe.  From pageable NumPy memory the driver copies through
-its own bounce buffers (about 10 GB/s up and, into freshly allocated result
-arrays that are still being faulted in, about 2 GB/s down).  Larger arrays go
-through page-locked memory from torch's pinned-memory cache instead: the input
-is copied into a pinned buffer by a multi-threaded host copy and then moved by
-DMA at PCIe speed, and results are copied by DMA straight into a pinned buffer
-that the returned array wraps (the buffer returns to torch's cache when the
-array is released).
+its images across PCIe.  Copies from and to pageable NumPy memory go through
+the driver's bounce buffers: about 10 GB/s up and, into a freshly allocated
+result that is still being faulted in, about 2 GB/s down (100 MB: 8 and
+45 ms).  Larger arrays go through page-locked staging buffers owned by this
+module instead: a multi-threaded host copy into the buffer and a DMA at PCIe
+speed (100 MB up 3.8 ms, down 5.1 ms).  Results are ordinary NumPy arrays; the
+staging buffers are reused, so retained results pin no memory.
+
+Per device there are two upload buffers, used alternately (the next upload
+into a buffer waits for its previous DMA), and one download buffer; each grows
+to the largest array moved through it, so a process that works on 2048 x 2048
+x 3 FP64 images keeps about 300 MB of page-locked memory.
 """
 
 from __future__ import annotations
+
+import threading
 
 import numpy as np
 import torch
 
 _STAGE_MIN_BYTES = 1 << 20  # smaller arrays take the direct path
+_UPLOAD_SLOTS = 2
+
+
+class _Slot:
+    def __init__(self):
+        self.buf: torch.Tensor | None = None  # uint8, page-locked
+        self.done: torch.cuda.Event | None = None  # recorded after the slot's last DMA
+
+    def take(self, nbytes: int) -> torch.Tensor:
+        if self.done is not None:
+            self.done.synchronize()
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = None
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        return self.buf[:nbytes]
+
+
+class _Pool:
+    def __init__(self):
+        self.lock = threading.Lock()
+        self.up = [_Slot() for _ in range(_UPLOAD_SLOTS)]
+        self.next_up = 0
+        self.down = _Slot()
+
+
+_POOLS: dict[int, _Pool] = {}
+_POOLS_LOCK = threading.Lock()
+
+
+def _pool(dev: torch.device) -> _Pool:
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    with _POOLS_LOCK:
+        pool = _POOLS.get(idx)
+        if pool is None:
+            pool = _POOLS[idx] = _Pool()
+    return pool
+
+
+def _view(raw: torch.Tensor, dtype: torch.dtype, shape) -> torch.Tensor:
+    return raw.view(dtype).view(shape)
 
 
 def upload(a, dev: torch.device, dtype=None) -> torch.Tensor:
@@ -25,16 +71,29 @@ def upload(a, dev: torch.device, dtype=None) -> torch.Tensor:
     src = torch.from_numpy(arr)
     if arr.nbytes < _STAGE_MIN_BYTES:
         return src.to(dev)
-    stage = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
-    stage.copy_(src)
-    return stage.to(dev, non_blocking=True)
+    pool = _pool(dev)
+    with pool.lock:
+        slot = pool.up[pool.next_up]
+        pool.next_up = (pool.next_up + 1) % _UPLOAD_SLOTS
+        stage = _view(slot.take(arr.nbytes), src.dtype, src.shape)
+        stage.copy_(src)
+        out = torch.empty(src.shape, dtype=src.dtype, device=dev)
+        out.copy_(stage, non_blocking=True)
+        slot.done = torch.cuda.Event()
+        slot.done.record(torch.cuda.current_stream(dev))
+    return out
 
 
 def download(t: torch.Tensor) -> np.ndarray:
-    """A device tensor as a NumPy array (contiguous, in page-locked memory when large)."""
-    if t.numel() * t.element_size() < _STAGE_MIN_BYTES:
+    """A device tensor as a new, contiguous NumPy array."""
+    nbytes = t.numel() * t.element_size()
+    if nbytes < _STAGE_MIN_BYTES:
         return t.cpu().numpy()
-    out = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
-    out.copy_(t, non_blocking=True)
-    torch.cuda.current_stream(t.device).synchronize()
-    return out.numpy()
+    pool = _pool(t.device)
+    with pool.lock:
+        stage = _view(pool.down.take(nbytes), t.dtype, tuple(t.shape))
+        stage.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+        out = np.empty(tuple(t.shape), dtype=stage.numpy().dtype)
+        torch.from_numpy(out).copy_(stage)
+    return out
