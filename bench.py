@@ -196,14 +196,15 @@ def ours(args) -> None:
     n_ch = rhs_np.shape[0]
     cells = n_ch * size * size
     f = torch.as_tensor(rhs_np).to(dev)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     insts = [Instance(size, size, "neumann", zero_mean=True) for _ in range(n_ch)]
+    # every solve starts from zero (as the reference's solve_neumann); x is only written
     plan = PoissonPlan(insts, SolveParams(precision="mixed", tolerance=args.tol,
-                                          sweeps=args.sweeps, reliable_delta=args.delta))
+                                          sweeps=args.sweeps, reliable_delta=args.delta,
+                                          zero_start=True))
     stream = torch.cuda.current_stream()
 
     def step(p):
-        x.zero_()
         return p.solve(list(f), list(x), scale=-1.0)
 
     def barrier():
@@ -270,7 +271,7 @@ def ours(args) -> None:
 
     # FP64 MGPCG on the same workload (the precision baseline)
     plan64 = PoissonPlan(insts, SolveParams(precision="fp64", tolerance=args.tol,
-                                            sweeps=args.sweeps))
+                                            sweeps=args.sweeps, zero_start=True))
     for _ in range(2):  # the second solve builds the plan's graph
         step(plan64)
     barrier()
@@ -287,31 +288,33 @@ def ours(args) -> None:
 
     # the literal GPU port of the reference mgcg (vertex-centred V-cycle, one kernel per
     # operation, FP64, scalars read back every iteration) against the B200 solver on the
-    # same 4096^2 Dirichlet manufactured problem (the reference mgcg is Dirichlet-only)
+    # same 4096^2 Dirichlet manufactured problem (the reference mgcg is Dirichlet-only);
+    # both device-resident: right-hand side on the device, solution left there
     port = None
     if rank == 0 and not args.no_port:
         from gradient_domain_b200 import benchmark as gbench
-        from gradient_domain_b200.solvers import SOLVERS
+        from gradient_domain_b200.solvers import _ref_pcg_dev
         bm, _ = gbench.manufactured_problem((size, size), seed=0)
-        SOLVERS["mgcg_port"](bm, 1.0, args.tol, 2000)  # warm-up: allocations, kernel loads
+        bmd = torch.as_tensor(bm).to(dev)
+        _ref_pcg_dev(bmd, 1.0, args.tol, 2000, "vcycle")  # warm-up: allocations, kernel loads
         torch.cuda.synchronize()
         t_port = []
         for _ in range(2):
             t0 = time.perf_counter()
-            _, it_port, ok_port = SOLVERS["mgcg_port"](bm, 1.0, args.tol, 2000)
+            _, it_port, ok_port = _ref_pcg_dev(bmd, 1.0, args.tol, 2000, "vcycle")
             torch.cuda.synchronize()
             t_port.append(time.perf_counter() - t0)
         t_port = min(t_port)
         pd = PoissonPlan([Instance(size, size, "dirichlet")],
                          SolveParams(precision="mixed", tolerance=args.tol, sweeps=args.sweeps,
-                                     reliable_delta=args.delta))
+                                     reliable_delta=args.delta, zero_start=True))
         fd = torch.as_tensor(bm).to(dev)
-        xd = torch.zeros_like(fd)
-        pd.solve([fd], [xd], scale=-1.0)
+        xd = torch.empty_like(fd)
+        for _ in range(2):  # the second solve captures the plan's graph
+            pd.solve([fd], [xd], scale=-1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(3):
-            xd.zero_()
             (rd,) = pd.solve([fd], [xd], scale=-1.0)
         torch.cuda.synchronize()
         t_ours = (time.perf_counter() - t0) / 3
@@ -469,17 +472,16 @@ def composite(args) -> None:
     n_ch, hb, wb = f_np.shape
     unknowns = int(unk_np.sum())
     f = torch.as_tensor(f_np).to(dev)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     unk = torch.as_tensor(unk_np.astype(np.uint8)).to(dev)
     plan = PoissonPlan([Instance(hb, wb, "masked") for _ in range(n_ch)],
                        SolveParams(tolerance=args.tol, sweeps=args.sweeps,
-                                   reliable_delta=args.delta))
+                                   reliable_delta=args.delta, zero_start=True))
 
     def step():
         for k in range(n_ch):
             plan.set_mask(k, unk)
         plan.prepare()
-        x.zero_()
         return plan.solve(list(f), list(x), scale=1.0)
 
     ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
@@ -557,18 +559,16 @@ def batch(args) -> None:
             fs.append(torch.as_tensor(np.ascontiguousarray(it["f"][k])).to(dev))
             masks.append(torch.as_tensor(it["unknown"].astype(np.uint8)).to(dev)
                          if it["boundary"] == "masked" else None)
-    xs = [torch.zeros_like(t) for t in fs]
+    xs = [torch.empty_like(t) for t in fs]
     cells = sum(t.numel() for t in fs)
     plan = PoissonPlan(insts, SolveParams(tolerance=args.tol, sweeps=args.sweeps,
-                                          reliable_delta=args.delta))
+                                          reliable_delta=args.delta, zero_start=True))
     for k, m in enumerate(masks):
         if m is not None:
             plan.set_mask(k, m)
     plan.prepare()
 
     def step():
-        for t in xs:
-            t.zero_()
         return plan.solve(fs, xs, scale=1.0)
 
     ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)

@@ -45,7 +45,7 @@ class Params(C.Structure):
                 ("tolerance", C.c_double), ("reliable_delta", C.c_double),
                 ("check_every", C.c_int32), ("use_graph", C.c_int32),
                 ("strip_target_warps", C.c_int32), ("bottom_cells", C.c_int32),
-                ("tile_cells", C.c_int32), ("reserved", C.c_int32)]
+                ("tile_cells", C.c_int32), ("zero_start", C.c_int32)]
 
 
 class Report(C.Structure):

@@ -225,6 +225,7 @@ struct Runner {
     a.tol2 = p->prm.tolerance * p->prm.tolerance;
     a.delta2 = p->fp64 ? 0.0 : p->prm.reliable_delta * p->prm.reliable_delta;
     a.max_iter = p->prm.max_iterations;
+    a.zero_start = p->prm.zero_start != 0;
     return a;
   }
 

@@ -76,7 +76,7 @@ struct InstState {
   int pcur;  // which of the two p buffers holds the current direction
   int xcur;  // where the current solution is: 0 the caller's x, 1 the plan's copy
   int refreshes;  // FP64 refreshes after the initial residual
-  int pad;
+  int xzero;      // the solution is known to be zero (zero-start solve, nothing folded yet)
 };
 
 struct Tile {
@@ -102,6 +102,7 @@ struct Args {
   int ninst;
   double tol2, delta2;
   int max_iter;
+  int zero_start;  // solves start from x = 0 without reading the caller's x
 };
 
 // Cell class: 0 = no unknown, else 1 + number of walls (missing neighbours).

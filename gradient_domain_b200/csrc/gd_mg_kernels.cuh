@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
-  if (I.zero_mean) {
+  if (I.zero_mean && !a.st[tl.inst].xzero) {  // a zero solution has mean zero
     const bool own = a.st[tl.inst].xcur != 0;
     const double *X = own ? a.xs + I.xs_off : I.x;
     const long long pitch = own ? (long long)I.pitch : I.upitch;
@@ -384,13 +384,16 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
 }
 
 // The solution into the caller's buffer: x - mean for zero-mean instances, a
-// copy when the last refresh left the solution in the plan's own copy.
+// copy when the last refresh left the solution in the plan's own copy, zeros
+// when a zero-start solve ended without folding a correction (the caller's x
+// was never read and may hold anything).
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const InstInfo &Ig = a.inst[tl.inst];
   const bool own = a.st[tl.inst].xcur != 0;
-  if (!Ig.zero_mean && !own) return;
+  const bool xz = a.st[tl.inst].xzero != 0;
+  if (!Ig.zero_mean && !own && !xz) return;
   const int ny = Ig.ny, nx = Ig.nx;
   const long long upitch = Ig.upitch;
   double *const X = Ig.x;
@@ -403,7 +406,8 @@ __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   for (int yb = Y0; yb < y1; yb += 8) {
     double v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = yb + k < y1 ? src[(long long)(yb + k) * spitch + gx] : 0.0;
+    for (int k = 0; k < 8; ++k)
+      v[k] = (yb + k < y1 && !xz) ? src[(long long)(yb + k) * spitch + gx] : 0.0;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
       if (yb + k < y1) X[(long long)(yb + k) * upitch + gx] = v[k] - m;

@@ -1115,6 +1115,7 @@ struct RefWarp {
   const unsigned char *codes;
   int ny, nx, pitch, x0, nv, y0, y1, ecol;
   bool masked, ecol_in;
+  bool xz;  // x is zero: nothing of it is read
   double scale, fmean, omw;
 };
 
@@ -1173,16 +1174,15 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
       if (lane == 0) {
         unsigned char *slot = brow + s * SM::SB;
         const unsigned xb = 128 * sizeof(double), db = FOLD ? 128 * sizeof(T) : 0;
-        bulk::arrive_expect(bar + s, (rok ? xb + db : 0u) + (pok ? xb : 0u));
-        if (rok) {
-          bulk::copy(slot, w.src + yy * w.spitch + col0, xb, bar + s);
-          if (FOLD) bulk::copy(slot + 2 * xb, w.D + (long long)yy * w.pitch + col0, db, bar + s);
-        }
+        const bool xok = rok && !w.xz;
+        bulk::arrive_expect(bar + s, (xok ? xb : 0u) + (rok ? db : 0u) + (pok ? xb : 0u));
+        if (xok) bulk::copy(slot, w.src + yy * w.spitch + col0, xb, bar + s);
+        if (FOLD && rok) bulk::copy(slot + 2 * xb, w.D + (long long)yy * w.pitch + col0, db, bar + s);
         if (pok) bulk::copy(slot + xb, w.F + p * w.upitch + col0, xb, bar + s);
       }
     } else {
       copy_row4(chunk(s, 0), chunk(s, 1), rok ? w.src + yy * w.spitch + x0 : w.src,
-                rok ? nv : 0);
+                rok && !w.xz ? nv : 0);
       if constexpr (FOLD) {
         const T *dr = rok ? w.D + (long long)yy * w.pitch + x0 : w.D;
 #pragma unroll
@@ -1197,8 +1197,9 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
     }
     if (edge_lane) {
       const bool eok = pin && w.ecol_in;
-      __pipeline_memcpy_async(eslot(s), eok ? w.src + p * w.spitch + w.ecol : w.src, 8,
-                              eok ? 0 : 8);
+      const bool exok = eok && !w.xz;
+      __pipeline_memcpy_async(eslot(s), exok ? w.src + p * w.spitch + w.ecol : w.src, 8,
+                              exok ? 0 : 8);
       if constexpr (FOLD)
         __pipeline_memcpy_async(eslot(s) + 8, eok ? w.D + (long long)p * w.pitch + w.ecol : w.D,
                                 sizeof(T), eok ? 0 : sizeof(T));
@@ -1229,7 +1230,7 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
       __pipeline_wait_prior(kRefRing - 2);
       const unsigned char *slot = brow + s * SM::SB;
       const bool pok = yy - 1 >= y0;
-      if (rok) {
+      if (rok && !w.xz) {
         read_row4(xd, slot + lane * 32, slot + lane * 32 + 16);
       } else {
 #pragma unroll
@@ -1328,7 +1329,7 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
             if (j < nv) drow[j] = xc[j];
         }
       }
-      if (INIT && masked) {  // the caller's x is zero where there is no unknown
+      if (INIT && masked && !w.xz) {  // the caller's x is zero where there is no unknown
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (j < nv && !on[j]) w.X[p * w.upitch + x0 + j] = 0.0;
@@ -1375,6 +1376,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
     w.scale = Ig.scale;
     w.fmean = a.st[tl.inst].fmean;
     w.omw = 1.0 - (double)L.wall;
+    w.xz = INIT ? a.zero_start != 0 : a.st[tl.inst].xzero != 0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = tl.tx * kFTX;
     w.x0 = col0 + 4 * lane;
@@ -1430,11 +1432,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
           S.beta = 0.0;
           S.pcur = 0;
           S.xcur = 0;
+          S.xzero = a.zero_start;
           S.refreshes = 0;
           S.status = GD_ACTIVE;
         } else {
           S.refreshes += 1;
-          if (!(S.flags & FLAG_DZERO)) S.xcur ^= 1;  // x + d went to the other copy
+          if (!(S.flags & FLAG_DZERO)) {
+            S.xcur ^= 1;  // x + d went to the other copy
+            S.xzero = 0;
+          }
         }
         // A refresh that barely lowers the true residual (less than 3x), once
         // it is already below 1e-6 of ||f||, means the FP64 rounding floor is

@@ -109,7 +109,7 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
         _dct_plan(h, w).solve(div, compressed)
     else:
         plan = cached_plan((Instance(h, w, "neumann", True),),
-                           SolveParams(tolerance=NEUMANN_TOLERANCE))
+                           SolveParams(tolerance=NEUMANN_TOLERANCE, zero_start=True))
         plan.solve([div], [compressed], scale=-1.0)
     image = torch.empty_like(rad)
     out = torch.empty_like(rad)

@@ -39,13 +39,15 @@ class SolveParams:
     strip_target_warps: int = 1800  # smoother strip height: warps per level launch (all instances)
     bottom_cells: int = 0         # largest level solved inside the one-CTA bottom (0 = 4096)
     tile_cells: int = 0           # largest coarse level on shared-memory tiles (0 = 262144)
+    zero_start: bool = False      # start from x = 0; x is only written (need not be zeroed)
 
     def c_params(self) -> _lib.Params:
         return _lib.Params(GD_FP64 if self.precision == "fp64" else GD_MIXED, self.sweeps,
                            self.sweeps, int(self.max_iterations), float(self.tolerance),
                            float(self.reliable_delta), int(self.check_every),
                            1 if self.use_graph else 0, int(self.strip_target_warps),
-                           int(self.bottom_cells), int(self.tile_cells), 0)
+                           int(self.bottom_cells), int(self.tile_cells),
+                           1 if self.zero_start else 0)
 
 
 @dataclass(frozen=True)

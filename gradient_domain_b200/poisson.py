@@ -109,9 +109,9 @@ def _dirichlet_from_div(div: torch.Tensor, bnd: np.ndarray, bnd_d: torch.Tensor,
             reports.append(rep)
         return (result[..., 0] if gray else result), reports
     params = SolveParams(precision="fp64" if method == "mgcg_fp64" else "mixed",
-                         tolerance=tolerance, max_iterations=max_iterations)
+                         tolerance=tolerance, max_iterations=max_iterations, zero_start=True)
     plan = cached_plan(tuple(Instance(h - 2, w - 2, "dirichlet") for _ in range(c)), params)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     started = time.perf_counter()
     results = plan.solve(list(f), list(x), scale=-1.0)
     elapsed = time.perf_counter() - started
@@ -161,11 +161,12 @@ def _masked_from_div(div: torch.Tensor, img_win: torch.Tensor, unk: torch.Tensor
         _lib.check(_lib.lib().gd_masked_rhs(_lib.ptr(f[k]), _lib.ptr(div[k]),
                                             _lib.ptr(img_win[k]), _lib.ptr(unk), hc, wc, -1.0,
                                             _lib.stream_handle()), "gd_masked_rhs")
-    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations)
+    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations,
+                         zero_start=True)
     plan = cached_plan(tuple(Instance(hc, wc, "masked") for _ in range(c)), params)
     for k in range(c):
         plan.set_mask(k, unk)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     started = time.perf_counter()
     results = plan.solve(list(f), list(x), scale=1.0)
     return x, results, time.perf_counter() - started

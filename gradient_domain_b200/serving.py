@@ -162,7 +162,7 @@ class GpuBackend:
         if cp is None:
             t0 = time.perf_counter()
             params = SolveParams(tolerance=tol, sweeps=self.sweeps, use_graph=self.use_graph,
-                                 check_every=self.check_every)
+                                 check_every=self.check_every, zero_start=True)
             cp = _CachedPlan(self.torch, self.device, insts, params, state["stream"])
             while len(plans) >= self.cache_per_worker:
                 plans.pop(next(iter(plans))).close()
@@ -199,7 +199,6 @@ class GpuBackend:
                     np.copyto(view.numpy().reshape(cp.f[i].shape), np.asarray(src[k]))
                     cp.f[i].copy_(view.view(cp.f[i].shape), non_blocking=True)
                     off += n
-                cp.x[i].zero_()
             masks = {}
             for i, (q, k) in enumerate(owners):
                 if requests[q].boundary == "masked":

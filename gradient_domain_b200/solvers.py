@@ -35,7 +35,7 @@ import ctypes as C
 import threading
 import time
 from collections import OrderedDict
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 import torch
@@ -72,9 +72,9 @@ def _plan_solve(b: np.ndarray, spacing: float, boundary: str, params: SolveParam
                 zero_mean: bool = False):
     dev = _lib.device()
     m, n = b.shape
-    plan = cached_plan((Instance(m, n, boundary, zero_mean),), params)
+    plan = cached_plan((Instance(m, n, boundary, zero_mean),), replace(params, zero_start=True))
     f = _dev_array(b, dev)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     (res,) = plan.solve([f], [x], scale=-(spacing * spacing))
     return download(x), res
 
@@ -98,10 +98,10 @@ def _solve_direct(b, spacing, tolerance, max_iterations):
     return u, 0, True
 
 
-def _ref_pcg(b, spacing, tolerance, max_iterations, precondition_kind: str):
-    """The reference's PCG loop (solvers.py:99-118, :142-160) with device arrays."""
-    dev = _lib.device()
-    b_d = _dev_array(b, dev)
+def _ref_pcg_dev(b_d: torch.Tensor, spacing, tolerance, max_iterations, precondition_kind: str):
+    """The reference's PCG loop (solvers.py:99-118, :142-160) on a device right-hand
+    side; returns the device solution, the iteration count and convergence."""
+    dev = b_d.device
     ws = RefWorkspace(tuple(b_d.shape), 8, dev)
     opts = MultigridOptions(pre_smoothing=1, post_smoothing=1)
     zeros = torch.zeros_like(b_d)
@@ -132,12 +132,19 @@ def _ref_pcg(b, spacing, tolerance, max_iterations, precondition_kind: str):
         ws.axpby(u, p, alpha, 1.0)
         ws.axpby(r, q, -alpha, 1.0)
         if float(np.sqrt(ws.dot(r, r))) <= target:
-            return download(u), it, True
+            return u, it, True
         z = precondition(r)
         rz_new = ws.dot(r, z)
         ws.axpby(p, z, 1.0, rz_new / rz)
         rz = rz_new
-    return download(u), max_iterations, False
+    return u, max_iterations, False
+
+
+def _ref_pcg(b, spacing, tolerance, max_iterations, precondition_kind: str):
+    """The reference's PCG loop with device arrays, from and to NumPy."""
+    u, it, ok = _ref_pcg_dev(_dev_array(b, _lib.device()), spacing, tolerance, max_iterations,
+                             precondition_kind)
+    return download(u), it, ok
 
 
 def _solve_cg(b, spacing, tolerance, max_iterations):
@@ -332,7 +339,7 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
             and b.device.type == "cpu" and out.device.type == "cpu" and b.is_pinned()
             and out.is_pinned() and out.shape == b.shape):
         params = SolveParams(precision=precision, tolerance=tolerance,
-                             max_iterations=max_iterations)
+                             max_iterations=max_iterations, zero_start=True)
         solve_neumann_batch.last_results = _pipelined_neumann(b, out, params)
         return out
     if isinstance(b, torch.Tensor):
@@ -342,9 +349,10 @@ def solve_neumann_batch(b, tolerance: float = NEUMANN_EXACT_TOLERANCE, max_itera
     if f.dim() != 3:
         raise ValueError("solve_neumann_batch expects an (n, h, w) stack")
     n, h, w = f.shape
-    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations)
+    params = SolveParams(precision=precision, tolerance=tolerance, max_iterations=max_iterations,
+                         zero_start=True)
     plan = cached_plan(tuple(Instance(h, w, "neumann", True) for _ in range(n)), params)
-    x = torch.zeros_like(f)
+    x = torch.empty_like(f)
     results = plan.solve(list(f), list(x), scale=-1.0)
     if out is not None:
         out.copy_(x, non_blocking=True)
@@ -409,7 +417,6 @@ def _pipelined_neumann(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
             stream.wait_stream(caller)
             with torch.cuda.stream(stream):
                 f.copy_(b[k], non_blocking=True)
-                x.zero_()
                 plan.solve_async([f], [x], scale=-1.0)
                 out[k].copy_(x, non_blocking=True)
         results = []

@@ -77,7 +77,9 @@ typedef struct gd_params {
                                  instances together (0 = 1800)                      */
   int32_t bottom_cells;       /* largest level the one-CTA bottom takes (0 = 4096)   */
   int32_t tile_cells;         /* largest coarse level on shared-memory tiles (0 = 262144) */
-  int32_t reserved;
+  int32_t zero_start;         /* nonzero: every solve starts from x = 0 and x is only
+                                 written (it need not be initialised), as the
+                                 reference's solvers start (solvers.py:143)           */
 } gd_params;
 
 typedef struct gd_report {

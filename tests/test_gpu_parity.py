@@ -286,6 +286,39 @@ def test_caller_buffers_of_any_alignment_and_pitch(precision):
         assert _rel(xs[0].cpu().numpy(), ref) < 1e-6
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_zero_start_ignores_the_initial_x(precision):
+    """With zero_start the caller's x is only written: from garbage it gives the
+    same bits and reports as a zero-initialised solve, including an instance
+    whose right-hand side is zero (no correction is ever folded) and the graph
+    solves after the first."""
+    rng = np.random.default_rng(37)
+    active = np.zeros((70, 90), bool)
+    active[6:60, 5:80] = True
+    active[20:40, 30:50] = False
+    shapes = [(70, 90, "neumann"), (64, 77, "dirichlet"), (70, 90, "masked"), (40, 40, "neumann")]
+    rhs = [torch.as_tensor(rng.standard_normal(s[:2])).cuda() for s in shapes]
+    rhs[3] = torch.zeros((40, 40), dtype=torch.float64, device="cuda")
+    runs = {}
+    for zero_start in (False, True):
+        plan = PoissonPlan([Instance(h, w, b, b == "neumann") for h, w, b in shapes],
+                           SolveParams(precision=precision, tolerance=1e-10, zero_start=zero_start))
+        plan.set_mask(2, torch.as_tensor(active.astype(np.uint8)).cuda())
+        out = []
+        for _ in range(3):
+            xs = [torch.full_like(r, float("nan")) if zero_start else torch.zeros_like(r)
+                  for r in rhs]
+            res = plan.solve(rhs, xs, scale=-1.0)
+            out.append(([t.clone() for t in xs],
+                        [(r.iterations, r.status, r.refreshes) for r in res]))
+        runs[zero_start] = out
+    for (xa, sa), (xb, sb) in zip(runs[True], runs[False]):
+        assert sa == sb
+        for a, b in zip(xa, xb):
+            assert torch.equal(a, b)
+    assert torch.all(runs[True][0][0][3] == 0) and runs[True][0][1][3][0] == 0
+
+
 def test_zero_and_nonfinite_rhs_are_reported_not_raised():
     plan = PoissonPlan([Instance(40, 40, "dirichlet"), Instance(40, 40, "dirichlet")],
                        SolveParams())
