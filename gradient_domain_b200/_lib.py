@@ -31,6 +31,7 @@ EXPORTS = (
     "gd_masked_rhs", "gd_guidance_divergence", "gd_tm_scratch_bytes", "gd_tm_log_luminance",
     "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose", "gd_dct_plan_create",
     "gd_dct_workspace_bytes", "gd_dct_plan_bind", "gd_dct_solve_neumann", "gd_dct_plan_destroy",
+    "gd_selftest_bounded_wait",
 )
 
 
@@ -104,6 +105,7 @@ def _declare(lib: C.CDLL) -> None:
         "gd_plan_apply_vcycle": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
         "gd_plan_set_profiling": (C.c_int, [_vp, _i32]),
         "gd_plan_kernel_times": (C.c_int, [_vp, C.POINTER(KernelTime), _i32]),
+        "gd_selftest_bounded_wait": (C.c_int, [_i32, _vp, _vp, _vp]),
         "gd_ref_workspace_bytes": (_sz, [_i32, _i32, _i32]),
         "gd_ref_vcycle": (C.c_int, [_vp, _vp, _i32, _i32, _f64, _i32, _i32, _i32, _i32, _vp,
                                     _sz, _vp]),

@@ -68,16 +68,18 @@ __device__ __forceinline__ bool try_wait(uint64_t *bar, unsigned parity) {
   return done != 0;
 }
 
-// Wait (bounded) for phase `parity` of `bar`; warp-uniform result.  On a
-// timeout the error word is set and the wait is retried once, bounded again,
-// so that copies still in flight land before the caller moves on.
-__device__ __forceinline__ void wait(uint64_t *bar, unsigned parity, unsigned *err) {
+// Wait (bounded: `tries` attempts) for phase `parity` of `bar`, called by a
+// whole warp.  On a timeout the error word is set and the wait is retried
+// once, bounded again, so that copies still in flight land before the caller
+// moves on.  Returns whether the phase completed.
+__device__ __forceinline__ bool wait(uint64_t *bar, unsigned parity, unsigned *err,
+                                     int tries = kWaitTries) {
   bool done = false;
-  for (int k = 0; k < kWaitTries && !done; ++k) done = try_wait(bar, parity);
-  if (__all_sync(0xffffffffu, done)) return;
+  for (int k = 0; k < tries && !done; ++k) done = try_wait(bar, parity);
+  if (__all_sync(0xffffffffu, done)) return true;
   if ((threadIdx.x & 31) == 0) atomicOr(err, kErrWait);
-  for (int k = 0; k < kWaitTries && !done; ++k) done = try_wait(bar, parity);
-  __syncwarp();
+  for (int k = 0; k < tries && !done; ++k) done = try_wait(bar, parity);
+  return __all_sync(0xffffffffu, done);
 }
 
 }  // namespace bulk

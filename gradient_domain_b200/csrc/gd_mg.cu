@@ -1089,3 +1089,29 @@ extern "C" int gd_plan_kernel_times(gd_plan p, gd_kernel_time *out, int32_t n) {
   }
   return GD_OK;
 }
+
+namespace {
+// Self-test of the bounded waits of the bulk-copy rings: one warp arms an
+// mbarrier for 16 bytes that no copy will deliver and waits for it with a limit
+// of `tries` attempts.  The wait gives up, sets the error bit and returns;
+// nothing is in flight when the block exits.
+__global__ void k_wait_selftest(unsigned *err, int tries, int *completed) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) bulk::init(&bar, 1);
+  bulk::init_fence();
+  __syncwarp();
+  if (threadIdx.x == 0) bulk::arrive_expect(&bar, 16);
+  __syncwarp();
+  const bool ok = bulk::wait(&bar, 0u, err, tries);
+  if (threadIdx.x == 0) *completed = ok ? 1 : 0;
+}
+}  // namespace
+
+extern "C" int gd_selftest_bounded_wait(int32_t tries, int32_t *err, int32_t *completed,
+                                        cudaStream_t st) {
+  GD_REQUIRE(err && completed && tries >= 1 && tries <= bulk::kWaitTries, GD_ERR_ARG,
+             "gd_selftest_bounded_wait: bad arguments");
+  k_wait_selftest<<<1, 32, 0, st>>>(reinterpret_cast<unsigned *>(err), tries, completed);
+  GD_CHECK_LAUNCH();
+  return GD_OK;
+}

@@ -221,6 +221,15 @@ int gd_plan_set_profiling(gd_plan plan, int32_t enable);
 /* Per-kind totals since gd_plan_set_profiling; out has GD_KERNEL_KINDS entries. */
 int gd_plan_kernel_times(gd_plan plan, gd_kernel_time *out, int32_t n);
 
+/* Self-test of the bounded waits (no counterpart in the reference).  The
+ * streaming kernels wait for their bulk copies on mbarriers with a limit; a
+ * wait that gives up sets bit 0 of an error word (a solve then fails with
+ * GD_ERR_CUDA) instead of hanging the GPU.  This launches one warp that arms an
+ * mbarrier for 16 bytes no copy will deliver and waits with `tries` attempts
+ * (1 .. 1<<22): afterwards *err (device int32) has bit 0 set and *completed
+ * (device int32) is 0, and the context stays usable.  Nothing is allocated. */
+int gd_selftest_bounded_wait(int32_t tries, int32_t *err, int32_t *completed, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Reference-exact vertex-centred FP64 multigrid (multigrid.py:147-215), used by
  * v_cycle, multigrid.solve and solve_system("multigrid" | "cg" | "mgcg_fp64").

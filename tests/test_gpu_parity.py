@@ -527,3 +527,24 @@ def test_operators_match_golden(golden):
     np.testing.assert_array_equal(gd.divergence(golden["op_vx"], golden["op_vy"]),
                                   golden["op_div"])
     np.testing.assert_array_equal(gd.laplacian(golden["op_u"], 0.5), golden["op_lap_h05"])
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """A bulk-copy wait whose bytes never arrive gives up after its attempt limit,
+    sets the error bit and returns; the context stays usable (a solve follows)."""
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    done = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    _lib.check(_lib.lib().gd_selftest_bounded_wait(2000, _lib.ptr(err), _lib.ptr(done),
+                                                   _lib.stream_handle()),
+               "gd_selftest_bounded_wait")
+    torch.cuda.synchronize()
+    assert err.item() == 1 and done.item() == 0
+    with pytest.raises(_lib.GDError):
+        _lib.check(_lib.lib().gd_selftest_bounded_wait(0, _lib.ptr(err), _lib.ptr(done),
+                                                       _lib.stream_handle()),
+                   "gd_selftest_bounded_wait")
+    f = torch.as_tensor(np.random.default_rng(5).standard_normal((64, 64))).cuda()
+    x = torch.empty_like(f)
+    plan = PoissonPlan([Instance(64, 64, "neumann", True)], SolveParams(zero_start=True))
+    (res,) = plan.solve([f], [x], scale=-1.0)
+    assert res.converged
