@@ -29,6 +29,7 @@ using namespace gd;
 
 struct gd_plan_s {
   int n = 0;
+  int sms = 148;  // SMs of the plan's device (tile launches below one CTA per SM run wider CTAs)
   gd_params prm{};
   bool fp64 = false;
   std::vector<InstInfo> inst;
@@ -197,6 +198,10 @@ struct Runner {
                          (int)tile::DownT<T, S>::smem);
     cudaFuncSetAttribute(tile::k_up_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)tile::UpT<T, S>::smem);
+    cudaFuncSetAttribute(tile::k_down_t<T, S, tile::kThreadsSmall>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile::DownT<T, S>::smem);
+    cudaFuncSetAttribute(tile::k_up_t<T, S, tile::kThreadsSmall>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile::UpT<T, S>::smem);
     cudaFuncSetAttribute(st::k_pupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)st::pupdate_smem<T>());
     cudaFuncSetAttribute(st::k_cgupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -245,8 +250,13 @@ struct Runner {
       }
       if (p->tdown_count[l] > 0) {
         prof_begin(p, GD_K_DOWN, p->tile_cells[l], st);
-        tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
-            at_tiles(a, p->tdown_base[l]));
+        if (p->tdown_count[l] < p->sms)
+          tile::k_down_t<T, S, tile::kThreadsSmall>
+              <<<p->tdown_count[l], tile::kThreadsSmall, tile::DownT<T, S>::smem, st>>>(
+                  at_tiles(a, p->tdown_base[l]));
+        else
+          tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
+              at_tiles(a, p->tdown_base[l]));
         prof_end(p, st);
       }
     }
@@ -256,8 +266,13 @@ struct Runner {
     for (int l = p->depth - 1; l >= 0; --l) {
       if (p->tup_count[l] > 0) {
         prof_begin(p, GD_K_UP, p->tile_cells[l], st);
-        tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
-            at_tiles(a, p->tup_base[l]));
+        if (p->tup_count[l] < p->sms)
+          tile::k_up_t<T, S, tile::kThreadsSmall>
+              <<<p->tup_count[l], tile::kThreadsSmall, tile::UpT<T, S>::smem, st>>>(
+                  at_tiles(a, p->tup_base[l]));
+        else
+          tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
+              at_tiles(a, p->tup_base[l]));
         prof_end(p, st);
       }
       if (p->up_count[l] <= 0) continue;
@@ -650,6 +665,14 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   if (p->prm.check_every <= 0) p->prm.check_every = 4;
   if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-4;
   p->fp64 = params->precision == GD_FP64;
+  {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        sms > 0)
+      p->sms = sms;
+    cudaGetLastError();  // no device (CPU-only build checks): keep the default
+  }
   p->mask_set.assign(n, 0);
   build_plan(p, grids);
   if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);

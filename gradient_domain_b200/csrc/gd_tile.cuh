@@ -29,7 +29,10 @@ namespace tile {
 
 constexpr int kTY = 32, kTX = 64;  // cells of a tile (even: whole coarse cells)
 constexpr int kHX = 8;             // halo columns on each side
-constexpr int kThreads = 256;
+// Threads per CTA: 256 where a level has at least one tile per SM (throughput),
+// 1024 on smaller levels, where each phase then takes one pass per thread
+// instead of four and the CTA's chain of phases is the launch's duration.
+constexpr int kThreads = 256, kThreadsSmall = 1024;
 
 template <typename T, int S1>
 struct DownT {
@@ -88,15 +91,15 @@ __device__ __forceinline__ void store_group(T *A, const LevelInfo &L, int y, int
 // `par0` is the parity of the region corner's grid coordinates.  A cell of one
 // colour only reads cells of the other, so every thread gathers the operands
 // of all its groups before it writes: the loads of different groups overlap.
-template <typename T, int RY, int RX>
+template <typename T, int RY, int RX, int NT>
 __device__ __forceinline__ void tsweep(T *u, const T *b, const unsigned *c, const T *dinv,
                                        int colour, int par0) {
-  constexpr int GX = RX / 4, M = (RY - 2) * GX, IT = (M + kThreads - 1) / kThreads;
+  constexpr int GX = RX / 4, M = (RY - 2) * GX, IT = (M + NT - 1) / NT;
   int at[IT];
   T v0[IT], v1[IT];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
-    const int g = threadIdx.x + it * kThreads;
+    const int g = threadIdx.x + it * NT;
     at[it] = -1;
     if (g < M) {
       const int ry = 1 + g / GX, gx = g - (ry - 1) * GX;
@@ -139,8 +142,8 @@ __device__ __forceinline__ int tmirror(int f, int n, bool neu) {
 
 // Down on one tile: S1 pre-sweeps from zero, the pre-smoothed iterate to w,
 // residual, restriction (P^T) into the coarse right-hand side.
-template <typename T, int S1>
-__global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
+template <typename T, int S1, int NT = kThreads>
+__global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
   using G = DownT<T, S1>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX;
   const Tile tl = a.tiles[blockIdx.x];
@@ -159,12 +162,12 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
   const int par0 = (gy0 + gx0) & 1;
   {  // load, applying the first half sweep (colour 0 from zero: u = b / d)
     const T *B = a.arena + L.b_off;
-    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    constexpr int NG = RY * GX, IT = (NG + NT - 1) / NT;
     st::V4<T> bv[IT];
     unsigned cv[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       const int ry = g / GX, gx = g - ry * GX;
       const int y = gy0 + ry, x = gx0 + 4 * gx;
       bv[it] = g < NG ? load_group(B, L, y, x) : st::zero4<T>();
@@ -172,7 +175,7 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       if (g >= NG) break;
       const int ry = g / GX;
       const int p = (par0 + ry) & 1;  // cells j with (j & 1) == p have colour 0
@@ -186,25 +189,25 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
     }
   }
   __syncthreads();
-  tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
+  tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 1, par0);
   for (int s = 1; s < S1; ++s) {
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, par0);
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
+    tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 0, par0);
+    tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 1, par0);
   }
   {  // the pre-smoothed iterate of the tile, for the up kernel
     T *W = a.arena + L.w_off;
     constexpr int TG = kTX / 4, M = kTY * TG;
-    for (int g = threadIdx.x; g < M; g += kThreads) {
+    for (int g = threadIdx.x; g < M; g += NT) {
       const int ty = g / TG, q = g - ty * TG;
       store_group(W, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
     }
   }
   {  // residual on the tile plus one ring, in place into b (groups 1 .. kTX/4 + 2)
-    constexpr int QG = kTX / 4 + 2, M = (kTY + 2) * QG, IT = (M + kThreads - 1) / kThreads;
+    constexpr int QG = kTX / 4 + 2, M = (kTY + 2) * QG, IT = (M + NT - 1) / NT;
     st::V4<T> res[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       res[it] = st::zero4<T>();
       if (g < M) {
         const int qy = g / QG, q = g - qy * QG;
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       if (g < M) {
         const int qy = g / QG, q = g - qy * QG;
         st::st4(sb + (qy + H - 1) * RX + 4 * (q + 1), res[it]);
@@ -237,7 +240,7 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
   const bool neu = L.bc == BC_NEU;
   T *Bc = a.arena + Lc.b_off;
   constexpr int CTY = kTY / 2, CTX = kTX / 2;
-  for (int k = threadIdx.x; k < CTY * CTX; k += kThreads) {
+  for (int k = threadIdx.x; k < CTY * CTX; k += NT) {
     const int qy = k / CTX, qx = k - qy * CTX;
     const int I = (y0 >> 1) + qy, J = (x0 >> 1) + qx;
     if (I >= Lc.ny || J >= Lc.nx) continue;
@@ -261,8 +264,8 @@ __global__ void __launch_bounds__(kThreads) k_down_t(Args<T> a) {
 
 // Up on one tile: u = w + P e (bilinear; Neumann clamps at the edge, other
 // boundaries read zero outside), then S2 post-sweeps, colour 1 first.
-template <typename T, int S2>
-__global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
+template <typename T, int S2, int NT = kThreads>
+__global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
   using G = UpT<T, S2>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX, CX = G::CX;
   const Tile tl = a.tiles[blockIdx.x];
@@ -286,14 +289,14 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     const T *E = a.arena + Lc.u_off;
     const T *B = a.arena + L.b_off;
     const T *W = a.arena + L.w_off;
-    constexpr int ITC = (G::CN + kThreads - 1) / kThreads;
-    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    constexpr int ITC = (G::CN + NT - 1) / NT;
+    constexpr int NG = RY * GX, IT = (NG + NT - 1) / NT;
     T ev[ITC];
     st::V4<T> bv[IT], wv[IT];
     unsigned cv[IT];
 #pragma unroll
     for (int it = 0; it < ITC; ++it) {
-      const int k = threadIdx.x + it * kThreads;
+      const int k = threadIdx.x + it * NT;
       const int ry = k / CX, rx = k - ry * CX;
       int cy = cy0 + ry, cx = cx0 + rx;
       bool ok = k < G::CN;
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       const int ry = g / GX, gx = g - ry * GX;
       const int y = gy0 + ry, x = gx0 + 4 * gx;
       cv[it] = g < NG ? st::row_classes(L, a.codes, y, x) : 0u;
@@ -316,12 +319,12 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < ITC; ++it) {
-      const int k = threadIdx.x + it * kThreads;
+      const int k = threadIdx.x + it * NT;
       if (k < G::CN) se[k] = ev[it];
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       if (g >= NG) break;
       st::V4<T> w = wv[it];
 #pragma unroll
@@ -335,11 +338,11 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
   __syncthreads();
   {  // u += P e on cells with an unknown (each group reads the coarse values
      // and only its own u)
-    constexpr int NG = RY * GX, IT = (NG + kThreads - 1) / kThreads;
+    constexpr int NG = RY * GX, IT = (NG + NT - 1) / NT;
     st::V4<T> pe[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       pe[it] = st::zero4<T>();
       const unsigned cl = g < NG ? sc[g] : 0u;
       if (cl) {
@@ -366,7 +369,7 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
     }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
-      const int g = threadIdx.x + it * kThreads;
+      const int g = threadIdx.x + it * NT;
       if (g < NG && sc[g]) {
         st::V4<T> u = st::ld4(su + 4 * g);
 #pragma unroll
@@ -377,12 +380,12 @@ __global__ void __launch_bounds__(kThreads) k_up_t(Args<T> a) {
   }
   __syncthreads();
   for (int s = 0; s < S2; ++s) {
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 1, par0);
-    tsweep<T, RY, RX>(su, sb, sc, tdinv, 0, par0);
+    tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 1, par0);
+    tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 0, par0);
   }
   T *U = a.arena + L.u_off;
   constexpr int TG = kTX / 4, M = kTY * TG;
-  for (int g = threadIdx.x; g < M; g += kThreads) {
+  for (int g = threadIdx.x; g < M; g += NT) {
     const int ty = g / TG, q = g - ty * TG;
     store_group(U, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
   }
