@@ -810,11 +810,15 @@ bool plan_any_mean(gd_plan p) {
 
 // After the loop: the mean of zero-mean instances, then the solution into the
 // caller's buffer (mean subtracted; copied from the plan's copy where the last
-// refresh left it there).
+// refresh left it there).  Every refresh that folds a correction leaves the
+// mean of the new solution in the instance state, and a zero-start solve that
+// never folds has mean zero, so only solves that start from the caller's x
+// (which may converge on its initial residual) need the separate mean pass.
 template <typename T>
 void launch_finish(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_MEAN, p->fine_cells, st);
-  if (plan_any_mean(p)) k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+  if (plan_any_mean(p) && !p->prm.zero_start)
+    k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
   k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
   prof_end(p, st);
 }

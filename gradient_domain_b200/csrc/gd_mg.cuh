@@ -77,6 +77,8 @@ struct InstState {
   int xcur;  // where the current solution is: 0 the caller's x, 1 the plan's copy
   int refreshes;  // FP64 refreshes after the initial residual
   int xzero;      // the solution is known to be zero (zero-start solve, nothing folded yet)
+  int mean_known; // mean holds the solution's mean (set by a refresh that folds)
+  int pad;
 };
 
 struct Tile {

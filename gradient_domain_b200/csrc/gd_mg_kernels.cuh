@@ -364,7 +364,8 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
-  if (I.zero_mean && !a.st[tl.inst].xzero) {  // a zero solution has mean zero
+  // only solutions no refresh has summed: a caller's x that met the tolerance at once
+  if (I.zero_mean && !a.st[tl.inst].mean_known) {
     const bool own = a.st[tl.inst].xcur != 0;
     const double *X = own ? a.xs + I.xs_off : I.x;
     const long long pitch = own ? (long long)I.pitch : I.upitch;
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const int warp = threadIdx.x >> 5;
   for (int i = warp; i < a.ninst; i += kLastWarps) {
     const InstInfo &J = a.inst[i];
-    if (!J.zero_mean) continue;
+    if (!J.zero_mean || a.st[i].mean_known) continue;
     const double s = warp_range_sum(a.part0, J.fine_begin, J.fine_end);
     if ((threadIdx.x & 31) == 0) a.st[i].mean = s / ((double)J.ny * (double)J.nx);
   }

@@ -1319,6 +1319,7 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
       for (int j = 0; j < 4; ++j) rv.v[j] = (T)res[j];
       if (FAST || nv > 0) st4(w.R + (long long)p * w.pitch + x0, rv);
       if constexpr (FOLD) {
+        part_f += (xc[0] + xc[1]) + (xc[2] + xc[3]);  // the solution's sum, for its mean
         double *drow = w.dst + p * w.dpitch + x0;
         if (FAST || (nv == 4 && (reinterpret_cast<uintptr_t>(drow) & 15) == 0)) {
           *reinterpret_cast<double2 *>(drow) = make_double2(xc[0], xc[1]);
@@ -1403,14 +1404,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
       }
     }
     part = block_sum<kThreads>(part);
-    if (INIT) {
-      __syncthreads();
-      part_f = block_sum<kThreads>(part_f);
-    }
+    __syncthreads();
+    part_f = block_sum<kThreads>(part_f);
   }
   if (threadIdx.x == 0) {
     a.part0[blockIdx.x] = part;
-    if (INIT) a.part1[blockIdx.x] = part_f;
+    a.part1[blockIdx.x] = part_f;  // INIT: ||f||^2; a refresh that folds: the sum of x + d
   }
   if (!last_block(a.counter + 2)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1421,11 +1420,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
     const bool part_of = INIT || (S.flags & FLAG_RU);
     if (part_of) {
       const double rr = warp_range_sum(a.part0, I.fine_begin, I.fine_end);
-      double ff = 0.0;
-      if (INIT) ff = warp_range_sum(a.part1, I.fine_begin, I.fine_end);
+      const double p1 = warp_range_sum(a.part1, I.fine_begin, I.fine_end);
       if (lane == 0) {
         if (INIT) {
-          S.ff = ff;
+          S.ff = p1;
+          S.mean = 0.0;
+          S.mean_known = a.zero_start;  // a zero start has mean zero
           S.iters = 0;
           S.first = 1;
           S.rz = 0.0;
@@ -1440,6 +1440,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
           if (!(S.flags & FLAG_DZERO)) {
             S.xcur ^= 1;  // x + d went to the other copy
             S.xzero = 0;
+            S.mean = p1 / ((double)I.ny * (double)I.nx);  // of the new solution
+            S.mean_known = 1;
           }
         }
         // A refresh that barely lowers the true residual (less than 3x), once
