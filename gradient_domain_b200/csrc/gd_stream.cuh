@@ -1346,6 +1346,60 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
   __pipeline_wait_prior(0);  // no copy may land after the shared memory is released
 }
 
+// Initial residual of a zero-start solve: with x = 0, r = scale (f - fmean)
+// where there is an unknown, no stencil, and ||r||^2 = ||f'||^2.  Element-wise
+// over the warp's rows with four rows' loads in flight per thread.
+template <typename T>
+__device__ __forceinline__ void init_zero_rows(const RefWarp<T> &w, double &part,
+                                               double &part_f) {
+  const int x0 = w.x0, nv = w.nv;
+  if (nv <= 0) return;
+  constexpr int K = 4;
+  for (int yb = w.y0; yb < w.y1; yb += K) {
+    double fv[K][4];
+    unsigned cw[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int y = yb + k;
+      cw[k] = 0u;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) fv[k][j] = 0.0;
+      if (y < w.y1) {
+        const double *row = w.F + y * w.upitch + x0;
+        if (nv == 4 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+          const double2 a0 = *reinterpret_cast<const double2 *>(row);
+          const double2 a1 = *reinterpret_cast<const double2 *>(row + 2);
+          fv[k][0] = a0.x; fv[k][1] = a0.y; fv[k][2] = a1.x; fv[k][3] = a1.y;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (j < nv) fv[k][j] = row[j];
+        }
+        if (w.masked)
+          cw[k] = *reinterpret_cast<const unsigned *>(w.codes + (long long)y * w.pitch + x0);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int y = yb + k;
+      if (y >= w.y1) break;
+      V4<T> rv;
+      double fq[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool on = j < nv && (!w.masked || ((cw[k] >> (8 * j)) & 0xffu) != 0u);
+        fq[j] = on ? w.scale * (fv[k][j] - w.fmean) : 0.0;
+        rv.v[j] = (T)fq[j];
+      }
+      // grouped as the stencil path groups its squares, so both give the same bits
+      const double sq = (fq[0] * fq[0] + fq[1] * fq[1]) + (fq[2] * fq[2] + fq[3] * fq[3]);
+      part += sq;
+      part_f += sq;
+      st4(w.R + (long long)y * w.pitch + x0, rv);
+    }
+  }
+}
+
 template <typename T, bool INIT>
 __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
@@ -1393,7 +1447,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
                          15) == 0 &&
                         (w.upitch & 1) == 0;
       if constexpr (INIT) {
-        if (fast) refresh_strip<T, true, false, true>(w, smem, err, part, part_f);
+        if (w.xz) init_zero_rows<T>(w, part, part_f);
+        else if (fast) refresh_strip<T, true, false, true>(w, smem, err, part, part_f);
         else refresh_strip<T, true, false, false>(w, smem, err, part, part_f);
       } else if (!(flags & FLAG_DZERO)) {
         if (fast) refresh_strip<T, false, true, true>(w, smem, err, part, part_f);
