@@ -46,8 +46,8 @@ BYTES_PER_CELL_MIXED = {
     "pupdate": 4 + 4 + 4,                   # read z, p; write p
     "cgupdate": 12 + 8,                     # read p, d, r; write d, r
     "resid": 8 + 4 + 8 + 8 + 4,             # read x, d, f; write x + d, r (refresh iterations)
-    "init": 8 + 8 + 8 + 4,                  # read f twice, x; write r
-    "mean": 8 + 16,                         # read x; read+write x
+    "init": 8 + 8 + 4,                      # read f twice (its mean, then r); write r; x = 0
+    "mean": 8 + 8,                          # read the solution; write x, mean subtracted
 }
 
 

@@ -1348,13 +1348,13 @@ __device__ __forceinline__ void refresh_strip(const RefWarp<T> &w, unsigned char
 
 // Initial residual of a zero-start solve: with x = 0, r = scale (f - fmean)
 // where there is an unknown, no stencil, and ||r||^2 = ||f'||^2.  Element-wise
-// over the warp's rows with four rows' loads in flight per thread.
+// over the warp's rows with eight rows' loads in flight per thread.
 template <typename T>
 __device__ __forceinline__ void init_zero_rows(const RefWarp<T> &w, double &part,
                                                double &part_f) {
   const int x0 = w.x0, nv = w.nv;
   if (nv <= 0) return;
-  constexpr int K = 4;
+  constexpr int K = 8;
   for (int yb = w.y0; yb < w.y1; yb += K) {
     double fv[K][4];
     unsigned cw[K];
