@@ -400,6 +400,8 @@ def ours(args) -> None:
     refreshes = max(r.refreshes for r in results)
     launches = args.steps * (2 + 1 + max(its) * (per_iter + 2) + refreshes + 1)
 
+    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
+
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -417,6 +419,7 @@ def ours(args) -> None:
         "iterations": its, "relative_residual": resid, "converged": converged,
         "port_equivalent_fp64": port,
         "dct_neumann": dct,
+        "smoother": smoother,
         "fp64_mgpcg": {"value": value64, "ms_per_step": ms64,
                        "iterations": [r.iterations for r in r64],
                        "mixed_over_fp64": value / value64},
@@ -435,6 +438,57 @@ def ours(args) -> None:
         print(json.dumps(line), flush=True)
     plan.close()
     replicas.finish(world)
+
+
+def smoother_gate(n: int, hbm: float, kinds: dict, sweeps: int, reps: int = 20) -> dict:
+    """The smoother against HBM: ``gd_rbgs_smooth`` (FP32, red-black Gauss-Seidel,
+    multigrid.py:147-165) on an n x n grid, 1 and 2 sweeps per launch.  A launch reads u
+    and b and writes the result once, 12 B/cell whatever the sweeps, so the sweep rate is
+    12 k B/cell per launch time.  The fused level-0 V-cycle kernels run `sweeps` sweeps
+    each inside the solve; their sweep rate is given the same way."""
+    import torch
+
+    from gradient_domain_b200 import _lib
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(7)
+    u = torch.randn((n, n), device=dev, generator=g)
+    b = torch.randn((n, n), device=dev, generator=g)
+    v = torch.empty_like(u)
+    stream = torch.cuda.current_stream()
+    fn, sh = _lib.lib().gd_rbgs_smooth, stream.cuda_stream
+
+    def launch(i, k):
+        src, dst = (u, v) if i % 2 == 0 else (v, u)
+        _lib.check(fn(src.data_ptr(), dst.data_ptr(), b.data_ptr(), n, n, n, 0, 1.0, k, sh),
+                   "gd_rbgs_smooth")
+
+    out = {"kernel": "k_rbgs<float>", "grid": f"{n}x{n}", "bytes_per_cell": 12,
+           "l2": "u, b and the result: 3 x 67 MB per launch, above the 126 MB L2"}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in (1, 2):
+        for i in range(4):
+            launch(i, k)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(reps):
+            launch(i, k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = 12 * n * n / (ms / 1e3) / 1e9
+        out[f"sweeps_{k}"] = {"ms": ms, "achieved_gbs": gbs, "frac": gbs / hbm,
+                              "sweep_gbs": k * gbs, "sweep_frac": k * gbs / hbm}
+    fused = {}
+    for kind in ("down0", "up0"):
+        d = kinds.get(kind)
+        if d and d["launches"]:
+            t = d["ms"] / d["launches"] / 1e3
+            cells_l = d["cells"] / d["launches"]
+            fused[kind] = {"sweeps": sweeps, "sweep_gbs": 12 * sweeps * cells_l / t / 1e9,
+                           "sweep_frac": 12 * sweeps * cells_l / t / 1e9 / hbm}
+    out["fused_level0"] = fused
+    return out
 
 
 def _timed_steps(step, steps, warmup, world, dev):
@@ -501,6 +555,8 @@ def composite(args) -> None:
     for _ in range(e2e_steps):
         out, reps = gd.seamless_clone(src, tgt, mask, (0, 0), domain="mask", tolerance=args.tol)
     e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
+    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
+
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -574,6 +630,8 @@ def batch(args) -> None:
     ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
     value = replicas.aggregate_rate(cells, world, ms / 1e3) / 1e6
     its = [r.iterations for r in res]
+    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
+
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -610,7 +668,7 @@ def main():
     ap.add_argument("--solve-only", action="store_true",
                     help="only the mixed-precision solves (small profiling runs): no FP64 plan, "
                          "no end-to-end leg, no oracle")
-    ap.add_argument("--config", choices=["tonemap", "composite", "batch", "serve"],
+    ap.add_argument("--config", choices=["tonemap", "composite", "batch", "serve", "smoother"],
                     default="tonemap", help="workload (default: the headline tone-mapping case)")
     ap.add_argument("--count", type=int, default=256, help="images in the batch workload")
     ap.add_argument("--rates", type=float, nargs="+", default=[200.0, 1000.0, 5000.0],
@@ -626,6 +684,13 @@ def main():
         composite(args)
     elif args.config == "batch":
         batch(args)
+    elif args.config == "smoother":
+        import torch
+        torch.cuda.set_device(0)
+        hbm, peak_kind = peaks()
+        line = smoother_gate(args.size, hbm, {}, args.sweeps, reps=max(args.steps, 1))
+        line["peak_source"] = peak_kind
+        print(json.dumps({"smoother": line}), flush=True)
     elif args.config == "serve":
         from gradient_domain_b200 import serving
         serving.bench_main(args)

@@ -9,7 +9,7 @@ running in hand-written sm_100a CUDA kernels behind the C ABI of
 
 from .benchmark import BenchmarkRecord, BenchmarkTable, manufactured_problem, solver_scaling
 from .hdr import ToneMapConfig, attenuation_field, tone_map
-from .multigrid import MultigridOptions, MultigridReport, solve, v_cycle
+from .multigrid import MultigridOptions, MultigridReport, smooth, solve, v_cycle
 from .operators import divergence, fold_boundary, gradient, laplacian, sparse_laplacian
 from .plan import Instance, PoissonPlan, SolveParams, cached_plan
 from .poisson import (
@@ -29,7 +29,7 @@ __all__ = [
     "gradient", "illumination_change", "laplacian", "manufactured_problem", "seamless_clone",
     "solve", "solve_dirichlet", "solve_masked", "solve_neumann", "solve_neumann_batch",
     "solve_system",
-    "solver_scaling", "sparse_laplacian", "texture_flatten", "tone_map", "v_cycle",
+    "smooth", "solver_scaling", "sparse_laplacian", "texture_flatten", "tone_map", "v_cycle",
 ]
 
 __version__ = "0.1.0"

@@ -96,6 +96,46 @@ def _to_dev(a, dev) -> torch.Tensor:
     return upload(a, dev, np.float64)
 
 
+def smooth(u, b, spacing: float = 1.0, sweeps: int = 1):
+    """``sweeps`` red-black Gauss-Seidel sweeps on ``laplacian(u) = b`` (multigrid.py:147-165).
+
+    Returns a new array (NumPy in, NumPy out; a CUDA tensor in, a CUDA tensor
+    out); ``u`` is not changed.  float64 gives the reference's ``_smooth``
+    bitwise; when ``u`` and ``b`` are both float32 the sweeps run in float32,
+    bitwise the same expression evaluated in float32.  Each device pass
+    (``gd_rbgs_smooth``) runs up to four sweeps, reading u and b once.
+    """
+    dev = _lib.device()
+    as_tensor = isinstance(u, torch.Tensor)
+    fp32 = all((x.dtype == torch.float32) if isinstance(x, torch.Tensor)
+               else (np.asarray(x).dtype == np.float32) for x in (u, b))
+    dtype = torch.float32 if fp32 else torch.float64
+
+    def to_dev(x):
+        if isinstance(x, torch.Tensor):
+            return x.to(device=dev, dtype=dtype).contiguous()
+        return upload(np.asarray(x), dev, np.float32 if fp32 else np.float64)
+
+    u_d, b_d = to_dev(u), to_dev(b)
+    if u_d.dim() != 2 or u_d.shape != b_d.shape:
+        raise ValueError("u and b must be 2-D arrays of the same shape")
+    ny, nx = u_d.shape
+    if sweeps <= 0 or u_d.numel() == 0:
+        out = u_d.clone()
+    else:
+        out, spare = torch.empty_like(u_d), torch.empty_like(u_d)
+        src, left = u_d, int(sweeps)
+        while left > 0:
+            k = min(4, left)
+            dst = out if src is not out else spare
+            _lib.check(_lib.lib().gd_rbgs_smooth(_lib.ptr(src), _lib.ptr(dst), _lib.ptr(b_d), ny,
+                                                 nx, nx, 0 if fp32 else 1, float(spacing), k,
+                                                 _lib.stream_handle()), "gd_rbgs_smooth")
+            src, left = dst, left - k
+        out = src
+    return out if as_tensor else download(out)
+
+
 def v_cycle(u, b, spacing: float, options: MultigridOptions) -> np.ndarray:
     """One V-cycle on ``laplacian(u) = b`` (multigrid.py:184-215); returns a new array."""
     dev = _lib.device()

@@ -263,6 +263,19 @@ int gd_ref_vcycle_static(double *u_dev, const double *b_dev, int32_t m, int32_t 
                          double spacing, int32_t pre, int32_t post, int32_t coarsest_size,
                          int32_t coarsest_sweeps, cudaStream_t stream);
 
+/* out <- sweeps (1-4) red-black Gauss-Seidel sweeps of multigrid._smooth
+ * (multigrid.py:147-165) on laplacian(u) = b with zeros outside the array:
+ * cells with (i + j) % 2 == 0 first, each u = 0.25 * (((up + down) + left) +
+ * right - spacing^2 b).  One temporally blocked pass: u and b are read once
+ * and out written once, whatever the number of sweeps.  fp64 = 1: double
+ * arrays, bitwise the reference's result; fp64 = 0: float arrays, bitwise the
+ * same expression evaluated in float32.  All three arrays are ny x nx with row
+ * pitch `pitch` elements; out must not overlap u or b (u and b may be the same
+ * array).  More sweeps: call again with u and out exchanged. */
+int gd_rbgs_smooth(const void *u_dev, void *out_dev, const void *b_dev, int32_t ny, int32_t nx,
+                   int32_t pitch, int32_t fp64, double spacing, int32_t sweeps,
+                   cudaStream_t stream);
+
 /* r <- b - laplacian(u, spacing) (multigrid.py:210, operators.py:86-107). */
 int gd_ref_residual(double *r_dev, const double *u_dev, const double *b_dev, int32_t m,
                     int32_t n, double spacing, cudaStream_t stream);

@@ -59,6 +59,19 @@ def main(reference_root: str) -> None:
     out["tr_restrict"] = multigrid._restrict(fine)
     out["tr_prolong"] = multigrid._prolong(coarse, (31, 25))
 
+    # red-black Gauss-Seidel sweeps (multigrid.py:147-165), from float64 and float32 arrays
+    for name, shape, sweeps, spacing in (("sm37x53", (37, 53), 1, 1.0),
+                                         ("sm37x53s3", (37, 53), 3, 0.5),
+                                         ("sm5x131", (5, 131), 2, 1.0),
+                                         ("sm70x260s6", (70, 260), 6, 0.75)):
+        rng = np.random.default_rng(sum(shape) + sweeps)
+        u0, b = rng.standard_normal(shape), rng.standard_normal(shape)
+        out[f"{name}_u0"], out[f"{name}_b"] = u0, b
+        out[f"{name}_opts"] = np.array([sweeps, spacing])
+        out[f"{name}_f64"] = multigrid._smooth(u0, b, spacing, sweeps)
+        out[f"{name}_f32"] = multigrid._smooth(u0.astype(np.float32), b.astype(np.float32),
+                                               spacing, sweeps)
+
     # multigrid.solve history (multigrid.py:218-255)
     b, _ = manufactured_problem((63, 63), seed=5)
     sol, rep = multigrid.solve(b, options=multigrid.MultigridOptions(tolerance=1e-10))

@@ -53,6 +53,20 @@ def test_v_cycle_matches_golden(golden, name):
         assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
 
 
+SMOOTH_CASES = ["sm37x53", "sm37x53s3", "sm5x131", "sm70x260s6"]
+
+
+@pytest.mark.parametrize("name", SMOOTH_CASES)
+def test_smooth_matches_golden_bitwise(golden, name):
+    sweeps, h = golden[f"{name}_opts"]
+    u0, b = golden[f"{name}_u0"], golden[f"{name}_b"]
+    got64 = multigrid.smooth(u0, b, float(h), int(sweeps))
+    got32 = multigrid.smooth(u0.astype(np.float32), b.astype(np.float32), float(h), int(sweeps))
+    assert got32.dtype == np.float32
+    np.testing.assert_array_equal(got64, golden[f"{name}_f64"])
+    np.testing.assert_array_equal(got32, golden[f"{name}_f32"])
+
+
 def test_transfers_match_golden(golden):
     np.testing.assert_allclose(multigrid.restrict(golden["tr_fine"]), golden["tr_restrict"],
                                rtol=0, atol=1e-14)
