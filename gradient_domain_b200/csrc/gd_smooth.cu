@@ -103,6 +103,17 @@ __device__ __forceinline__ Q4<T> load4(const T *A, const SmoothArgs<T> &a, int y
 template <int J0, typename T>
 __device__ __forceinline__ void half_row(Q4<T> &u, const Q4<T> &nb1, const Q4<T> &nb2,
                                          const T *bq, T h2, unsigned inside) {
+  // one 16-byte read per lane (FP32; two for FP64): a warp reads 512 contiguous
+  // bytes without bank conflicts, where scalar reads at a 16-byte stride conflict 4-way
+  T bv[4];
+  if (sizeof(T) == 4) {
+    const float4 t = *reinterpret_cast<const float4 *>(bq);
+    bv[0] = (T)t.x; bv[1] = (T)t.y; bv[2] = (T)t.z; bv[3] = (T)t.w;
+  } else {
+    const double2 t0 = reinterpret_cast<const double2 *>(bq)[0];
+    const double2 t1 = reinterpret_cast<const double2 *>(bq)[1];
+    bv[0] = (T)t0.x; bv[1] = (T)t0.y; bv[2] = (T)t1.x; bv[3] = (T)t1.y;
+  }
   T side;
   if (J0 == 0) side = __shfl_up_sync(0xffffffffu, u.v[3], 1);  // column x0 - 1
   else side = __shfl_down_sync(0xffffffffu, u.v[0], 1);        // column x0 + 4
@@ -112,7 +123,7 @@ __device__ __forceinline__ void half_row(Q4<T> &u, const Q4<T> &nb1, const Q4<T>
     const T right = j == 3 ? side : u.v[j + 1];
     // ((up + down) + left) + right; up + down commutes exactly, whichever walk direction
     const T s = add_rn(add_rn(add_rn(nb1.v[j], nb2.v[j]), left), right);
-    const T v = mul_rn(T(0.25), sub_rn(s, mul_rn(h2, bq[j])));
+    const T v = mul_rn(T(0.25), sub_rn(s, mul_rn(h2, bv[j])));
     if (inside & (1u << j)) u.v[j] = v;
   }
 }
@@ -135,7 +146,9 @@ __device__ __forceinline__ constexpr int sl(int ph, int k) {
 }
 
 // Rows of prefetch in registers: U for FP32, 2 for FP64 (both divide the even U).
-// (Eight rows for one FP32 sweep need 157 registers, or spill at 128.)
+// (Measured alternatives for one FP32 sweep on 4096^2: eight rows need 157
+// registers, or spill at 128; a per-lane cp.async ring in shared memory with five
+// rows in flight at 59 registers was 3-7 % slower.)
 template <typename T, int S>
 struct SmPrefetch {
   static constexpr int P = sizeof(T) == 4 ? SmGeom<S>::U : 2;
@@ -243,14 +256,20 @@ __global__ void __launch_bounds__(kSmThreads) k_rbgs(SmoothArgs<T> a) {
   }
 }
 
-// Resident CTAs per SM of one kernel instance, looked up once.
-template <typename T, int S, bool VEC>
+// Kernel kinds: 0 scalar global accesses, 1 vector accesses (16-byte aligned rows).
+template <typename T, int S, int KIND>
+constexpr auto kernel_of() {
+  return &k_rbgs<T, S, KIND == 1>;
+}
+
+// Resident CTAs per SM of one kernel, looked up once.
+template <typename T, int S, int KIND>
 int resident_ctas() {
   static std::atomic<int> cached{0};
   int v = cached.load(std::memory_order_relaxed);
   if (v > 0) return v;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_rbgs<T, S, VEC>, kSmThreads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of<T, S, KIND>(), kSmThreads, 0) !=
           cudaSuccess ||
       n <= 0)
     n = 1;
@@ -258,14 +277,14 @@ int resident_ctas() {
   return n;
 }
 
-template <typename T, int S, bool VEC>
+template <typename T, int S, int KIND>
 int launch_rbgs(const T *u, T *out, const T *b, int ny, int nx, int pitch, double spacing,
                 cudaStream_t st) {
   using G = SmGeom<S>;
   int dev = 0, sms = 0;
   GD_CHECK_CUDA(cudaGetDevice(&dev));
   GD_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int ctas = resident_ctas<T, S, VEC>() * sms;
+  const int ctas = resident_ctas<T, S, KIND>() * sms;
   SmoothArgs<T> a;
   a.u = u;
   a.out = out;
@@ -286,7 +305,7 @@ int launch_rbgs(const T *u, T *out, const T *b, int ny, int nx, int pitch, doubl
   GD_REQUIRE(items < (1ll << 30), GD_ERR_ARG, "gd_rbgs_smooth: grid too large");
   a.items = (int)items;
   const int grid = (int)std::min<long long>(ceil_div(a.items, kSmThreads / 32), ctas);
-  k_rbgs<T, S, VEC><<<grid, kSmThreads, 0, st>>>(a);
+  kernel_of<T, S, KIND>()<<<grid, kSmThreads, 0, st>>>(a);
   GD_CHECK_LAUNCH();
   return GD_OK;
 }
@@ -298,10 +317,10 @@ int dispatch(const T *u, T *out, const T *b, int ny, int nx, int pitch, double s
                    (reinterpret_cast<uintptr_t>(b) & 15) == 0 &&
                    (reinterpret_cast<uintptr_t>(out) & 15) == 0 &&
                    ((size_t)pitch * sizeof(T)) % 16 == 0;
-#define GD_RBGS_CASE(S)                                                               \
-  case S:                                                                             \
-    return vec ? launch_rbgs<T, S, true>(u, out, b, ny, nx, pitch, spacing, st)      \
-               : launch_rbgs<T, S, false>(u, out, b, ny, nx, pitch, spacing, st);
+#define GD_RBGS_CASE(S)                                                           \
+  case S:                                                                         \
+    return vec ? launch_rbgs<T, S, 1>(u, out, b, ny, nx, pitch, spacing, st)      \
+               : launch_rbgs<T, S, 0>(u, out, b, ny, nx, pitch, spacing, st);
   switch (sweeps) {
     GD_RBGS_CASE(1)
     GD_RBGS_CASE(2)
