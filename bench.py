@@ -140,9 +140,15 @@ def cpu_baseline_tonemap(rhs: np.ndarray, budget_s: float = 20.0) -> dict:
         osolvers.solve_neumann(rhs[done], workers=cores)
         done += 1
     dt = time.perf_counter() - t0
+    # the same solve on one core (one fft worker; the NumPy steps are single-threaded)
+    t1 = time.perf_counter()
+    osolvers.solve_neumann(rhs[0], workers=1)
+    dt1 = time.perf_counter() - t1
     return {"value": done * h * w / dt / 1e6, "unit": "Mpix/s", "cores": cores, "kind": "port",
             "sample": f"{done} of {n_ch} channels of {h}x{w}, scipy DCT solve_neumann "
-                      f"restatement, {cores} fft workers, {dt:.2f} s"}
+                      f"restatement, {cores} fft workers, {dt:.2f} s",
+            "single_core": {"value": h * w / dt1 / 1e6, "unit": "Mpix/s", "cores": 1,
+                            "sample": f"1 channel of {h}x{w}, 1 fft worker, {dt1:.2f} s"}}
 
 
 def reference_arm(args) -> None:
