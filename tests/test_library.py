@@ -36,3 +36,19 @@ def test_no_gpu_means_loud_failure(monkeypatch):
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     with pytest.raises(_lib.GDError):
         _lib.device()
+
+
+def test_smoother_argument_checks_run_on_the_host():
+    """gd_rbgs_smooth rejects bad arguments before touching a device (dummy, never
+    dereferenced pointers: every call below fails its checks first)."""
+    fn = _lib.lib().gd_rbgs_smooth
+    u, out, b = 256, 512, 768
+    assert fn(None, out, b, 8, 8, 8, 0, 1.0, 1, None) == -1
+    assert fn(u, u, b, 8, 8, 8, 0, 1.0, 1, None) == -1           # out is u
+    assert fn(u, b, b, 8, 8, 8, 0, 1.0, 1, None) == -1           # out is b
+    assert fn(u, out, b, 8, 8, 7, 0, 1.0, 1, None) == -1         # pitch below the width
+    assert fn(u, out, b, 0, 8, 8, 0, 1.0, 1, None) == -1
+    assert fn(u, out, b, 8, 8, 8, 3, 1.0, 1, None) == -1         # element type flag
+    for sweeps in (0, 5, -1):
+        assert fn(u, out, b, 8, 8, 8, 0, 1.0, sweeps, None) == -1
+        assert b"sweeps" in _lib.lib().gd_last_error()
