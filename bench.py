@@ -497,6 +497,35 @@ def smoother_gate(n: int, hbm: float, kinds: dict, sweeps: int, reps: int = 20) 
     return out
 
 
+def autotune_main(args) -> None:
+    """Tune the headline plan (size x size x channels Neumann) from its defaults on its own
+    right-hand sides, into a cache file of its own, and print the search."""
+    import tempfile
+
+    import torch
+
+    from gradient_domain_b200 import autotune, workloads
+    from gradient_domain_b200.plan import Instance, SolveParams
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rhs_np = workloads.tonemap_rhs(args.size, seed=1, channels=args.channels)
+    rhs = [torch.as_tensor(r).to(dev) for r in rhs_np]
+    insts = [Instance(args.size, args.size, "neumann", True) for _ in range(len(rhs))]
+    params = SolveParams(tolerance=args.tol, sweeps=args.sweeps, reliable_delta=args.delta)
+    path = os.path.join(tempfile.mkdtemp(), "autotune.json")
+    t0 = time.perf_counter()
+    tuned = autotune.tune(insts, params, rhs=rhs, reps=max(args.steps, 3), path=path,
+                          force=True, scale=-1.0)
+    with open(path) as fh:
+        entry = json.load(fh)[autotune.tune_key(insts, params)]
+    print(json.dumps({"autotune": {
+        "workload": f"tonemap-neumann {args.size}x{args.size}x{len(rhs)}", "key":
+        autotune.tune_key(insts, params), "default_ms": entry["default_ms"], "tuned_ms": entry["ms"],
+        "choice": {k: getattr(tuned, k) for k, _ in autotune.SPACE}, "trials": entry["trials"],
+        "seconds": time.perf_counter() - t0}}), flush=True)
+
+
 def _timed_steps(step, steps, warmup, world, dev):
     """Warm up, then device-time exactly `steps` calls of step() (max over ranks)."""
     import torch
@@ -674,7 +703,8 @@ def main():
     ap.add_argument("--solve-only", action="store_true",
                     help="only the mixed-precision solves (small profiling runs): no FP64 plan, "
                          "no end-to-end leg, no oracle")
-    ap.add_argument("--config", choices=["tonemap", "composite", "batch", "serve", "smoother"],
+    ap.add_argument("--config", choices=["tonemap", "composite", "batch", "serve", "smoother",
+                                         "autotune"],
                     default="tonemap", help="workload (default: the headline tone-mapping case)")
     ap.add_argument("--count", type=int, default=256, help="images in the batch workload")
     ap.add_argument("--rates", type=float, nargs="+", default=[200.0, 1000.0, 5000.0],
@@ -690,6 +720,8 @@ def main():
         composite(args)
     elif args.config == "batch":
         batch(args)
+    elif args.config == "autotune":
+        autotune_main(args)
     elif args.config == "smoother":
         import torch
         torch.cuda.set_device(0)
