@@ -20,7 +20,9 @@ winner is cached under :func:`tune_key` - boundary types, level-0 size bucket
 (powers of two of cells), instance-count bucket and precision - in memory and
 in a JSON file (``$GD_AUTOTUNE_CACHE``, default
 ``~/.cache/gradient_domain_b200/autotune.json``); :func:`lookup` returns the
-cached parameters for a plan without timing anything.
+cached parameters for a plan without timing anything, and :func:`resolve` -
+which the plan cache, the pipelined batch solves and the serving workers call -
+applies them to the fields a caller left at their defaults.
 
 Tuned parameters change the arithmetic (sweeps, which levels run on which
 kernel kind), never the stopping rule: every candidate solve has to converge
@@ -85,6 +87,7 @@ def _load(path: str) -> dict:
 
 
 def _store(path: str, key: str, entry: dict) -> None:
+    _MEMORY[(path, key)] = entry
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     data = _load(path)
     data[key] = entry
@@ -109,12 +112,31 @@ def lookup(instances: Sequence[Instance], params: SolveParams | None = None,
     key = tune_key(instances, params)
     path = path or cache_path()
     with _CACHE_LOCK:
-        entry = _MEMORY.get((path, key)) if (path, key) in _MEMORY else _load(path).get(key)
-        if entry is not None:
+        if (path, key) in _MEMORY:
+            entry = _MEMORY[(path, key)]
+        else:  # read the file once per key; an untuned key is remembered as such
+            entry = _load(path).get(key) or {}
             _MEMORY[(path, key)] = entry
     if not entry:
         return params
     return _apply(params, entry.get("choice", {}))
+
+
+def resolve(instances: Sequence[Instance], params: SolveParams | None = None,
+            path: str | None = None) -> SolveParams:
+    """The parameters a plan for ``instances`` is built with: the cached tuned values
+    applied to the fields that ``params`` leaves at their defaults (an explicit choice of
+    the caller, e.g. ``sweeps=3``, is kept); ``params`` itself if the key was never tuned."""
+    params = params or SolveParams()
+    tuned = lookup(instances, params, path)
+    if tuned == params:
+        return params
+    default = SolveParams()
+    over = {name: getattr(tuned, name) for name, _ in SPACE
+            if getattr(params, name) == getattr(default, name)}
+    if params.precision == default.precision:
+        over["precision"] = tuned.precision
+    return replace(params, **over)
 
 
 def coordinate_descent(evaluate: Callable[[dict], float], start: dict,
@@ -261,7 +283,6 @@ def tune(instances: Sequence[Instance], params: SolveParams | None = None,
              "trials": len(history), "seconds": time.perf_counter() - t0,
              "device": torch.cuda.get_device_name(dev)}
     with _CACHE_LOCK:
-        _MEMORY[(path, key)] = entry
         _store(path, key, entry)
     return _apply(params, best)
 

@@ -229,7 +229,11 @@ CACHE_LIMIT = 32
 
 
 def cached_plan(instances: tuple[Instance, ...], params: SolveParams) -> PoissonPlan:
-    """A plan for this exact instance list, kept resident for reuse (LRU)."""
+    """A plan for this exact instance list, kept resident for reuse (LRU), built with the
+    autotuner's cached parameters for its shape class where the caller left defaults."""
+    from .autotune import resolve
+
+    params = resolve(instances, params)
     key = (instances, params)
     with _CACHE_LOCK:
         plan = _CACHE.get(key)

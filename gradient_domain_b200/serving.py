@@ -117,8 +117,9 @@ class _CachedPlan:
     """A plan and the device buffers of its right-hand sides and solutions."""
 
     def __init__(self, torch, device, insts, params, stream):
+        from .autotune import resolve
         from .plan import PoissonPlan
-        self.plan = PoissonPlan(insts, params, stream=stream)
+        self.plan = PoissonPlan(insts, resolve(insts, params), stream=stream)
         self.f = [torch.empty((i.height, i.width), dtype=torch.float64, device=device)
                   for i in insts]
         self.x = [torch.empty_like(t) for t in self.f]

@@ -42,6 +42,7 @@ import torch
 
 from . import _lib
 from ._host import download, upload
+from .autotune import resolve
 from .multigrid import MultigridOptions, RefWorkspace
 from .plan import Instance, PoissonPlan, SolveParams, cached_plan
 
@@ -382,10 +383,12 @@ def _take_pipeline(h: int, w: int, params: SolveParams, n: int):
         return key, pipe
     dev = _lib.device()
     pipe = []
+    inst = Instance(h, w, "neumann", True)
+    params = resolve([inst], params)
     for _ in range(n):
         stream = torch.cuda.Stream(dev)
         with torch.cuda.stream(stream):
-            plan = PoissonPlan([Instance(h, w, "neumann", True)], params, stream=stream)
+            plan = PoissonPlan([inst], params, stream=stream)
             f = torch.empty((h, w), dtype=torch.float64, device=dev)
             x = torch.empty_like(f)
         pipe.append((plan, stream, f, x))

@@ -76,3 +76,30 @@ def test_a_tuned_precision_is_applied():
     got = autotune._apply(SolveParams(), {"sweeps": 1, "precision": "fp64"})
     assert got.precision == "fp64" and got.sweeps == 1
     assert autotune._apply(SolveParams(), {"precision": "bogus"}).precision == "mixed"
+
+
+def test_resolve_applies_tuned_values_only_where_the_caller_kept_defaults(tmp_path):
+    path = str(tmp_path / "tune.json")
+    insts = [Instance(256, 256, "neumann", True)]
+    assert autotune.resolve(insts, SolveParams(), path) == SolveParams()   # nothing tuned
+    key = autotune.tune_key(insts, SolveParams())
+    choice = {"sweeps": 3, "strip_target_warps": 900, "tile_cells": 65536, "bottom_cells": 1024,
+              "precision": "fp64"}
+    autotune._store(path, key, {"choice": choice, "ms": 1.0, "default_ms": 1.1})
+    got = autotune.resolve(insts, SolveParams(tolerance=1e-6, zero_start=True), path)
+    assert (got.sweeps, got.strip_target_warps, got.tile_cells, got.bottom_cells,
+            got.precision) == (3, 900, 65536, 1024, "fp64")
+    assert got.tolerance == 1e-6 and got.zero_start
+    mine = autotune.resolve(insts, SolveParams(sweeps=1, tile_cells=262144), path)
+    assert mine.sweeps == 1 and mine.tile_cells == 262144 and mine.strip_target_warps == 900
+
+
+def test_untuned_keys_are_read_from_the_file_once(tmp_path, monkeypatch):
+    path = str(tmp_path / "tune.json")
+    reads = []
+    real = autotune._load
+    monkeypatch.setattr(autotune, "_load", lambda p: reads.append(p) or real(p))
+    insts = [Instance(96, 80, "dirichlet")]
+    for _ in range(3):
+        assert autotune.resolve(insts, SolveParams(), path) == SolveParams()
+    assert len(reads) == 1
