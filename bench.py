@@ -12,6 +12,7 @@ buffers, including both copies; the FP64 MGPCG on the same plan shape is
 timed for the mixed-vs-FP64 ratio.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py --config composite|batch|serve|smoother|autotune
 
 Under torchrun each rank solves its own replica (no collective on the data
 path; ``scaling`` = weak) and rank 0 prints one JSON line with the max over
