@@ -128,7 +128,8 @@ __device__ __forceinline__ void half_row(Q4<T> &u, const Q4<T> &nb1, const Q4<T>
   }
 }
 
-// The lane's four b values into / out of its slot of the warp's b window.
+// The lane's four values to q (16-byte aligned): its slot of the warp's b window,
+// or an output row of a vector-aligned array.
 template <typename T>
 __device__ __forceinline__ void put4(T *q, const Q4<T> &v) {
   if (sizeof(T) == 4) {
