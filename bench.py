@@ -591,7 +591,6 @@ def composite(args) -> None:
     for _ in range(e2e_steps):
         out, reps = gd.seamless_clone(src, tgt, mask, (0, 0), domain="mask", tolerance=args.tol)
     e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
-    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
@@ -666,7 +665,6 @@ def batch(args) -> None:
     ms, res = _timed_steps(step, args.steps, args.warmup, world, dev)
     value = replicas.aggregate_rate(cells, world, ms / 1e3) / 1e6
     its = [r.iterations for r in res]
-    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,

@@ -28,6 +28,7 @@ EXPORTS = (
     "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static", "gd_rbgs_smooth",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
+    "gd_fold_boundary",
     "gd_masked_rhs", "gd_guidance_divergence", "gd_tm_scratch_bytes", "gd_tm_log_luminance",
     "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose", "gd_dct_plan_create",
     "gd_dct_workspace_bytes", "gd_dct_plan_bind", "gd_dct_solve_neumann", "gd_dct_plan_destroy",
@@ -118,6 +119,7 @@ def _declare(lib: C.CDLL) -> None:
         "gd_gradient": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_divergence": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_fold_dirichlet": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+        "gd_fold_boundary": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _f64, _vp]),
         "gd_masked_rhs": (C.c_int, [_vp, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
         "gd_guidance_divergence": (C.c_int, [_vp, C.POINTER(FieldDesc), _i32, _i32, _i32, _i32,
                                              _vp]),

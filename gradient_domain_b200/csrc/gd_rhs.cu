@@ -68,6 +68,28 @@ __global__ void k_fold(double *__restrict__ f, const double *__restrict__ div,
   f[k] = __dmul_rn(scale, v);
 }
 
+// fold_boundary for any spacing and channel count (operators.py:139-169):
+// rhs and out are (h-2, w-2, c), bnd is (h, w, c), channels interleaved.  The
+// four ring subtractions run in the reference's order (first row, last row,
+// first column, last column), each subtracting the rounded product
+// weight * boundary, so a corner cell sees two of them in that order.
+__global__ void k_fold_ring(double *out, const double *rhs, const double *__restrict__ bnd,
+                            int h, int w, int c, double weight) {
+  const int m = h - 2, n = w - 2;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (long long)m * n * c) return;
+  const int ch = (int)(k % c);
+  const long long cell = k / c;
+  const int i = (int)(cell / n), j = (int)(cell % n);
+  auto ring = [&](int r, int col) { return bnd[((long long)r * w + col) * c + ch]; };
+  double v = rhs[k];
+  if (i == 0) v = __dsub_rn(v, __dmul_rn(weight, ring(0, j + 1)));
+  if (i == m - 1) v = __dsub_rn(v, __dmul_rn(weight, ring(h - 1, j + 1)));
+  if (j == 0) v = __dsub_rn(v, __dmul_rn(weight, ring(i + 1, 0)));
+  if (j == n - 1) v = __dsub_rn(v, __dmul_rn(weight, ring(i + 1, w - 1)));
+  out[k] = v;
+}
+
 __global__ void k_masked_rhs(double *__restrict__ f, const double *__restrict__ div,
                              const double *__restrict__ img, const unsigned char *__restrict__ unk,
                              int h, int w, double scale) {
@@ -205,6 +227,19 @@ extern "C" int gd_fold_dirichlet(double *f, const double *div, const double *bnd
                                  int32_t w, double scale, cudaStream_t st) {
   GD_REQUIRE(f && div && bnd && h > 2 && w > 2, GD_ERR_ARG, "gd_fold_dirichlet: bad arguments");
   k_fold<<<blocks((long long)(h - 2) * (w - 2)), 256, 0, st>>>(f, div, bnd, h, w, scale);
+  GD_CHECK_LAUNCH();
+  return GD_OK;
+}
+
+extern "C" int gd_fold_boundary(double *out, const double *rhs, const double *bnd, int32_t h,
+                                int32_t w, int32_t channels, double spacing, cudaStream_t st) {
+  GD_REQUIRE(out && rhs && bnd && h > 2 && w > 2 && channels > 0, GD_ERR_ARG,
+             "gd_fold_boundary: bad arguments");
+  GD_REQUIRE(spacing != 0.0 && std::isfinite(spacing), GD_ERR_ARG,
+             "gd_fold_boundary: spacing must be finite and nonzero");
+  const double weight = 1.0 / (spacing * spacing);
+  k_fold_ring<<<blocks((long long)(h - 2) * (w - 2) * channels), 256, 0, st>>>(
+      out, rhs, bnd, h, w, channels, weight);
   GD_CHECK_LAUNCH();
   return GD_OK;
 }

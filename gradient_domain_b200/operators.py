@@ -100,19 +100,16 @@ def fold_boundary(right_hand_side, boundary, spacing: float = 1.0) -> np.ndarray
     """Move the Dirichlet ring of ``boundary`` into the interior right-hand side."""
     rhs = np.asarray(right_hand_side, dtype=float)
     bnd = np.asarray(boundary, dtype=float)
-    if rhs.ndim == 3 or spacing != 1.0:
-        folded = np.array(rhs, copy=True)
-        w = 1.0 / (spacing * spacing)
-        folded[0] -= w * bnd[0, 1:-1]
-        folded[-1] -= w * bnd[-1, 1:-1]
-        folded[:, 0] -= w * bnd[1:-1, 0]
-        folded[:, -1] -= w * bnd[1:-1, -1]
-        return folded
+    if rhs.ndim not in (2, 3) or bnd.ndim != rhs.ndim:
+        raise ValueError("right_hand_side and boundary must both be (h, w) or (h, w, c)")
+    h, w = bnd.shape[:2]
+    channels = bnd.shape[2] if bnd.ndim == 3 else 1
+    if rhs.shape != (h - 2, w - 2) + bnd.shape[2:]:
+        raise ValueError(f"right_hand_side {rhs.shape} is not the interior of boundary {bnd.shape}")
     dev = _lib.device()
-    h, w = bnd.shape
-    div = torch.zeros((h, w), dtype=torch.float64, device=dev)
-    div[1:-1, 1:-1] = _dev(rhs, dev)
-    out = torch.empty((h - 2, w - 2), dtype=torch.float64, device=dev)
-    _lib.check(_lib.lib().gd_fold_dirichlet(_lib.ptr(out), _lib.ptr(div), _lib.ptr(_dev(bnd, dev)),
-                                            h, w, 1.0, _lib.stream_handle()), "gd_fold_dirichlet")
+    rd = _dev(rhs, dev)
+    out = torch.empty_like(rd)
+    _lib.check(_lib.lib().gd_fold_boundary(_lib.ptr(out), _lib.ptr(rd), _lib.ptr(_dev(bnd, dev)),
+                                           h, w, channels, float(spacing), _lib.stream_handle()),
+               "gd_fold_boundary")
     return download(out)

@@ -305,6 +305,16 @@ int gd_divergence(double *div_dev, const double *gx_dev, const double *gy_dev, i
 int gd_fold_dirichlet(double *f_dev, const double *div_dev, const double *boundary_dev,
                       int32_t h, int32_t w, double scale, cudaStream_t stream);
 
+/* out_dev <- fold_boundary(rhs, boundary, spacing) (operators.py:139-169) for any
+ * spacing and channel count: rhs and out are (h-2, w-2, channels), boundary is
+ * (h, w, channels), contiguous with channels interleaved (channels = 1 for 2-D
+ * arrays).  Each cell next to the ring subtracts (1 / spacing^2) * ring value,
+ * first row, last row, first column, last column in that order, as the
+ * reference does.  out may be rhs (in place). */
+int gd_fold_boundary(double *out_dev, const double *rhs_dev, const double *boundary_dev,
+                     int32_t h, int32_t w, int32_t channels, double spacing,
+                     cudaStream_t stream);
+
 /* Guidance fields of the editing entry points, built on the device from the
  * images themselves (poisson.py:52-92 and the field set-up of seamless_clone,
  * texture_flatten, illumination_change, poisson.py:306-431). */

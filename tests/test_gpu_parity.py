@@ -527,6 +527,30 @@ def test_operators_match_golden(golden):
     np.testing.assert_array_equal(gd.divergence(golden["op_vx"], golden["op_vy"]),
                                   golden["op_div"])
     np.testing.assert_array_equal(gd.laplacian(golden["op_u"], 0.5), golden["op_lap_h05"])
+    # the reference's fold at spacing 0.5 (operators.py:139-169), on the device
+    np.testing.assert_array_equal(gd.fold_boundary(np.zeros((12, 16)), golden["op_ring"], 0.5),
+                                  golden["op_fold"])
+
+
+@pytest.mark.parametrize("shape,channels,spacing", [((14, 18), 0, 1.0), ((14, 18), 3, 0.5),
+                                                    ((3, 3), 2, 0.3), ((3, 40), 1, 2.0),
+                                                    ((57, 4), 4, 0.75)])
+def test_fold_boundary_on_device_matches_oracle(shape, channels, spacing):
+    """Multichannel and spacing != 1 fold on the device, bitwise the reference's
+    sequence of subtractions (corners take two, in the reference's order)."""
+    rng = np.random.default_rng(sum(shape) + channels)
+    extra = (channels,) if channels else ()
+    bnd = rng.standard_normal(shape + extra)
+    rhs = rng.standard_normal((shape[0] - 2, shape[1] - 2) + extra)
+    got = gd.fold_boundary(rhs, bnd, spacing)
+    np.testing.assert_array_equal(got, ops.fold_boundary(rhs, bnd, spacing))
+    # the reference's own pins (test_operators.py:78-90): the fold completes the stencil
+    full = rng.standard_normal(shape)
+    folded = ops.laplacian(full[1:-1, 1:-1]) - gd.fold_boundary(np.zeros(
+        (shape[0] - 2, shape[1] - 2)), full)
+    np.testing.assert_allclose(folded, ops.laplacian(full)[1:-1, 1:-1], atol=1e-12)
+    with pytest.raises(ValueError):
+        gd.fold_boundary(rhs, bnd[:-1], spacing)
 
 
 def test_bounded_wait_gives_up_and_reports():
