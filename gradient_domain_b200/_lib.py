@@ -27,7 +27,7 @@ EXPORTS = (
     "gd_plan_workspace_bytes", "gd_plan_bind", "gd_plan_set_mask", "gd_plan_prepare",
     "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static", "gd_rbgs_smooth",
-    "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
+    "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_ref_restrict", "gd_ref_prolong_add", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
     "gd_fold_boundary",
     "gd_masked_rhs", "gd_guidance_divergence", "gd_tm_scratch_bytes", "gd_tm_log_luminance",
     "gd_tm_downsample", "gd_tm_level_factor", "gd_tm_compose", "gd_dct_plan_create",
@@ -116,6 +116,8 @@ def _declare(lib: C.CDLL) -> None:
         "gd_ref_residual": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),
         "gd_ref_dot": (C.c_int, [_vp, _vp, _vp, _i64, _vp, _sz, _vp]),
         "gd_ref_axpby": (C.c_int, [_vp, _vp, _f64, _f64, _i64, _vp]),
+        "gd_ref_restrict": (C.c_int, [_vp, _vp, _i32, _i32, _vp]),
+        "gd_ref_prolong_add": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp]),
         "gd_gradient": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_divergence": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
         "gd_fold_dirichlet": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _f64, _vp]),

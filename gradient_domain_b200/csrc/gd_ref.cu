@@ -311,6 +311,25 @@ extern "C" int gd_ref_axpby(double *y, const double *x, double alpha, double bet
   return GD_OK;
 }
 
+extern "C" int gd_ref_restrict(double *rc, const double *r, int32_t m, int32_t n,
+                               cudaStream_t st) {
+  GD_REQUIRE(rc && r && m >= 3 && n >= 3, GD_ERR_ARG,
+             "gd_ref_restrict: needs a fine grid of at least 3 x 3");
+  const int mc = (m - 1) / 2, nc = (n - 1) / 2;
+  ref_restrict_kernel<<<blocks_for((long long)mc * nc, 256), 256, 0, st>>>(rc, r, m, n, mc, nc);
+  GD_CHECK_LAUNCH();
+  return GD_OK;
+}
+
+extern "C" int gd_ref_prolong_add(double *u, const double *e, int32_t m, int32_t n, int32_t mc,
+                                  int32_t nc, cudaStream_t st) {
+  GD_REQUIRE(u && e && m > 0 && n > 0 && mc > 0 && nc > 0, GD_ERR_ARG,
+             "gd_ref_prolong_add: bad arguments");
+  ref_prolong_add_kernel<<<blocks_for((long long)m * n, 256), 256, 0, st>>>(u, e, m, n, mc, nc);
+  GD_CHECK_LAUNCH();
+  return GD_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free variant of gd_ref_vcycle.
 //

@@ -136,6 +136,31 @@ def smooth(u, b, spacing: float = 1.0, sweeps: int = 1):
     return out if as_tensor else download(out)
 
 
+def _restrict(residual) -> np.ndarray:
+    """Full-weighting restriction, 0.25 Rows^T r Cols (multigrid.py:169-174), on the device;
+    an (m, n) grid goes to ((m - 1) // 2, (n - 1) // 2)."""
+    dev = _lib.device()
+    r = _to_dev(np.asarray(residual, dtype=float), dev)
+    m, n = r.shape
+    rc = torch.empty(((m - 1) // 2, (n - 1) // 2), dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().gd_ref_restrict(_lib.ptr(rc), _lib.ptr(r), m, n, _lib.stream_handle()),
+               "gd_ref_restrict")
+    return download(rc)
+
+
+def _prolong(correction, shape) -> np.ndarray:
+    """Bilinear interpolation Rows e Cols^T of a coarse correction onto an ``shape`` grid,
+    zero outside the coarse grid (multigrid.py:177-181), on the device."""
+    dev = _lib.device()
+    e = _to_dev(np.asarray(correction, dtype=float), dev)
+    m, n = int(shape[0]), int(shape[1])
+    u = torch.zeros((m, n), dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib().gd_ref_prolong_add(_lib.ptr(u), _lib.ptr(e), m, n, e.shape[0],
+                                             e.shape[1], _lib.stream_handle()),
+               "gd_ref_prolong_add")
+    return download(u)
+
+
 def v_cycle(u, b, spacing: float, options: MultigridOptions) -> np.ndarray:
     """One V-cycle on ``laplacian(u) = b`` (multigrid.py:184-215); returns a new array."""
     dev = _lib.device()

@@ -16,6 +16,8 @@ the GPU solver and the CPU baseline see identical inputs.
 * ``composite_case``: seamless compositing of two blob images inside a
   random 12-vertex star polygon (radii 300-800 px around the centre of a
   2048 x 2048 canvas), the reference's masked setup (poisson.py:154-244).
+* ``batch_instances``: the uneven batch of integration and compositing
+  problems (sides 64-2048, one or three channels).
 """
 
 from __future__ import annotations
@@ -142,20 +144,24 @@ def composite_case(size=2048, seed=2):
     return source, target, mask
 
 
-def masked_system(source, target, mask):
+def masked_system(source, target, mask, crop=True):
     """Masked Poisson system of seamless cloning in "import" mode at offset (0, 0).
 
     Returns (f, unknown, window): per-channel right-hand sides of the reference
-    sign convention A x = f (A positive) on the bounding box of the unknowns
-    plus a one-pixel ring, the unknown mask on that box, and the box slices.
-    The system is the one poisson.py:154-244 assembles for
+    sign convention A x = f (A positive), the unknown mask and the window they
+    cover.  With ``crop`` the window is the bounding box of the unknowns plus a
+    one-pixel ring, otherwise the whole canvas.  The system is the one
+    poisson.py:154-244 assembles for
     seamless_clone(source, target, mask, (0, 0), mode="import", domain="mask").
     """
     inner = np.zeros(mask.shape, dtype=bool)
     inner[1:-1, 1:-1] = mask[1:-1, 1:-1]
-    rows = np.nonzero(inner.any(axis=1))[0]
-    cols = np.nonzero(inner.any(axis=0))[0]
-    win = (slice(rows[0] - 1, rows[-1] + 2), slice(cols[0] - 1, cols[-1] + 2))
+    if crop:
+        rows = np.nonzero(inner.any(axis=1))[0]
+        cols = np.nonzero(inner.any(axis=0))[0]
+        win = (slice(rows[0] - 1, rows[-1] + 2), slice(cols[0] - 1, cols[-1] + 2))
+    else:
+        win = (slice(0, mask.shape[0]), slice(0, mask.shape[1]))
     unk = inner[win]
     f = []
     for c in range(target.shape[2]):
@@ -175,14 +181,30 @@ def masked_system(source, target, mask):
     return np.stack(f), unk, win
 
 
+def blob_pair(shape, channels, rng):
+    """Source and target images (h, w, channels) in [0, 1], sums of 32 blobs each."""
+    m = min(shape)
+
+    def image():
+        img = np.stack([blob_image(shape, 32, rng, sigma=(0.005 * m + 1.0, 0.06 * m + 1.0))
+                        for _ in range(channels)], axis=2)
+        img -= img.min()
+        return img / max(img.max(), 1e-12)
+
+    return image(), image()
+
+
 def batch_instances(count=256, seed=3, side=(64, 2048)):
     """The uneven batch: `count` images of 1 or 3 channels (p = 0.5).
 
     Sides are log-uniform in [64, 2048], the aspect ratio uniform in [0.5, 2],
     both sides rounded to multiples of 8.  Even-numbered images are Neumann
-    integrations of a blob gradient field, odd ones Dirichlet problems on a
-    star-polygon mask.  Returns a list of dicts with keys boundary, f (c, h, w)
-    and, for masks, unknown (h, w).
+    integrations of a blob gradient field (the single-image integration case),
+    odd ones seamless composites: a blob source pasted into a blob target
+    inside a 12-vertex star polygon (radii 0.15-0.45 of the shorter side), the
+    masked system of the compositing case on the whole canvas.  Returns a list
+    of dicts with keys boundary, f (c, h, w) and, for masks, unknown (h, w),
+    source and target (h, w, c).
     """
     rng = np.random.default_rng(seed)
     out = []
@@ -198,10 +220,10 @@ def batch_instances(count=256, seed=3, side=(64, 2048)):
         else:
             m = min(h, w)
             mask = star_polygon_mask_shape((h, w), rng, rmin=0.15 * m, rmax=0.45 * m)
-            unk = np.zeros_like(mask)
-            unk[1:-1, 1:-1] = mask[1:-1, 1:-1]
-            f = np.stack([np.where(unk, rng.standard_normal((h, w)), 0.0) for _ in range(ch)])
-            out.append({"boundary": "masked", "f": f, "unknown": unk})
+            source, target = blob_pair((h, w), ch, rng)
+            f, unk, _ = masked_system(source, target, mask, crop=False)
+            out.append({"boundary": "masked", "f": f, "unknown": unk, "source": source,
+                        "target": target})
     return out
 
 

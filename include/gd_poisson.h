@@ -288,6 +288,17 @@ int gd_ref_dot(double *out_dev, const double *a_dev, const double *b_dev, int64_
 int gd_ref_axpby(double *y_dev, const double *x_dev, double alpha, double beta,
                  int64_t count, cudaStream_t stream);
 
+/* rc ((m-1)/2 x (n-1)/2) <- _restrict(r) = 0.25 Rows^T r Cols, full weighting
+ * (multigrid.py:169-174); r is m x n contiguous, m, n >= 3. */
+int gd_ref_restrict(double *rc_dev, const double *r_dev, int32_t m, int32_t n,
+                    cudaStream_t stream);
+
+/* u (m x n) += _prolong(e, (m, n)) = Rows e Cols^T, bilinear with zeros outside
+ * the coarse grid (multigrid.py:177-181, _prolongation_1d :111-133); e is
+ * mc x nc contiguous. */
+int gd_ref_prolong_add(double *u_dev, const double *e_dev, int32_t m, int32_t n, int32_t mc,
+                       int32_t nc, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Right-hand-side assembly (operators.py:53-83, :139-169; poisson.py:210-224).
  * -------------------------------------------------------------------------*/

@@ -134,5 +134,45 @@ def main(reference_root: str) -> None:
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path) / 1024:.0f} KiB")
 
 
+def suite(reference_root: str) -> None:
+    """Inputs of the reference's own test suite (gradient-domain/tests), made by the
+    reference's procedural image generators (synthetic.py), written to suite.npz.
+
+    tests/test_reference_suite.py re-runs every case of test_solvers.py,
+    test_operators.py and test_applications.py on these inputs through the B200
+    package; the generators themselves are test data, not part of the solve path.
+    """
+    sys.dont_write_bytecode = True
+    sys.path.insert(0, os.path.join(reference_root, "gradient-domain", "src"))
+    from gradient_domain import synthetic
+    from gradient_domain.benchmark import manufactured_problem
+
+    out: dict[str, np.ndarray] = {}
+    # test_applications.py:32-34 (module fixture)
+    ex = synthetic.make_compositing_example(shape=(160, 240), seed=0)
+    out["ex_target"], out["ex_source"] = ex.target, ex.source
+    out["ex_mask"], out["ex_offset"] = ex.mask, np.array(ex.offset)
+    out["ex_naive"] = ex.naive_composite()
+    # test_applications.py:149-164
+    for shape in ((96, 96), (128, 128)):
+        image, edges = synthetic.make_texture_example(shape=shape, seed=1)
+        out[f"tex{shape[0]}_image"], out[f"tex{shape[0]}_edges"] = image, edges
+    # test_applications.py:178-198
+    for shape in ((128, 176), (96, 128)):
+        out[f"rad{shape[0]}x{shape[1]}"] = synthetic.make_radiance_map(shape=shape, seed=2)
+    # the manufactured right-hand sides the solver tests draw (test_solvers.py), to pin
+    # this package's restatement of benchmark.manufactured_problem
+    for shape, seed in (((63, 63), 3), ((47, 61), 4), ((127, 127), 7), ((33, 33), 10),
+                        ((31, 31), 5)):
+        out[f"mp{shape[0]}x{shape[1]}s{seed}"] = manufactured_problem(shape, seed=seed)[0]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "suite.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path) / 1024:.0f} KiB")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else "/root/reference"
+    if "--suite" not in sys.argv:
+        main(root)
+    suite(root)

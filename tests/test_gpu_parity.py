@@ -532,6 +532,16 @@ def test_operators_match_golden(golden):
                                   golden["op_fold"])
 
 
+def test_transfers_match_golden(golden):
+    """Full-weighting restriction and bilinear prolongation of the reference
+    (multigrid.py:169-181) on the device."""
+    from gradient_domain_b200.multigrid import _prolong, _restrict
+    np.testing.assert_allclose(_restrict(golden["tr_fine"]), golden["tr_restrict"], rtol=1e-12,
+                               atol=1e-15)
+    np.testing.assert_allclose(_prolong(golden["tr_coarse"], (31, 25)), golden["tr_prolong"],
+                               rtol=1e-12, atol=1e-15)
+
+
 @pytest.mark.parametrize("shape,channels,spacing", [((14, 18), 0, 1.0), ((14, 18), 3, 0.5),
                                                     ((3, 3), 2, 0.3), ((3, 40), 1, 2.0),
                                                     ((57, 4), 4, 0.75)])

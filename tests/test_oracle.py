@@ -191,3 +191,18 @@ def test_operator_adjointness_and_folding():
     assert np.allclose(operators.laplacian(inner) - operators.fold_boundary(np.zeros_like(inner),
                                                                            full),
                        operators.laplacian(full)[1:-1, 1:-1])
+
+
+@pytest.mark.parametrize("key", ["mp63x63s3", "mp47x61s4", "mp127x127s7", "mp33x33s10",
+                                 "mp31x31s5"])
+def test_package_manufactured_problem_matches_reference(key):
+    """The package's benchmark.manufactured_problem (the known-answer generator the
+    reference's solver tests use) against the reference's own output."""
+    import os
+
+    from gradient_domain_b200.benchmark import manufactured_problem
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "suite.npz")
+    shape_s, seed = key[2:].split("s")
+    shape = tuple(int(v) for v in shape_s.split("x"))
+    with np.load(path) as data:
+        np.testing.assert_array_equal(manufactured_problem(shape, seed=int(seed))[0], data[key])
