@@ -352,7 +352,7 @@ def ours(args) -> None:
         ms_dct = e0.elapsed_time(e1) / args.steps
         dct = {"ms_per_step": ms_dct, "mpix_s": cells / (ms_dct / 1e3) / 1e6,
                "note": "exact transform solve (the reference's solve_neumann algorithm), "
-                       "cuFFT FFTs with this library's permutation / twiddle / eigenvalue kernels"}
+                       "this library's FFT kernels: rows, columns with the eigenvalue division, rows"}
         if not args.no_cpu:
             from oracle import solvers as osolvers
             ref0 = osolvers.solve_neumann(rhs_np[0], workers=os.cpu_count())
@@ -439,12 +439,84 @@ def ours(args) -> None:
         "profiled_pass_ms_per_step": ms_prof,
     }
     line.update(extra)
+    if rank == 0 and not args.no_serve:
+        line["serving"] = serving_1mp(args)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_tonemap(rhs_np)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
     replicas.finish(world)
+
+
+def serving_1mp(args) -> dict:
+    """Served latency of 1 MP requests: ready 1024 x 1024 Neumann systems (blob
+    gradient fields) from pinned host memory at 100 req/s, open-loop Poisson
+    arrivals, through the continuous-batching server; latency from the scheduled
+    arrival to the solution on the host (upload, solve to 1e-8, download)."""
+    from gradient_domain_b200 import loadgen
+    from gradient_domain_b200.serving import GpuBackend, PoissonServer
+    with PoissonServer(GpuBackend(sweeps=args.sweeps), workers=3) as server:
+        r = loadgen.latency_1mp(server, requests=args.requests_1mp, rate=100.0)
+        server.backend.pool.clear()
+    return {"workload": "1024x1024x1 Neumann systems, 100 req/s open-loop Poisson arrivals",
+            "requests": r.requests, "p50_ms": r.p50_ms, "p99_ms": r.p99_ms,
+            "solves_per_s": r.solves_per_s, "converged": r.converged, "batches": r.batches,
+            "latency": "scheduled arrival to the solution on the host: pinned upload, "
+                       "solve to a 1e-8 true relative residual, download",
+            "target_p99_ms": 5.0}
+
+
+def serve_main(args) -> None:
+    """`--config serve`: the open-loop serving benchmark.  `--requests` requests per
+    offered load (default 20000), each built from its own seed (kind uniform over
+    composite / flatten / tone-map, side log-uniform in [256, 4096]); p50 / p99
+    latency and solves/s per load, plans built, the 1 MP latency, and the plain
+    per-request FP64 GPU solve (exact-size plan per request, no reuse) on a sample
+    of the same stream."""
+    import torch
+
+    from gradient_domain_b200 import loadgen
+    from gradient_domain_b200.serving import GpuBackend, PoissonServer
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    cv = loadgen.Canvases(side=4096, seed=41).build()
+
+    def stream(base):
+        return lambda i: loadgen.build(loadgen.describe(base + i, cv.side), cv)
+
+    out = {"metric": "served p50/p99 latency", "unit": "ms", "config": {
+        "workload": "open-loop Poisson arrivals; per-request seeds: kind uniform over "
+                    "composite / flatten / tone-map, side log-uniform 256-4096",
+        "requests_per_rate": args.requests, "rates": args.rates, "hbm_fraction": 0.8,
+        "canvas_seconds": round(time.perf_counter() - t0, 2)}}
+    with PoissonServer(GpuBackend(sweeps=args.sweeps), workers=3) as server:
+        out["budget_gb"] = round(server.budget / 1e9, 1)
+        warm = loadgen.run_load(server, stream(10 ** 8), args.warm_requests, 100.0, seed=1)
+        out["warm_up"] = {"requests": warm.requests, "plans_built": warm.extra.get("plans_built")}
+        loads = []
+        for k, rate in enumerate(args.rates):
+            r = loadgen.run_load(server, stream((k + 1) * 10 ** 7), args.requests, rate,
+                                 seed=int(rate))
+            loads.append(r.__dict__)
+            print(json.dumps({"load": r.__dict__}), flush=True)
+        out["loads"] = loads
+        r1 = loadgen.latency_1mp(server, requests=args.requests_1mp, rate=100.0)
+        out["one_mp"] = r1.__dict__
+        server.backend.pool.clear()
+    # the plain per-request FP64 GPU solve: one worker, one request per batch, a plan of
+    # the request's exact size built, solved once and freed, no graph
+    sample = [loadgen.build(loadgen.describe(10 ** 7 + i, cv.side), cv)
+              for i in range(args.baseline_requests)]
+    with PoissonServer(GpuBackend(sweeps=args.sweeps, precision="fp64", resident=False),
+                       workers=1, max_batch_requests=1) as base:
+        t0 = time.perf_counter()
+        res = [base.submit(r).result() for r in sample]
+        dt = time.perf_counter() - t0
+    out["fp64_per_request"] = {"requests": len(sample), "solves_per_s": len(sample) / dt,
+                               "converged": sum(r.converged for r in res),
+                               "note": "sequential; the first requests of the rated streams"}
+    print(json.dumps(out), flush=True)
 
 
 def smoother_gate(n: int, hbm: float, kinds: dict, sweeps: int, reps: int = 20) -> dict:
@@ -708,10 +780,15 @@ def main():
     ap.add_argument("--count", type=int, default=256, help="images in the batch workload")
     ap.add_argument("--rates", type=float, nargs="+", default=[200.0, 1000.0, 5000.0],
                     help="serving: offered loads in requests per second")
-    ap.add_argument("--requests", type=int, default=2000, help="serving: requests per load")
-    ap.add_argument("--requests-1mp", type=int, default=400,
+    ap.add_argument("--requests", type=int, default=20000, help="serving: requests per load")
+    ap.add_argument("--requests-1mp", type=int, default=300,
                     help="serving: 1 MP requests for the latency target")
-    ap.add_argument("--pool", type=int, default=12, help="serving: distinct requests per type")
+    ap.add_argument("--warm-requests", type=int, default=300,
+                    help="serving: warm-up requests before the rated loads")
+    ap.add_argument("--baseline-requests", type=int, default=60,
+                    help="serving: requests of the per-request FP64 baseline")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the 1 MP serving latency of the default line")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -729,8 +806,7 @@ def main():
         line["peak_source"] = peak_kind
         print(json.dumps({"smoother": line}), flush=True)
     elif args.config == "serve":
-        from gradient_domain_b200 import serving
-        serving.bench_main(args)
+        serve_main(args)
     else:
         ours(args)
 

@@ -128,7 +128,7 @@ def _declare(lib: C.CDLL) -> None:
         "gd_tm_scratch_bytes": (_sz, []),
         "gd_dct_plan_create": (C.c_int, [_i32, _i32, C.POINTER(C.c_void_p)]),
         "gd_dct_workspace_bytes": (_sz, [_vp]),
-        "gd_dct_plan_bind": (C.c_int, [_vp, _vp, _sz]),
+        "gd_dct_plan_bind": (C.c_int, [_vp, _vp, _sz, _vp]),
         "gd_dct_solve_neumann": (C.c_int, [_vp, _vp, _vp, _i32, _vp]),
         "gd_dct_plan_destroy": (None, [_vp]),
         "gd_tm_log_luminance": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),

@@ -19,10 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgd_poisson.so")
 
-# cuFFT runs the FFTs of the DCT Neumann solver (gd_dct.cu)
-LINK = ["-lcufft", "-Xlinker", "-rpath," + os.path.join(
-    os.path.dirname(os.path.dirname(os.path.realpath(os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")))),
-    "lib64")]
+# the library links only the CUDA runtime (every kernel, the DCT's FFTs included, is its own)
+LINK: list[str] = []
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -76,20 +76,14 @@ def attenuation_field(log_luminance, config: ToneMapConfig) -> np.ndarray:
     return download(_attenuation_dev(logl, config, _scratch(dev)))
 
 
-def tone_map(radiance, config: ToneMapConfig | None = None):
-    """Compress a linear HDR radiance map (h, w, 3) to display values in [0, 1].
-
-    Returns the image and the attenuation factor that was applied.  Raises
-    ``ValueError`` if the input is not a three-channel image.
-    """
-    config = config or ToneMapConfig()
-    radiance = np.asarray(radiance, dtype=float)
-    if radiance.ndim != 3 or radiance.shape[2] != 3:
-        raise ValueError("tone mapping expects a three-channel radiance map")
-    h, w, _ = radiance.shape
-    dev = _lib.device()
+def tone_map_device(rad: torch.Tensor, config: ToneMapConfig, dct=None):
+    """The tone-mapping pipeline on a device radiance map (h, w, 3) FP64, on the
+    current stream; returns the display image (h, w, 3) and the factor (h, w),
+    both on the device.  ``dct`` is the DCT solver of this shape to use (a
+    ``DctPlan``; by default the process-wide one of the shape)."""
+    h, w, _ = rad.shape
+    dev = rad.device
     lib, st = _lib.lib(), _lib.stream_handle()
-    rad = upload(radiance, dev, np.float64)
     logl = torch.empty((h, w), dtype=torch.float64, device=dev)
     lum = torch.empty_like(logl)
     _lib.check(lib.gd_tm_log_luminance(_lib.ptr(logl), _lib.ptr(lum), _lib.ptr(rad), h, w, st),
@@ -104,9 +98,10 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
     _lib.check(lib.gd_guidance_divergence(_lib.ptr(div), C.byref(desc), 0, 0, h, w, st),
                "gd_guidance_divergence")
     compressed = torch.zeros_like(div)
-    if h >= 2 and w >= 2:  # the reference's exact transform solve (solvers.py:224-262)
-        from .solvers import _dct_plan
-        _dct_plan(h, w).solve(div, compressed)
+    from .solvers import DCT_MAX_SIDE, _dct_plan
+    if 2 <= min(h, w) and max(h, w) <= DCT_MAX_SIDE:
+        # the reference's exact transform solve (solvers.py:224-262)
+        (dct or _dct_plan(h, w)).solve(div, compressed)
     else:
         plan = cached_plan((Instance(h, w, "neumann", True),),
                            SolveParams(tolerance=NEUMANN_TOLERANCE, zero_start=True))
@@ -116,4 +111,18 @@ def tone_map(radiance, config: ToneMapConfig | None = None):
     _lib.check(lib.gd_tm_compose(_lib.ptr(out), _lib.ptr(image), _lib.ptr(rad), _lib.ptr(lum),
                                  _lib.ptr(compressed), h, w, float(config.saturation), 99.5,
                                  _lib.ptr(scratch), st), "gd_tm_compose")
+    return out, factor
+
+
+def tone_map(radiance, config: ToneMapConfig | None = None):
+    """Compress a linear HDR radiance map (h, w, 3) to display values in [0, 1].
+
+    Returns the image and the attenuation factor that was applied.  Raises
+    ``ValueError`` if the input is not a three-channel image.
+    """
+    config = config or ToneMapConfig()
+    radiance = np.asarray(radiance, dtype=float)
+    if radiance.ndim != 3 or radiance.shape[2] != 3:
+        raise ValueError("tone mapping expects a three-channel radiance map")
+    out, factor = tone_map_device(upload(radiance, _lib.device(), np.float64), config)
     return download(out), download(factor)

@@ -220,8 +220,12 @@ def solve_system(b, method: str = "mgcg", spacing: float = 1.0, tolerance: float
 NEUMANN_EXACT_TOLERANCE = 1e-14
 
 
+DCT_MAX_SIDE = 8192  # longest line a DCT pass holds in shared memory
+
+
 class DctPlan:
-    """cuFFT-based DCT Neumann solver for one grid shape (gd_dct_* of the C ABI)."""
+    """DCT Neumann solver for one grid shape (gd_dct_* of the C ABI): the library's own
+    FFT kernels, three passes over the grid, sides of 2 to 8192 cells."""
 
     def __init__(self, h: int, w: int):
         self.shape = (h, w)
@@ -232,8 +236,8 @@ class DctPlan:
         self._handle = handle
         nbytes = int(lib.gd_dct_workspace_bytes(handle))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
-        _lib.check(lib.gd_dct_plan_bind(handle, _lib.ptr(self.workspace), nbytes),
-                   "gd_dct_plan_bind")
+        _lib.check(lib.gd_dct_plan_bind(handle, _lib.ptr(self.workspace), nbytes,
+                                        _lib.stream_handle()), "gd_dct_plan_bind")
 
     def solve(self, b: torch.Tensor, u: torch.Tensor) -> torch.Tensor:
         """u = zero-mean solution of laplacian(u) = b (FP64 device tensors, one row pitch)."""
@@ -241,8 +245,8 @@ class DctPlan:
             if (t.dtype != torch.float64 or t.device != self.device or tuple(t.shape) != self.shape
                     or t.stride(1) != 1):
                 raise ValueError(f"expected {self.shape} float64 tensors on {self.device}")
-        if b.stride(0) != u.stride(0) or b.data_ptr() == u.data_ptr():
-            raise ValueError("b and u must share a row pitch and may not alias")
+        if b.stride(0) != u.stride(0):
+            raise ValueError("b and u must share a row pitch (u may be b: solved in place)")
         _lib.check(_lib.lib().gd_dct_solve_neumann(self._handle, _lib.ptr(b), _lib.ptr(u),
                                                    u.stride(0), _lib.stream_handle()),
                    "gd_dct_solve_neumann")
@@ -282,7 +286,8 @@ def solve_neumann(b, tolerance: float = NEUMANN_EXACT_TOLERANCE,
     drives the true relative residual to 1e-14, so that even the smoothest
     error mode is reduced to the rounding level of the exact transform solve.
     ``method="dct"`` runs the reference's own algorithm (forward DCT-II,
-    division by the eigenvalues, inverse) on the device with cuFFT.  Either
+    division by the eigenvalues, inverse) on the device with this library's
+    FFT kernels (sides up to 8192; larger grids raise ``ValueError``).  Either
     way any constant component of ``b`` is discarded and the solution has
     zero mean.
     """
@@ -290,8 +295,9 @@ def solve_neumann(b, tolerance: float = NEUMANN_EXACT_TOLERANCE,
     if b.ndim != 2:
         raise ValueError("solve_neumann expects a 2-D right-hand side")
     if method == "dct":
-        if min(b.shape) < 2:
-            raise ValueError("the DCT solver needs at least 2 x 2 cells")
+        if min(b.shape) < 2 or max(b.shape) > DCT_MAX_SIDE:
+            raise ValueError(f"the DCT solver takes sides of 2 to {DCT_MAX_SIDE} cells, "
+                             f"not {b.shape}")
         dev = _lib.device()
         bd = _dev_array(b, dev)
         return download(_dct_plan(*b.shape).solve(bd, torch.empty_like(bd)))

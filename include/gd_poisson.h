@@ -152,17 +152,21 @@ int gd_plan_apply_vcycle(gd_plan plan, int32_t instance, const double *r_dev,
                          double *z_dev, int32_t pitch, cudaStream_t stream);
 
 /* Exact Neumann solve by the discrete cosine transform, the algorithm of
- * solvers.py:224-262 (replaces scipy dctn / idctn with cuFFT-based DCT-II
- * kernels): u = zero-mean solution of laplacian(u) = b with edge-replicated
- * (Neumann) boundaries, any constant component of b dropped.  Grids of at
- * least 2 x 2.  The plan holds cuFFT plans made without work-area allocation;
- * the caller binds a 256-byte aligned workspace of gd_dct_workspace_bytes
- * (buffers and the cuFFT work area) before solving.  b and u have row pitch
- * `pitch` (elements) and may not alias. */
+ * solvers.py:224-262 (replaces scipy dctn / idctn; the FFTs are this
+ * library's own shared-memory kernels): u = zero-mean solution of
+ * laplacian(u) = b with edge-replicated (Neumann) boundaries, any constant
+ * component of b dropped.  Sides of 2 to 8192 cells (GD_ERR_UNSUPPORTED
+ * beyond).  Three passes: rows, columns (with the eigenvalue division) and
+ * rows again, through one coefficient buffer.  The plan allocates nothing on
+ * the device; the caller binds a 256-byte aligned workspace of
+ * gd_dct_workspace_bytes (the coefficient buffer and the twiddle and
+ * eigenvalue tables, filled at bind on `stream`, which bind then waits for)
+ * before solving.  b and u have row pitch
+ * `pitch` (elements) and may alias (u = b solves in place). */
 typedef struct gd_dct_plan_s *gd_dct_plan;
 int gd_dct_plan_create(int32_t h, int32_t w, gd_dct_plan *out);
 size_t gd_dct_workspace_bytes(gd_dct_plan plan);
-int gd_dct_plan_bind(gd_dct_plan plan, void *workspace_dev, size_t bytes);
+int gd_dct_plan_bind(gd_dct_plan plan, void *workspace_dev, size_t bytes, cudaStream_t stream);
 int gd_dct_solve_neumann(gd_dct_plan plan, const double *b_dev, double *u_dev, int32_t pitch,
                          cudaStream_t stream);
 void gd_dct_plan_destroy(gd_dct_plan plan);

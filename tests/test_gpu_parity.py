@@ -78,15 +78,28 @@ def test_solve_neumann_matches_golden(golden, key):
     assert abs(float(got.mean())) < 1e-12
 
 
-@pytest.mark.parametrize("shape", [(2, 2), (3, 5), (64, 64), (97, 130), (257, 2), (1024, 768)])
+@pytest.mark.parametrize("shape", [(2, 2), (3, 5), (64, 64), (97, 130), (257, 2), (1024, 768),
+                                   (7, 11), (49, 121), (1000, 1080), (2187, 6), (8192, 10),
+                                   (10, 8192), (4096, 4096), (509, 1021), (128, 512),
+                                   (2048, 256)])
 def test_dct_neumann_matches_oracle(shape):
-    """The cuFFT DCT solver against the oracle's scipy DCT solve."""
+    """The hand-written DCT solver against the oracle's scipy DCT solve: radices 8, 4,
+    2, 3, 5, 7, large primes (97, 257, 509, 1021, 13), odd lines (one unpaired row or
+    column per pass) and the longest supported line (8192)."""
     rng = np.random.default_rng(shape[0] * 7 + shape[1])
     b = rng.standard_normal(shape)
     got = gd.solve_neumann(b, method="dct")
     want = osolvers.solve_neumann(b)
     assert _rel(got, want) <= 1e-12
     assert abs(got.mean()) <= 1e-12 * np.abs(got).max()
+
+
+def test_dct_neumann_rejects_sides_beyond_its_line_limit():
+    with pytest.raises(ValueError):
+        gd.solve_neumann(np.zeros((8193, 4)), method="dct")
+    with pytest.raises(_lib.GDError):
+        from gradient_domain_b200.solvers import DctPlan
+        DctPlan(4, 8193)
 
 
 def test_dct_neumann_batch_matches_single():
