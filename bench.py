@@ -26,6 +26,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -789,7 +790,12 @@ def main():
                     help="serving: requests of the per-request FP64 baseline")
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the 1 MP serving latency of the default line")
+    ap.add_argument("--autotune-cache", default=None,
+                    help="autotuner cache file for plans built with unset knobs (default: a "
+                         "fresh empty file, so no earlier tuning changes the measured plans)")
     args = ap.parse_args()
+    os.environ["GD_AUTOTUNE_CACHE"] = args.autotune_cache or os.path.join(
+        tempfile.mkdtemp(prefix="gd_autotune_bench_"), "autotune.json")
     if args.impl == "reference":
         reference_arm(args)
     elif args.config == "composite":

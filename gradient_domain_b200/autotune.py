@@ -17,12 +17,12 @@ number of instances in a plan and the boundary type:
 graph path after warm-up) and runs a coordinate descent from the defaults over
 :data:`SPACE`, keeping a change only when it gains at least ``min_gain``.  The
 winner is cached under :func:`tune_key` - boundary types, level-0 size bucket
-(powers of two of cells), instance-count bucket and precision - in memory and
-in a JSON file (``$GD_AUTOTUNE_CACHE``, default
+(powers of two of cells), instance-count bucket, precision and device name - in
+memory and in a JSON file (``$GD_AUTOTUNE_CACHE``, default
 ``~/.cache/gradient_domain_b200/autotune.json``); :func:`lookup` returns the
 cached parameters for a plan without timing anything, and :func:`resolve` -
 which the plan cache, the pipelined batch solves and the serving workers call -
-applies them to the fields a caller left at their defaults.
+applies them to the fields a caller left unset (None).
 
 Tuned parameters change the arithmetic (sweeps, which levels run on which
 kernel kind), never the stopping rule: every candidate solve has to converge
@@ -65,8 +65,14 @@ def cache_path() -> str:
                         "autotune.json")
 
 
-def tune_key(instances: Sequence[Instance], params: SolveParams | None = None) -> str:
-    """Cache key: boundary types, level-0 size bucket, instance-count bucket, precision."""
+def device_name() -> str:
+    return torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+
+
+def tune_key(instances: Sequence[Instance], params: SolveParams | None = None,
+             device: str | None = None) -> str:
+    """Cache key: boundary types, level-0 size bucket, instance-count bucket, precision and
+    the device the entry was timed on (entries of another GPU model never apply)."""
     params = params or SolveParams()
     if not instances:
         raise ValueError("no instances")
@@ -74,7 +80,8 @@ def tune_key(instances: Sequence[Instance], params: SolveParams | None = None) -
     cells = max(inst.height * inst.width for inst in instances)
     size_bucket = int(round(math.log2(max(cells, 1))))
     count_bucket = 1 << int(math.ceil(math.log2(len(instances)))) if len(instances) > 1 else 1
-    return f"{kinds}|cells~2^{size_bucket}|n<={count_bucket}|{params.precision}"
+    return (f"{kinds}|cells~2^{size_bucket}|n<={count_bucket}|{params.value('precision')}|"
+            f"{device or device_name()}")
 
 
 def _load(path: str) -> dict:
@@ -117,7 +124,7 @@ def lookup(instances: Sequence[Instance], params: SolveParams | None = None,
         else:  # read the file once per key; an untuned key is remembered as such
             entry = _load(path).get(key) or {}
             _MEMORY[(path, key)] = entry
-    if not entry:
+    if not entry or entry.get("device", device_name()) != device_name():
         return params
     return _apply(params, entry.get("choice", {}))
 
@@ -125,16 +132,15 @@ def lookup(instances: Sequence[Instance], params: SolveParams | None = None,
 def resolve(instances: Sequence[Instance], params: SolveParams | None = None,
             path: str | None = None) -> SolveParams:
     """The parameters a plan for ``instances`` is built with: the cached tuned values
-    applied to the fields that ``params`` leaves at their defaults (an explicit choice of
-    the caller, e.g. ``sweeps=3``, is kept); ``params`` itself if the key was never tuned."""
+    applied to the fields that ``params`` leaves unset (None); a value the caller set,
+    even one equal to the default (e.g. ``sweeps=2``), is kept.  ``params`` itself if
+    the key was never tuned."""
     params = params or SolveParams()
     tuned = lookup(instances, params, path)
     if tuned == params:
         return params
-    default = SolveParams()
-    over = {name: getattr(tuned, name) for name, _ in SPACE
-            if getattr(params, name) == getattr(default, name)}
-    if params.precision == default.precision:
+    over = {name: getattr(tuned, name) for name, _ in SPACE if getattr(params, name) is None}
+    if params.precision is None:
         over["precision"] = tuned.precision
     return replace(params, **over)
 
@@ -270,18 +276,23 @@ def tune(instances: Sequence[Instance], params: SolveParams | None = None,
     best, best_ms, history = coordinate_descent(
         lambda choice: time_solve(instances, _apply(params, choice), rhs, masks, reps, scale),
         start, SPACE, min_gain)
+    precision_ms = None
     if tune_precision:
-        other = "fp64" if params.precision == "mixed" else "mixed"
+        own = params.value("precision")
+        other = "fp64" if own == "mixed" else "mixed"
         cand = dict(best, precision=other)
         ms = time_solve(instances, _apply(params, cand), rhs, masks, reps, scale)
         history.append((cand, ms))
+        precision_ms = {own: best_ms, other: ms}
         if ms < best_ms * (1.0 - min_gain):
             best, best_ms = cand, ms
     if not math.isfinite(best_ms):
         raise _lib.GDError(f"autotune {key}: no configuration converged")
     entry = {"choice": best, "ms": best_ms, "default_ms": history[0][1],
              "trials": len(history), "seconds": time.perf_counter() - t0,
-             "device": torch.cuda.get_device_name(dev)}
+             "device": torch.cuda.get_device_name(dev), "min_gain": min_gain}
+    if precision_ms is not None:
+        entry["precision_ms"] = precision_ms
     with _CACHE_LOCK:
         _store(path, key, entry)
     return _apply(params, best)

@@ -649,6 +649,9 @@ inline bool has_large_prime(const Radices &r) {
 
 inline size_t a256(size_t v) { return (v + 255) & ~(size_t)255; }
 inline size_t smem_bytes(int n) { return (size_t)n * sizeof(double2); }
+// the most dynamic shared memory any DCT kernel launch asks for (a line of
+// kMaxLen complex values and the power-of-two twiddle tables)
+constexpr size_t kMaxSmemBytes = (size_t)kMaxLen * sizeof(double2) + Pow2Fft<13>::extra_smem(0);
 
 template <class T>
 struct Tag {
@@ -761,22 +764,24 @@ extern "C" int gd_dct_plan_bind(gd_dct_plan p, void *ws, size_t bytes, cudaStrea
   GD_CHECK_LAUNCH();
   // the tables must be complete before a solve on any stream (set-up, once per plan)
   GD_CHECK_CUDA(cudaStreamSynchronize(st));
-  // shared memory of the kernels this plan launches
+  // Shared memory of the kernels this plan launches.  The limit is one value per
+  // kernel for the whole process, so every plan sets the same value, the most any
+  // length needs: a plan bound later for a shorter line must not lower the limit
+  // under a plan of a longer one (its next launch would fail).
   cudaError_t err = cudaSuccess;
-  auto allow = [&](const void *fn, size_t bytes) {
+  auto allow = [&](const void *fn) {
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)bytes);
+                                               (int)dct::kMaxSmemBytes);
     if (e != cudaSuccess) err = e;
   };
   dct::with_fft(p->rw, [&](auto tag) {
     using F = typename decltype(tag)::type;
-    const size_t b = dct::smem_bytes(p->w) + F::extra_smem(p->w);
-    allow((const void *)dct::k_dct_rows<F>, b);
-    allow((const void *)dct::k_idct_rows<F>, b);
+    allow((const void *)dct::k_dct_rows<F>);
+    allow((const void *)dct::k_idct_rows<F>);
   });
   dct::with_fft(p->rh, [&](auto tag) {
     using F = typename decltype(tag)::type;
-    allow((const void *)dct::k_dct_cols<F>, dct::smem_bytes(p->h) + F::extra_smem(p->h));
+    allow((const void *)dct::k_dct_cols<F>);
   });
   GD_CHECK_CUDA(err);
   return GD_OK;

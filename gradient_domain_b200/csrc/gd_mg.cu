@@ -677,6 +677,10 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   build_plan(p, grids);
   if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);
   else Runner<float>::dispatch_attrs(p->prm.pre_sweeps);
+  // the limits above are constants every plan sets alike; a failure (no device in a
+  // CPU-only check) must not stay behind as this thread's last error, where a later
+  // launch check would report it as its own
+  cudaGetLastError();
   p->h_st_bytes = sizeof(InstState) * n;
   p->h_nact = static_cast<int *>(pinned_get(2 * sizeof(int)));  // active count, error word
   p->h_st = static_cast<InstState *>(pinned_get(p->h_st_bytes));

@@ -381,13 +381,16 @@ extern "C" int gd_ref_vcycle_static(double *u, const double *b, int32_t m, int32
   size_t need = 0;
   const int nlev = ref_levels(m, n, coarsest_size, lv, 64, &need);
   GD_REQUIRE(nlev > 0, GD_ERR_ARG, "gd_ref_vcycle_static: hierarchy too deep");
-  GD_REQUIRE(need <= (size_t)GD_STATIC_SCRATCH_BYTES, GD_ERR_ARG,
-             "gd_ref_vcycle_static: a %d x %d grid needs %zu bytes of scratch, more than the "
-             "%zu-byte static array; use gd_ref_vcycle with a workspace",
-             m, n, need, (size_t)GD_STATIC_SCRATCH_BYTES);
+  // a single-level hierarchy is the coarsest solve in place on u: no scratch at all
   void *ws = nullptr;
-  const int rc = static_scratch(&ws);
-  if (rc != GD_OK) return rc;
+  if (nlev > 1) {
+    GD_REQUIRE(need <= (size_t)GD_STATIC_SCRATCH_BYTES, GD_ERR_ARG,
+               "gd_ref_vcycle_static: a %d x %d grid needs %zu bytes of scratch, more than "
+               "the %zu-byte static array; use gd_ref_vcycle with a workspace",
+               m, n, need, (size_t)GD_STATIC_SCRATCH_BYTES);
+    const int rc = static_scratch(&ws);
+    if (rc != GD_OK) return rc;
+  }
   // ref_vcycle_rec zeroes every coarse iterate before use, so the contents left
   // by the previous call do not leak into this one.
   return ref_vcycle_rec(lv, nlev, 0, u, b, spacing, pre, post, coarsest_sweeps, (char *)ws, st);

@@ -140,7 +140,7 @@ def run_load(server, make, count: int, rate: float, seed: int, lookahead: int = 
     on the host."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, count)
-    lat, fin, conv, late = [], [], [], []
+    lat, fin, conv, late, errors = [], [], [], [], []
     cells = [0]
     lock = threading.Lock()
     done = threading.Event()
@@ -150,12 +150,19 @@ def run_load(server, make, count: int, rate: float, seed: int, lookahead: int = 
     b0 = server.batches
 
     def consume(fut):
-        r = fut.result()
+        try:
+            r = fut.result()
+        except Exception as exc:  # a failed request still ends: counted, not waited for
+            with lock:
+                errors.append(repr(exc)[:200])
+                if len(lat) + len(errors) == count:
+                    done.set()
+            return
         with lock:
             lat.append(r.latency * 1e3)
             fin.append(r.finished)
             conv.append(r.converged)
-            if len(lat) == count:
+            if len(lat) + len(errors) == count:
                 done.set()
         r.x = None  # a client takes its result and lets it go
 
@@ -177,10 +184,11 @@ def run_load(server, make, count: int, rate: float, seed: int, lookahead: int = 
             fut = server.submit(req, submitted=float(when))
             fut.add_done_callback(consume)
     done.wait()
-    t1 = max(fin)
-    lat_a = np.array(lat)
+    t1 = max(fin) if fin else time.perf_counter()
+    lat_a = np.array(lat) if lat else np.array([np.nan])
     extra = {"late_submissions": len(late),
-             "late_p99_ms": float(np.percentile(late, 99)) if late else 0.0}
+             "late_p99_ms": float(np.percentile(late, 99)) if late else 0.0,
+             "failed": len(errors), "first_errors": sorted(set(errors))[:3]}
     if pool:
         extra["plans_built"] = pool.built - built0
         extra["plan_build_s"] = round(pool.build_s - build_s0, 4)

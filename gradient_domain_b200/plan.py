@@ -14,7 +14,7 @@ from __future__ import annotations
 import ctypes as C
 import threading
 from collections import OrderedDict
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 import torch
@@ -25,29 +25,49 @@ from ._lib import GD_DIRICHLET, GD_FP64, GD_MASKED, GD_MIXED, GD_NEUMANN  # noqa
 BOUNDARIES = {"dirichlet": GD_DIRICHLET, "neumann": GD_NEUMANN, "masked": GD_MASKED}
 
 
+# values of the SolveParams fields that None leaves to the library (or to the autotuner's
+# cached choice for the plan's shape class, see autotune.resolve)
+DEFAULTS = {"precision": "mixed", "sweeps": 2, "strip_target_warps": 1800, "bottom_cells": 0,
+            "tile_cells": 0}
+
+
 @dataclass(frozen=True)
 class SolveParams:
-    """Knobs of the B200 MGPCG; the defaults follow solvers.py:171-177."""
+    """Knobs of the B200 MGPCG; the defaults follow solvers.py:171-177.
 
-    precision: str = "mixed"      # "mixed" (FP32 V-cycle, FP64 refinement) or "fp64"
-    sweeps: int = 2               # RB-GS sweeps before and after each coarse correction
+    Fields that are None take the library default (``DEFAULTS``) or, where a
+    plan is built through ``autotune.resolve``, the tuned value of the plan's
+    shape class; a value the caller sets, even one equal to the default, is
+    always kept."""
+
+    precision: str | None = None  # "mixed" (FP32 V-cycle, FP64 refinement) or "fp64"
+    sweeps: int | None = None     # RB-GS sweeps before and after each coarse correction (2)
     max_iterations: int = 2000
     tolerance: float = 1e-8
     reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
     check_every: int = 4          # host poll interval of solves on direct launches
     use_graph: bool = True        # from a plan's second solve on: one graph, device-side loop
-    strip_target_warps: int = 1800  # smoother strip height: warps per level launch (all instances)
-    bottom_cells: int = 0         # largest level solved inside the one-CTA bottom (0 = 4096)
-    tile_cells: int = 0           # largest coarse level on shared-memory tiles (0 = 262144)
+    strip_target_warps: int | None = None  # smoother strip height: warps per level launch (1800)
+    bottom_cells: int | None = None  # largest level solved inside the one-CTA bottom (0 = 4096)
+    tile_cells: int | None = None    # largest coarse level on shared-memory tiles (0 = 262144)
     zero_start: bool = False      # start from x = 0; x is only written (need not be zeroed)
 
+    def value(self, name: str):
+        """The field's value, with the library default in place of None."""
+        v = getattr(self, name)
+        return DEFAULTS[name] if v is None else v
+
+    def concrete(self) -> "SolveParams":
+        return replace(self, **{k: self.value(k) for k in DEFAULTS})
+
     def c_params(self) -> _lib.Params:
-        return _lib.Params(GD_FP64 if self.precision == "fp64" else GD_MIXED, self.sweeps,
-                           self.sweeps, int(self.max_iterations), float(self.tolerance),
-                           float(self.reliable_delta), int(self.check_every),
-                           1 if self.use_graph else 0, int(self.strip_target_warps),
-                           int(self.bottom_cells), int(self.tile_cells),
-                           1 if self.zero_start else 0)
+        p = self.concrete()
+        return _lib.Params(GD_FP64 if p.precision == "fp64" else GD_MIXED, int(p.sweeps),
+                           int(p.sweeps), int(p.max_iterations), float(p.tolerance),
+                           float(p.reliable_delta), int(p.check_every),
+                           1 if p.use_graph else 0, int(p.strip_target_warps),
+                           int(p.bottom_cells), int(p.tile_cells),
+                           1 if p.zero_start else 0)
 
 
 @dataclass(frozen=True)

@@ -500,15 +500,23 @@ class GpuBackend:
         return plan
 
     def _up(self, a, dtype=None):
-        """Host array (NumPy or pinned torch) to the device on the current stream."""
+        """Host array (NumPy, any strides, or a pinned torch tensor) to the device on the
+        current stream.  NumPy inputs of 1 MiB and more take one multi-threaded copy into
+        a page-locked buffer from torch's caching host allocator (recycled once its DMA
+        is done), then the DMA; a window cut from a larger image is read in place."""
         torch = self.torch
         if _is_pinned(a):
             return a.to(self.device, non_blocking=True)
-        arr = np.ascontiguousarray(a, dtype=dtype)
-        host = torch.from_numpy(arr)
-        if arr.nbytes >= (1 << 20):
-            host = host.pin_memory()
-        return host.to(self.device, non_blocking=True)
+        arr = np.asarray(a, dtype=dtype)
+        if arr.nbytes < (1 << 20):
+            return torch.from_numpy(np.ascontiguousarray(arr)).to(self.device)
+        if arr.dtype == np.bool_:
+            arr = arr.view(np.uint8)
+        src = torch.from_numpy(arr) if all(st > 0 for st in arr.strides) else \
+            torch.from_numpy(np.ascontiguousarray(arr))
+        stage = torch.empty(tuple(arr.shape), dtype=src.dtype, pin_memory=True)
+        stage.copy_(src)
+        return stage.to(self.device, non_blocking=True)
 
     def _down(self, t):
         """Device tensor into a pinned host tensor on the current stream."""
@@ -516,12 +524,9 @@ class GpuBackend:
         out.copy_(t, non_blocking=True)
         return out
 
-    def solve(self, state, requests: list):
+    def _plan_for(self, requests):
+        """(pool key, builder, channels) of the plan a batch of ``requests`` runs on."""
         key = requests[0].batch_key
-        if key[0] == "tonemap":
-            return self._tonemap(state, requests)
-        if key[0] == "copy":
-            return [self._trivial(r) for r in requests]
         channels = sum(r.channels for r in requests)
         k = slot_count(channels)
         bh, bw = key[1], key[2]
@@ -539,6 +544,15 @@ class GpuBackend:
                 insts = [Instance(bh, bw, "neumann", True) for _ in range(k)]
             return _PooledPlan(self.torch, self.device, pkey, insts, self._params(key[3]))
 
+        return pkey, build, channels
+
+    def solve(self, state, requests: list):
+        key = requests[0].batch_key
+        if key[0] == "tonemap":
+            return self._tonemap(state, requests)
+        if key[0] == "copy":
+            return [self._trivial(r) for r in requests]
+        pkey, build, channels = self._plan_for(requests)
         if not self.resident:
             pp = build()
             try:
@@ -550,6 +564,24 @@ class GpuBackend:
             return self._solve_plan(pp, requests, channels)
         finally:
             self.pool.checkin(pp)
+
+    def warm(self, state, requests: list, copies: int = 1) -> None:
+        """Make ``copies`` resident plans for this batch (built, solved twice so their
+        graphs are captured), so that as many concurrent batches of its key find a
+        ready plan; tone-map batches just run once."""
+        key = requests[0].batch_key
+        if key[0] in ("tonemap", "copy") or not self.resident:
+            self.solve(state, requests)
+            return
+        pkey, build, channels = self._plan_for(requests)
+        plans = [self.pool.checkout(pkey, build) for _ in range(copies)]
+        try:
+            for pp in plans:
+                for _ in range(2):
+                    self._solve_plan(pp, requests, channels)
+        finally:
+            for pp in plans:
+                self.pool.checkin(pp)
 
     def _trivial(self, r):
         img = r.target if isinstance(r, CompositeRequest) else r.image
@@ -632,10 +664,15 @@ class GpuBackend:
         if isinstance(r, PoissonRequest):
             h, w = r.shape
             unk = self._up(r.unknown, np.uint8) if r.boundary == "masked" else None
+            full = (h, w) == tuple(pp.f.shape[1:])
             for q, s in enumerate(slots):
-                pp.f[s].zero_()
                 src = r.f[q]
-                pp.f[s, :h, :w].copy_(self._up(src, np.float64), non_blocking=True)
+                if full and _is_pinned(src):  # straight into the slot
+                    pp.f[s].copy_(src, non_blocking=True)
+                else:
+                    if not full:
+                        pp.f[s].zero_()
+                    pp.f[s, :h, :w].copy_(self._up(src, np.float64), non_blocking=True)
                 if r.boundary == "masked":
                     self._set_mask(pp, s, unk, h, w)
                 elif r.boundary == "dirichlet":
@@ -776,16 +813,21 @@ class PoissonServer:
     def waiting(self) -> int:
         return self._waiting
 
-    def warm(self, requests: list, batch_sizes=(1,)) -> None:
-        """Solve batches of ``b`` copies of each request (for every ``b`` in
-        ``batch_sizes``) twice, so that the plans of the batches the dispatcher
-        will form (hierarchies, buffers, CUDA graphs) exist before traffic."""
+    def warm(self, requests: list, batch_sizes=(1,), copies: int | None = None) -> None:
+        """Prepare the plans of the batches the dispatcher will form: for every request
+        and every ``b`` in ``batch_sizes``, ``copies`` (default: one per worker) resident
+        plans of a batch of ``b`` copies of it, solved twice so that hierarchies,
+        buffers and CUDA graphs exist before traffic arrives."""
         if self._states[0] is None:
             self._states[0] = self.backend.new_worker_state()
+        copies = self.workers if copies is None else copies
         for r in requests:
             for b in batch_sizes:
-                for _ in range(2):  # the second solve captures the plan's graph
-                    self.backend.solve(self._states[0], [r] * b)
+                if hasattr(self.backend, "warm"):
+                    self.backend.warm(self._states[0], [r] * b, copies)
+                else:
+                    for _ in range(2):
+                        self.backend.solve(self._states[0], [r] * b)
 
     # -- lifecycle -----------------------------------------------------------
     def start(self):

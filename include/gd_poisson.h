@@ -258,8 +258,12 @@ int gd_ref_vcycle(double *u_dev, const double *b_dev, int32_t m, int32_t n, doub
  * coarse-level scratch is a GD_STATIC_SCRATCH_BYTES (4 MiB) static device
  * array that every GPU loading this library holds until exit; grids needing
  * more (gd_ref_workspace_bytes > 4 MiB, about 500 x 500 and up) are rejected
- * with GD_ERR_ARG.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * with GD_ERR_ARG (a grid whose hierarchy is a single level, the coarsest solve
+ * in place, uses no scratch and is never rejected).  The first call on a device
+ * that needs the scratch looks up the array's address (cudaGetSymbolAddress)
+ * and keeps it for the life of the process, so make that call before any
+ * stream capture; after cudaDeviceReset on that device the kept address is
+ * stale and the entry point must not be called again.  All calls
  * share the array: calls that overlap on the GPU (different streams or
  * threads) race and must be serialised by the caller.  Nothing is allocated
  * or freed; the coarse iterates are zeroed on every call. */

@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import os
 import sys
+import tempfile
 
 import numpy as np
 import pytest
@@ -11,6 +12,11 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+
+# the tests never read or write the user's autotuner cache: plans built here use the
+# defaults unless a test tunes them into its own file
+os.environ["GD_AUTOTUNE_CACHE"] = os.path.join(
+    tempfile.mkdtemp(prefix="gd_autotune_tests_"), "autotune.json")
 
 
 def pytest_configure(config):

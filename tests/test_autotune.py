@@ -38,15 +38,26 @@ def test_small_gains_and_failures_keep_the_defaults():
     assert best["tile_cells"] == 65536 and best["sweeps"] == 2
 
 
-def test_keys_bucket_size_count_boundary_and_precision():
-    k = autotune.tune_key([Instance(4096, 4096, "neumann", True)] * 3)
-    assert k == "neumann|cells~2^24|n<=4|mixed"
-    assert autotune.tune_key([Instance(1000, 1000)]) == "dirichlet|cells~2^20|n<=1|mixed"
+def test_keys_bucket_size_count_boundary_precision_and_device():
+    k = autotune.tune_key([Instance(4096, 4096, "neumann", True)] * 3, device="B200")
+    assert k == "neumann|cells~2^24|n<=4|mixed|B200"
+    assert autotune.tune_key([Instance(1000, 1000)], device="B200") == \
+        "dirichlet|cells~2^20|n<=1|mixed|B200"
     mixed = autotune.tune_key([Instance(64, 64, "masked"), Instance(128, 128, "neumann")],
-                              SolveParams(precision="fp64"))
-    assert mixed == "masked+neumann|cells~2^14|n<=2|fp64"
+                              SolveParams(precision="fp64"), device="H100")
+    assert mixed == "masked+neumann|cells~2^14|n<=2|fp64|H100"
+    assert autotune.tune_key([Instance(8, 8)]).endswith("|" + autotune.device_name())
     with pytest.raises(ValueError):
         autotune.tune_key([])
+
+
+def test_an_entry_timed_on_another_device_is_ignored(tmp_path):
+    path = str(tmp_path / "tune.json")
+    insts = [Instance(128, 128, "neumann", True)]
+    key = autotune.tune_key(insts)
+    autotune._store(path, key, {"choice": {"sweeps": 3}, "ms": 1.0, "default_ms": 2.0,
+                                "device": "another GPU"})
+    assert autotune.lookup(insts, SolveParams(), path) == SolveParams()
 
 
 def test_cache_round_trip_and_lookup(tmp_path):
@@ -75,7 +86,7 @@ def test_masked_instances_need_masks(tmp_path):
 def test_a_tuned_precision_is_applied():
     got = autotune._apply(SolveParams(), {"sweeps": 1, "precision": "fp64"})
     assert got.precision == "fp64" and got.sweeps == 1
-    assert autotune._apply(SolveParams(), {"precision": "bogus"}).precision == "mixed"
+    assert autotune._apply(SolveParams(), {"precision": "bogus"}).value("precision") == "mixed"
 
 
 def test_resolve_applies_tuned_values_only_where_the_caller_kept_defaults(tmp_path):
@@ -92,6 +103,9 @@ def test_resolve_applies_tuned_values_only_where_the_caller_kept_defaults(tmp_pa
     assert got.tolerance == 1e-6 and got.zero_start
     mine = autotune.resolve(insts, SolveParams(sweeps=1, tile_cells=262144), path)
     assert mine.sweeps == 1 and mine.tile_cells == 262144 and mine.strip_target_warps == 900
+    # an explicit value equal to the default is the caller's choice too
+    same = autotune.resolve(insts, SolveParams(sweeps=2, precision="mixed"), path)
+    assert same.sweeps == 2 and same.precision == "mixed" and same.bottom_cells == 1024
 
 
 def test_untuned_keys_are_read_from_the_file_once(tmp_path, monkeypatch):

@@ -94,6 +94,20 @@ def test_dct_neumann_matches_oracle(shape):
     assert abs(got.mean()) <= 1e-12 * np.abs(got).max()
 
 
+def test_dct_plans_of_different_lengths_coexist():
+    """Binding a plan of short lines after one of long lines leaves the long one
+    usable (the kernels' shared-memory limit is process-wide and never lowered)."""
+    from gradient_domain_b200.solvers import DctPlan
+    rng = np.random.default_rng(5)
+    shapes = [(4096, 24), (24, 4096), (3600, 20), (40, 40), (64, 48)]
+    plans = [DctPlan(*s) for s in shapes]  # long lines bound first, short ones after
+    for plan, shape in zip(plans, shapes):
+        b = rng.standard_normal(shape)
+        bd = torch.as_tensor(b).cuda()
+        got = plan.solve(bd, torch.empty_like(bd)).cpu().numpy()
+        assert _rel(got, osolvers.solve_neumann(b)) <= 1e-12, shape
+
+
 def test_dct_neumann_rejects_sides_beyond_its_line_limit():
     with pytest.raises(ValueError):
         gd.solve_neumann(np.zeros((8193, 4)), method="dct")

@@ -50,8 +50,30 @@ def test_static_vcycle_matches_allocating_vcycle_twice():
         _allocating(expected, b, spacing)
         _static(got, b, spacing)
         torch.cuda.synchronize()
-        err = float((got - expected).abs().max()) / max(float(expected.abs().max()), 1.0)
-        assert err <= 1e-12, (call, err)
+        # the same kernels in the same order: bitwise equal
+        assert torch.equal(got, expected), call
+
+
+def test_single_level_grids_need_no_scratch():
+    """A grid that is already the coarsest (here its short side is coarsest_size) is
+    smoothed in place without scratch, so it is accepted even when the allocating
+    cycle's workspace for it would exceed the static array, and matches that cycle."""
+    dev = _lib.device()
+    m, n, sweeps = 70000, 8, 4
+    assert _lib.lib().gd_ref_workspace_bytes(m, n, 8) > (4 << 20)
+    rng = np.random.default_rng(7)
+    b = torch.as_tensor(rng.standard_normal((m, n))).to(dev)
+    expected, got = torch.zeros_like(b), torch.zeros_like(b)
+    nbytes = int(_lib.lib().gd_ref_workspace_bytes(m, n, 8))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    _lib.check(_lib.lib().gd_ref_vcycle(_lib.ptr(expected), _lib.ptr(b), m, n, 1.0, 2, 2, 8,
+                                        sweeps, _lib.ptr(ws), nbytes, _lib.stream_handle()),
+               "gd_ref_vcycle")
+    _lib.check(_lib.lib().gd_ref_vcycle_static(_lib.ptr(got), _lib.ptr(b), m, n, 1.0, 2, 2, 8,
+                                               sweeps, _lib.stream_handle()),
+               "gd_ref_vcycle_static")
+    torch.cuda.synchronize()
+    assert torch.equal(got, expected)
 
 
 def test_static_vcycle_rejects_grids_beyond_its_scratch():
