@@ -47,7 +47,8 @@ class Params(C.Structure):
                 ("tolerance", C.c_double), ("reliable_delta", C.c_double),
                 ("check_every", C.c_int32), ("use_graph", C.c_int32),
                 ("strip_target_warps", C.c_int32), ("bottom_cells", C.c_int32),
-                ("tile_cells", C.c_int32), ("zero_start", C.c_int32)]
+                ("tile_cells", C.c_int32), ("zero_start", C.c_int32),
+                ("persistent_coarse", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -73,7 +74,7 @@ class KernelTime(C.Structure):
 
 
 KERNEL_KINDS = ("down0", "down", "bottom", "up", "up0", "pupdate", "cgupdate", "fold", "resid",
-                "init", "mean")
+                "init", "mean", "coarse")
 
 
 class GDError(RuntimeError):

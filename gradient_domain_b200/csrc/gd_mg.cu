@@ -22,6 +22,7 @@
 #include <mutex>
 #include <vector>
 
+#include "gd_coarse.cuh"
 #include "gd_stream.cuh"
 #include "gd_tile.cuh"
 
@@ -43,6 +44,12 @@ struct gd_plan_s {
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
          o_xs = 0, o_p0 = 0, o_p1 = 0, o_cnt = 0, o_nact = 0, o_trip = 0, total = 0;
   size_t bottom_smem = 0;
+  // persistent launch of the coarse levels (gd_coarse.cuh): used when the plan has
+  // tile levels below its strips and the device takes cooperative launches
+  bool persistent = false;
+  int coarse_from = 0;   // first level index with no strip launch at or below it
+  int coarse_grid = 0;   // CTAs of the persistent launch (at most one per SM)
+  coarse::Phases phases{};
   char *ws = nullptr;
   bool prepared = false;
   std::vector<char> mask_set;
@@ -210,6 +217,44 @@ struct Runner {
                          (int)st::refresh_smem<T>());
     cudaFuncSetAttribute(st::k_refresh_s<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)st::refresh_smem<T>());
+    cudaFuncSetAttribute(coarse::k_coarse<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)coarse_smem_max<S>());
+  }
+
+  // Shared memory of the persistent coarse launch: the larger of the bottom's
+  // (at most kBottomSmem) and a tile's.
+  template <int S>
+  static constexpr size_t coarse_smem_max() {
+    return std::max<size_t>((size_t)kBottomSmem,
+                            std::max(tile::DownT<T, S>::smem, tile::UpT<T, S>::smem));
+  }
+
+  // The coarse levels and the bottom in one cooperative launch; false when the
+  // launch was refused (the caller then runs them level by level, and the plan
+  // stops using the persistent form).
+  template <int S>
+  static bool launch_coarse(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    const size_t smem = std::max(p->bottom_smem,
+                                 std::max(tile::DownT<T, S>::smem, tile::UpT<T, S>::smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)p->coarse_grid);
+    cfg.blockDim = dim3(kBThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    prof_begin(p, GD_K_COARSE, 0.0, st);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, coarse::k_coarse<T, S>, a, p->phases);
+    prof_end(p, st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p->persistent = false;
+      return false;
+    }
+    return true;
   }
 
   static Args<T> args(gd_plan p) {
@@ -240,51 +285,64 @@ struct Runner {
   }
 
   template <int S>
-  static void vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
-    for (int l = 0; l < p->depth; ++l) {
-      if (p->down_count[l] > 0) {
-        prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
-        st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-            at_tiles(a, p->down_base[l]));
-        prof_end(p, st);
-      }
-      if (p->tdown_count[l] > 0) {
-        prof_begin(p, GD_K_DOWN, p->tile_cells[l], st);
-        if (p->tdown_count[l] < p->sms)
-          tile::k_down_t<T, S, tile::kThreadsSmall>
-              <<<p->tdown_count[l], tile::kThreadsSmall, tile::DownT<T, S>::smem, st>>>(
-                  at_tiles(a, p->tdown_base[l]));
-        else
-          tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
-              at_tiles(a, p->tdown_base[l]));
-        prof_end(p, st);
-      }
-    }
-    prof_begin(p, GD_K_BOTTOM, 0.0, st);
-    k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
-    prof_end(p, st);
-    for (int l = p->depth - 1; l >= 0; --l) {
-      if (p->tup_count[l] > 0) {
-        prof_begin(p, GD_K_UP, p->tile_cells[l], st);
-        if (p->tup_count[l] < p->sms)
-          tile::k_up_t<T, S, tile::kThreadsSmall>
-              <<<p->tup_count[l], tile::kThreadsSmall, tile::UpT<T, S>::smem, st>>>(
-                  at_tiles(a, p->tup_base[l]));
-        else
-          tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
-              at_tiles(a, p->tup_base[l]));
-        prof_end(p, st);
-      }
-      if (p->up_count[l] <= 0) continue;
-      prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
-      if (l == 0)
-        st::k_up_s<T, S, S, true><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-            at_tiles(a, p->up_base[l]));
-      else
-        st::k_up_s<T, S, S, false><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-            at_tiles(a, p->up_base[l]));
+  static void down_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
+    if (p->down_count[l] > 0) {
+      prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
+      st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+          at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
+    if (p->tdown_count[l] > 0) {
+      prof_begin(p, GD_K_DOWN, p->tile_cells[l], st);
+      if (p->tdown_count[l] < p->sms)
+        tile::k_down_t<T, S, tile::kThreadsSmall>
+            <<<p->tdown_count[l], tile::kThreadsSmall, tile::DownT<T, S>::smem, st>>>(
+                at_tiles(a, p->tdown_base[l]));
+      else
+        tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
+            at_tiles(a, p->tdown_base[l]));
+      prof_end(p, st);
+    }
+  }
+
+  template <int S>
+  static void up_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
+    if (p->tup_count[l] > 0) {
+      prof_begin(p, GD_K_UP, p->tile_cells[l], st);
+      if (p->tup_count[l] < p->sms)
+        tile::k_up_t<T, S, tile::kThreadsSmall>
+            <<<p->tup_count[l], tile::kThreadsSmall, tile::UpT<T, S>::smem, st>>>(
+                at_tiles(a, p->tup_base[l]));
+      else
+        tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
+            at_tiles(a, p->tup_base[l]));
+      prof_end(p, st);
+    }
+    if (p->up_count[l] <= 0) return;
+    prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
+    if (l == 0)
+      st::k_up_s<T, S, S, true><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+          at_tiles(a, p->up_base[l]));
+    else
+      st::k_up_s<T, S, S, false><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
+          at_tiles(a, p->up_base[l]));
+    prof_end(p, st);
+  }
+
+  // Levels at and below coarse_from (no strips there) and the bottom go to the
+  // persistent launch when the plan uses it, else one launch per level.
+  template <int S>
+  static void vcycle(gd_plan p, const Args<T> &a, cudaStream_t st) {
+    const int top = p->persistent ? p->coarse_from : p->depth;
+    for (int l = 0; l < top; ++l) down_level<S>(p, a, st, l);
+    if (!(p->persistent && launch_coarse<S>(p, a, st))) {
+      for (int l = top; l < p->depth; ++l) down_level<S>(p, a, st, l);
+      prof_begin(p, GD_K_BOTTOM, 0.0, st);
+      k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
+      prof_end(p, st);
+      for (int l = p->depth - 1; l >= top; --l) up_level<S>(p, a, st, l);
+    }
+    for (int l = top - 1; l >= 0; --l) up_level<S>(p, a, st, l);
   }
 
   // One Krylov iteration; `refresh` false leaves out the FP64 refresh, which
@@ -608,6 +666,35 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     bsm = std::max(bsm, (size_t)bottom_layout(p, p->inst[i].bottom, p->inst[i].coarsest, es,
                                               true));
   p->bottom_smem = bsm;
+  // the persistent coarse launch: tile levels below the last strip level, the
+  // bottom, and the tile levels again on the way up
+  {
+    // below the last strip level, and from the first level whose tiles are fewer
+    // than the SMs (which the per-level path also runs with kBThreads-thread CTAs):
+    // larger tile levels keep their own launch of many smaller CTAs
+    int top = 0;
+    for (int l = 0; l < p->depth; ++l)
+      if (p->down_count[l] > 0 || p->tdown_count[l] >= p->sms) top = l + 1;
+    coarse::Phases ph{};
+    auto add = [&](int kind, int base, int items) {
+      ph.kind[ph.count] = kind;
+      ph.base[ph.count] = base;
+      ph.items[ph.count] = items;
+      ++ph.count;
+    };
+    for (int l = top; l < p->depth; ++l)
+      if (p->tdown_count[l] > 0) add(coarse::kPhaseDown, p->tdown_base[l], p->tdown_count[l]);
+    add(coarse::kPhaseBottom, 0, p->n);
+    for (int l = p->depth - 1; l >= top; --l)
+      if (p->tup_count[l] > 0) add(coarse::kPhaseUp, p->tup_base[l], p->tup_count[l]);
+    int items = 0;
+    for (int q = 0; q < ph.count; ++q) items = std::max(items, ph.items[q]);
+    p->coarse_from = top;
+    p->phases = ph;
+    p->coarse_grid = std::min(p->sms, items);
+    // a single phase (the bottom alone) gains nothing from the persistent form
+    p->persistent = p->persistent && ph.count > 1;
+  }
   p->arena_elems = arena;
   p->code_bytes = std::max<size_t>(codes, kArrayAlign);
   p->dense_elems = std::max<size_t>(dense, 32);
@@ -665,13 +752,17 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   if (p->prm.check_every <= 0) p->prm.check_every = 4;
   if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-4;
   p->fp64 = params->precision == GD_FP64;
+  GD_REQUIRE(params->persistent_coarse == 0 || params->persistent_coarse == 1, GD_ERR_ARG,
+             "gd_plan_create: persistent_coarse must be 0 or 1");
   {
-    int dev = 0, sms = 0;
+    int dev = 0, sms = 0, coop = 0;
     if (cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
         sms > 0)
       p->sms = sms;
-    cudaGetLastError();  // no device (CPU-only build checks): keep the default
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) coop = 0;
+    cudaGetLastError();  // no device (CPU-only build checks): keep the defaults
+    p->persistent = params->persistent_coarse == 1 && coop != 0;
   }
   p->mask_set.assign(n, 0);
   build_plan(p, grids);
@@ -960,7 +1051,13 @@ int enqueue_solve(gd_plan p, cudaStream_t st) {
   const bool graph = p->prm.use_graph && !p->profiling && p->solves >= 1;
   if (graph) {
     if (!p->gexec) {
-      const int rc = build_solve_graph<T>(p, a, fine);
+      int rc = build_solve_graph<T>(p, a, fine);
+      if (rc != GD_OK && p->persistent) {
+        // a graph that cannot hold the cooperative launch: levels one by one
+        cudaGetLastError();
+        p->persistent = false;
+        rc = build_solve_graph<T>(p, a, fine);
+      }
       if (rc != GD_OK) return rc;
     }
     GD_CHECK_CUDA(cudaGraphLaunch(p->gexec, st));
@@ -1004,9 +1101,15 @@ int collect_reports(gd_plan p, gd_report *reports) {
   GD_CHECK_CUDA(cudaEventSynchronize(p->done_ev));
   p->pending = false;
   prof_collect(p);
-  GD_REQUIRE(p->h_nact[1] == 0, GD_ERR_CUDA,
+  const unsigned err = (unsigned)p->h_nact[1];
+  GD_REQUIRE(!(err & bulk::kErrWait), GD_ERR_CUDA,
              "solve: a kernel's bounded wait for its bulk copies gave up (error word %#x); "
-             "the solution is not valid", (unsigned)p->h_nact[1]);
+             "the solution is not valid", err);
+  GD_REQUIRE(!(err & coarse::kErrBarrier), GD_ERR_CUDA,
+             "solve: a grid barrier of the persistent coarse launch gave up (error word %#x); "
+             "the solution is not valid", err);
+  GD_REQUIRE(err == 0, GD_ERR_CUDA, "solve: device error word %#x; the solution is not valid",
+             err);
   for (int i = 0; i < p->n; ++i) {
     const InstState &S = p->h_st[i];
     gd_report &R = reports[i];

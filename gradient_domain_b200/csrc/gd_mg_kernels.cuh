@@ -131,13 +131,13 @@ __device__ __forceinline__ int bot_mirror(int f, int n, bool neu) {
   return f;
 }
 
+// The bottom of one active instance, by the whole CTA (kBThreads threads); the
+// CTA's shared memory is free on entry and may be reused on return.
 template <typename T, int S1, int S2>
-__global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
-  const int inst = blockIdx.x;
+__device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst,
+                                                unsigned char *smem) {
   InstState &S = a.st[inst];
-  if (S.status != GD_ACTIVE) return;
   const InstInfo &I = a.inst[inst];
-  extern __shared__ __align__(16) unsigned char smem[];
   __shared__ T tdiag[kBottomLevels][8], tdinv[kBottomLevels][8];
   const int nb = I.coarsest - I.bottom + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -307,6 +307,14 @@ __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
     part = block_sum<kBThreads>(part);
     if (threadIdx.x == 0) finish_rz(S, part);
   }
+}
+
+// One CTA per instance.
+template <typename T, int S1, int S2>
+__global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
+  if (a.st[blockIdx.x].status != GD_ACTIVE) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  bottom_instance<T, S1, S2>(a, blockIdx.x, smem);
 }
 
 // ---------------------------------------------------------------------------

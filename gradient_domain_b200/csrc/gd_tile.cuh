@@ -141,16 +141,15 @@ __device__ __forceinline__ int tmirror(int f, int n, bool neu) {
 }
 
 // Down on one tile: S1 pre-sweeps from zero, the pre-smoothed iterate to w,
-// residual, restriction (P^T) into the coarse right-hand side.
-template <typename T, int S1, int NT = kThreads>
-__global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
+// residual, restriction (P^T) into the coarse right-hand side.  Called by the
+// whole CTA (NT threads) for an active instance's tile; the CTA's shared
+// memory is free on entry and may be reused on return.
+template <typename T, int S1, int NT>
+__device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, unsigned char *smem) {
   using G = DownT<T, S1>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX;
-  const Tile tl = a.tiles[blockIdx.x];
-  if (a.st[tl.inst].status != GD_ACTIVE) return;
   const LevelInfo L = a.lv[tl.level];
   const LevelInfo Lc = a.lv[L.coarse];
-  extern __shared__ __align__(16) unsigned char smem[];
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
   unsigned *sc = reinterpret_cast<unsigned *>(su + N);
@@ -263,16 +262,14 @@ __global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
 }
 
 // Up on one tile: u = w + P e (bilinear; Neumann clamps at the edge, other
-// boundaries read zero outside), then S2 post-sweeps, colour 1 first.
-template <typename T, int S2, int NT = kThreads>
-__global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
+// boundaries read zero outside), then S2 post-sweeps, colour 1 first.  Same
+// calling convention as down_tile.
+template <typename T, int S2, int NT>
+__device__ __forceinline__ void up_tile(const Args<T> &a, const Tile tl, unsigned char *smem) {
   using G = UpT<T, S2>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX, CX = G::CX;
-  const Tile tl = a.tiles[blockIdx.x];
-  if (a.st[tl.inst].status != GD_ACTIVE) return;
   const LevelInfo L = a.lv[tl.level];
   const LevelInfo Lc = a.lv[L.coarse];
-  extern __shared__ __align__(16) unsigned char smem[];
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
   T *se = su + N;
@@ -389,6 +386,23 @@ __global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
     const int ty = g / TG, q = g - ty * TG;
     store_group(U, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
   }
+}
+
+// One launch per level: a CTA per tile.
+template <typename T, int S1, int NT = kThreads>
+__global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  if (a.st[tl.inst].status != GD_ACTIVE) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  down_tile<T, S1, NT>(a, tl, smem);
+}
+
+template <typename T, int S2, int NT = kThreads>
+__global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
+  const Tile tl = a.tiles[blockIdx.x];
+  if (a.st[tl.inst].status != GD_ACTIVE) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  up_tile<T, S2, NT>(a, tl, smem);
 }
 
 }  // namespace tile

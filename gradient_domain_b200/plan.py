@@ -51,6 +51,7 @@ class SolveParams:
     bottom_cells: int | None = None  # largest level solved inside the one-CTA bottom (0 = 4096)
     tile_cells: int | None = None    # largest coarse level on shared-memory tiles (0 = 262144)
     zero_start: bool = False      # start from x = 0; x is only written (need not be zeroed)
+    persistent_coarse: bool = False  # small coarse levels + bottom in one persistent launch
 
     def value(self, name: str):
         """The field's value, with the library default in place of None."""
@@ -67,7 +68,7 @@ class SolveParams:
                            float(p.reliable_delta), int(p.check_every),
                            1 if p.use_graph else 0, int(p.strip_target_warps),
                            int(p.bottom_cells), int(p.tile_cells),
-                           1 if p.zero_start else 0)
+                           1 if p.zero_start else 0, 1 if p.persistent_coarse else 0)
 
 
 @dataclass(frozen=True)

@@ -80,6 +80,13 @@ typedef struct gd_params {
   int32_t zero_start;         /* nonzero: every solve starts from x = 0 and x is only
                                  written (it need not be initialised), as the
                                  reference's solvers start (solvers.py:143)           */
+  int32_t persistent_coarse;  /* 1: the V-cycle levels below the strips whose tiles are
+                                 fewer than the SMs, the bottom, and those levels again on
+                                 the way up run as one persistent cooperative launch per
+                                 V-cycle, a grid barrier between levels (per-level launches
+                                 where the device or the graph cannot take it); 0 (the
+                                 default): one launch per level, measured faster on the
+                                 B200 inside the solve graph                            */
 } gd_params;
 
 typedef struct gd_report {
@@ -209,7 +216,8 @@ enum gd_kernel_kind {
   GD_K_RESID = 8,   /* FP64 residual refresh and convergence test        */
   GD_K_INIT = 9,    /* right-hand-side mean and initial FP64 residual    */
   GD_K_MEAN = 10,   /* zero-mean projection of Neumann solutions         */
-  GD_KERNEL_KINDS = 11
+  GD_K_COARSE = 11, /* the persistent launch of the coarse levels and bottom */
+  GD_KERNEL_KINDS = 12
 };
 
 typedef struct gd_kernel_time {

@@ -609,3 +609,46 @@ def test_bounded_wait_gives_up_and_reports():
     plan = PoissonPlan([Instance(64, 64, "neumann", True)], SolveParams(zero_start=True))
     (res,) = plan.solve([f], [x], scale=-1.0)
     assert res.converged
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_persistent_coarse_launch_equals_level_launches(precision):
+    """The coarse levels and the bottom in one persistent cooperative launch give
+    bitwise the results of one launch per level (the same per-tile and per-instance
+    device functions run in the same order), on an uneven batch of all boundary
+    types, on direct launches and on the graph of later solves."""
+    rng = np.random.default_rng(17)
+    shapes = [(1100, 900, "neumann"), (700, 1300, "dirichlet"), (600, 640, "masked"),
+              (300, 200, "neumann"), (90, 70, "dirichlet")]
+    yy, xx = np.mgrid[0:600, 0:640]
+    mask = ((yy - 300.0) ** 2 + (xx - 320.0) ** 2 < 260.0 ** 2).astype(np.uint8)
+    rhs = []
+    for h, w, kind in shapes:
+        f = rng.standard_normal((h, w))
+        if kind == "masked":
+            f = np.where(mask, f, 0.0)
+        rhs.append(torch.as_tensor(f).cuda())
+    insts = [Instance(h, w, kind, kind == "neumann") for h, w, kind in shapes]
+    out = {}
+    for mode in (1, 0):
+        plan = PoissonPlan(insts, SolveParams(precision=precision, tolerance=1e-9,
+                                              persistent_coarse=bool(mode), zero_start=True))
+        plan.set_mask(2, torch.as_tensor(mask).cuda())
+        plan.prepare()
+        sols = []
+        for _ in range(2):  # direct launches, then the solve graph
+            x = [torch.empty_like(f) for f in rhs]
+            res = plan.solve(rhs, x, scale=1.0)
+            assert all(r.converged for r in res), res
+            sols.append((x, [r.iterations for r in res]))
+        plan.set_profiling(True)
+        plan.solve(rhs, [torch.empty_like(f) for f in rhs], scale=1.0)
+        kt = plan.kernel_times()
+        assert (kt["coarse"]["launches"] > 0) == (mode == 1)
+        assert (kt["bottom"]["launches"] > 0) == (mode == 0)
+        plan.close()
+        out[mode] = sols
+    for (xa, ia), (xb, ib) in zip(out[0], out[1]):
+        assert ia == ib
+        for a, b in zip(xa, xb):
+            assert torch.equal(a, b)
