@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "active"
 EXPORTS = (
     "gd_last_error", "gd_version", "gd_plan_create", "gd_plan_destroy",
     "gd_plan_workspace_bytes", "gd_plan_bind", "gd_plan_set_mask", "gd_plan_prepare",
-    "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times",
+    "gd_solve", "gd_solve_async", "gd_solve_finish", "gd_plan_apply_vcycle", "gd_plan_set_profiling", "gd_plan_kernel_times", "gd_plan_level_times",
     "gd_ref_workspace_bytes", "gd_ref_vcycle", "gd_ref_vcycle_static", "gd_rbgs_smooth",
     "gd_ref_residual", "gd_ref_dot", "gd_ref_axpby", "gd_ref_restrict", "gd_ref_prolong_add", "gd_gradient", "gd_divergence", "gd_fold_dirichlet",
     "gd_fold_boundary",
@@ -75,6 +75,7 @@ class KernelTime(C.Structure):
 
 KERNEL_KINDS = ("down0", "down", "bottom", "up", "up0", "pupdate", "cgupdate", "fold", "resid",
                 "init", "mean", "coarse")
+PROFILE_LEVELS = 32
 
 
 class GDError(RuntimeError):
@@ -107,6 +108,7 @@ def _declare(lib: C.CDLL) -> None:
         "gd_plan_apply_vcycle": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
         "gd_plan_set_profiling": (C.c_int, [_vp, _i32]),
         "gd_plan_kernel_times": (C.c_int, [_vp, C.POINTER(KernelTime), _i32]),
+        "gd_plan_level_times": (C.c_int, [_vp, C.POINTER(KernelTime), _i32]),
         "gd_selftest_bounded_wait": (C.c_int, [_i32, _vp, _vp, _vp]),
         "gd_ref_workspace_bytes": (_sz, [_i32, _i32, _i32]),
         "gd_ref_vcycle": (C.c_int, [_vp, _vp, _i32, _i32, _f64, _i32, _i32, _i32, _i32, _vp,

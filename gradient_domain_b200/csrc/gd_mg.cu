@@ -68,11 +68,13 @@ struct gd_plan_s {
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<int> ev_kind;
+  std::vector<int> ev_level;
   std::vector<double> ev_cells;
   size_t ev_used = 0;
   double prof_ms[GD_KERNEL_KINDS] = {0};
   double prof_cells[GD_KERNEL_KINDS] = {0};
   long long prof_launches[GD_KERNEL_KINDS] = {0};
+  gd_kernel_time prof_level[GD_KERNEL_KINDS * GD_PROFILE_LEVELS] = {};
   std::vector<double> launch_cells;  // fine cells covered by each launch map
   std::vector<double> tile_cells;    // cells covered by the tile maps of each level
   double fine_cells = 0;
@@ -144,8 +146,9 @@ void capture_stream_put(int device, cudaStream_t s) {
   pools().streams.emplace(device, s);
 }
 
-// Record an event before a launch of `kind` covering `cells` grid cells.
-void prof_begin(gd_plan p, int kind, double cells, cudaStream_t st) {
+// Record an event before a launch of `kind` covering `cells` grid cells of
+// multigrid level `level` (0 for launches not tied to one level).
+void prof_begin(gd_plan p, int kind, double cells, cudaStream_t st, int level = 0) {
   if (!p->profiling) return;
   while (p->ev_pool.size() < p->ev_used + 2) {
     cudaEvent_t e;
@@ -154,9 +157,11 @@ void prof_begin(gd_plan p, int kind, double cells, cudaStream_t st) {
   }
   if (p->ev_kind.size() < p->ev_used + 2) {
     p->ev_kind.resize(p->ev_used + 2);
+    p->ev_level.resize(p->ev_used + 2);
     p->ev_cells.resize(p->ev_used + 2);
   }
   p->ev_kind[p->ev_used] = kind;
+  p->ev_level[p->ev_used] = std::min(std::max(level, 0), GD_PROFILE_LEVELS - 1);
   p->ev_cells[p->ev_used] = cells;
   cudaEventRecord(p->ev_pool[p->ev_used], st);
   p->ev_used += 1;
@@ -178,6 +183,10 @@ void prof_collect(gd_plan p) {
     p->prof_ms[kind] += ms;
     p->prof_cells[kind] += p->ev_cells[k];
     p->prof_launches[kind] += 1;
+    gd_kernel_time &t = p->prof_level[kind * GD_PROFILE_LEVELS + p->ev_level[k]];
+    t.milliseconds += ms;
+    t.cells += p->ev_cells[k];
+    t.launches += 1;
   }
   p->ev_used = 0;
 }
@@ -287,13 +296,13 @@ struct Runner {
   template <int S>
   static void down_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->down_count[l] > 0) {
-      prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st);
+      prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st, l);
       st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
           at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     if (p->tdown_count[l] > 0) {
-      prof_begin(p, GD_K_DOWN, p->tile_cells[l], st);
+      prof_begin(p, GD_K_DOWN, p->tile_cells[l], st, l);
       if (p->tdown_count[l] < p->sms)
         tile::k_down_t<T, S, tile::kThreadsSmall>
             <<<p->tdown_count[l], tile::kThreadsSmall, tile::DownT<T, S>::smem, st>>>(
@@ -308,7 +317,7 @@ struct Runner {
   template <int S>
   static void up_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->tup_count[l] > 0) {
-      prof_begin(p, GD_K_UP, p->tile_cells[l], st);
+      prof_begin(p, GD_K_UP, p->tile_cells[l], st, l);
       if (p->tup_count[l] < p->sms)
         tile::k_up_t<T, S, tile::kThreadsSmall>
             <<<p->tup_count[l], tile::kThreadsSmall, tile::UpT<T, S>::smem, st>>>(
@@ -319,7 +328,7 @@ struct Runner {
       prof_end(p, st);
     }
     if (p->up_count[l] <= 0) return;
-    prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st);
+    prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st, l);
     if (l == 0)
       st::k_up_s<T, S, S, true><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
           at_tiles(a, p->up_base[l]));
@@ -337,7 +346,7 @@ struct Runner {
     for (int l = 0; l < top; ++l) down_level<S>(p, a, st, l);
     if (!(p->persistent && launch_coarse<S>(p, a, st))) {
       for (int l = top; l < p->depth; ++l) down_level<S>(p, a, st, l);
-      prof_begin(p, GD_K_BOTTOM, 0.0, st);
+      prof_begin(p, GD_K_BOTTOM, 0.0, st, p->depth);
       k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
       prof_end(p, st);
       for (int l = p->depth - 1; l >= top; --l) up_level<S>(p, a, st, l);
@@ -1209,6 +1218,7 @@ extern "C" int gd_plan_set_profiling(gd_plan p, int32_t enable) {
     p->prof_cells[k] = 0.0;
     p->prof_launches[k] = 0;
   }
+  for (gd_kernel_time &t : p->prof_level) t = gd_kernel_time{0, 0.0, 0.0};
   p->ev_used = 0;
   return GD_OK;
 }
@@ -1221,6 +1231,14 @@ extern "C" int gd_plan_kernel_times(gd_plan p, gd_kernel_time *out, int32_t n) {
     out[k].milliseconds = p->prof_ms[k];
     out[k].cells = p->prof_cells[k];
   }
+  return GD_OK;
+}
+
+extern "C" int gd_plan_level_times(gd_plan p, gd_kernel_time *out, int32_t n) {
+  GD_REQUIRE(p && out && n >= GD_KERNEL_KINDS * GD_PROFILE_LEVELS, GD_ERR_ARG,
+             "gd_plan_level_times: need room for %d entries",
+             GD_KERNEL_KINDS * GD_PROFILE_LEVELS);
+  std::copy(p->prof_level, p->prof_level + GD_KERNEL_KINDS * GD_PROFILE_LEVELS, out);
   return GD_OK;
 }
 

@@ -148,6 +148,8 @@ def run_load(server, make, count: int, rate: float, seed: int, lookahead: int = 
     built0 = pool.built if pool else 0
     build_s0 = pool.build_s if pool else 0.0
     b0 = server.batches
+    busy0 = getattr(server, "busy_s", 0.0)
+    stages0 = dict(getattr(server.backend, "stage_s", {}))
 
     def consume(fut):
         try:
@@ -189,6 +191,11 @@ def run_load(server, make, count: int, rate: float, seed: int, lookahead: int = 
     extra = {"late_submissions": len(late),
              "late_p99_ms": float(np.percentile(late, 99)) if late else 0.0,
              "failed": len(errors), "first_errors": sorted(set(errors))[:3]}
+    if hasattr(server, "busy_s"):
+        extra["worker_busy"] = round((server.busy_s - busy0) / (server.workers * (t1 - t0)), 3)
+    stages = getattr(server.backend, "stage_s", None)
+    if stages:
+        extra["stage_s"] = {k: round(v - stages0.get(k, 0.0), 3) for k, v in stages.items()}
     if pool:
         extra["plans_built"] = pool.built - built0
         extra["plan_build_s"] = round(pool.build_s - build_s0, 4)

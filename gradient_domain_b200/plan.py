@@ -229,6 +229,21 @@ class PoissonPlan:
         return {name: {"launches": int(out[k].launches), "ms": float(out[k].milliseconds),
                        "cells": float(out[k].cells)} for k, name in enumerate(_lib.KERNEL_KINDS)}
 
+    def level_times(self) -> dict[tuple[str, int], dict]:
+        """The same totals keyed by (kind, multigrid level), launched kinds only."""
+        nl = _lib.PROFILE_LEVELS
+        n = len(_lib.KERNEL_KINDS) * nl
+        out = (_lib.KernelTime * n)()
+        _lib.check(_lib.lib().gd_plan_level_times(self._handle, out, n), "gd_plan_level_times")
+        res = {}
+        for k, name in enumerate(_lib.KERNEL_KINDS):
+            for lvl in range(nl):
+                t = out[k * nl + lvl]
+                if t.launches:
+                    res[(name, lvl)] = {"launches": int(t.launches), "ms": float(t.milliseconds),
+                                        "cells": float(t.cells)}
+        return res
+
     def close(self) -> None:
         if getattr(self, "_handle", None):
             # only this plan's stream can still use its workspace

@@ -449,6 +449,16 @@ class GpuBackend:
         self.resident = resident
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.pool = PlanPool()
+        # seconds the workers spent per stage, summed over batches: host staging and
+        # launches of the inputs / fields / right-hand sides, the solve (until its
+        # results are on the host), composition and copies down (until the stream
+        # is idle), and whole tone-map batches
+        self.stage_s = {"prepare": 0.0, "solve": 0.0, "finish": 0.0, "tonemap": 0.0}
+        self._stage_lock = threading.Lock()
+
+    def _stage(self, name: str, seconds: float) -> None:
+        with self._stage_lock:
+            self.stage_s[name] += seconds
 
     # -- memory ----------------------------------------------------------------
     def memory_budget(self, fraction: float) -> int:
@@ -593,6 +603,7 @@ class GpuBackend:
         from .hdr import tone_map_device
         stream = state["stream"]
         outs = []
+        t0 = time.perf_counter()
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
             for r in requests:
                 rad = self._up(r.radiance, np.float64)
@@ -601,6 +612,7 @@ class GpuBackend:
                 img, factor = tone_map_device(rad, r.config, dct)
                 outs.append((self._down(img), self._down(factor) if r.return_factor else None))
             stream.synchronize()
+        self._stage("tonemap", time.perf_counter() - t0)
         res = []
         for img, factor in outs:
             extra = {"factor": factor.numpy()} if factor is not None else {}
@@ -614,6 +626,7 @@ class GpuBackend:
         lib, st = _lib.lib(), None
         k, bh, bw = pp.f.shape
         posts = []  # per request: a function of the solutions that gives its result
+        t0 = time.perf_counter()
         with torch.cuda.device(self.device), torch.cuda.stream(pp.stream):
             st = _lib.stream_handle(pp.stream)
             slot = 0
@@ -628,9 +641,15 @@ class GpuBackend:
                     self._set_rect(pp, s, 0, 0)
             if pp.masked:
                 pp.plan.prepare()
+            t1 = time.perf_counter()
             results = pp.plan.solve(list(pp.f), list(pp.x), scale=1.0)
+            t2 = time.perf_counter()
             outs = [post() for _, _, post in posts]
             pp.stream.synchronize()
+        t3 = time.perf_counter()
+        self._stage("prepare", t1 - t0)
+        self._stage("solve", t2 - t1)
+        self._stage("finish", t3 - t2)
         per = []
         for (r, slots, _), out in zip(posts, outs):
             per.append((out.numpy() if hasattr(out, "numpy") else out,
@@ -783,6 +802,7 @@ class PoissonServer:
         self.batches = 0
         self.max_concurrent = 0
         self._active_batches = 0
+        self.busy_s = 0.0  # worker seconds spent running batches
 
     # -- client side ---------------------------------------------------------
     def submit(self, request, submitted: float | None = None) -> Future:
@@ -984,6 +1004,7 @@ class PoissonServer:
                     job.future.set_exception(exc)
         finally:
             with self._cv:
+                self.busy_s += time.perf_counter() - started
                 self.in_use -= sum(j.request.footprint for j in batch)
                 self._idle.append(wid)
                 self._active_batches -= 1

@@ -233,6 +233,13 @@ int gd_plan_set_profiling(gd_plan plan, int32_t enable);
 /* Per-kind totals since gd_plan_set_profiling; out has GD_KERNEL_KINDS entries. */
 int gd_plan_kernel_times(gd_plan plan, gd_kernel_time *out, int32_t n);
 
+/* The same totals split by multigrid level: out[kind * GD_PROFILE_LEVELS + level]
+ * (n >= GD_KERNEL_KINDS * GD_PROFILE_LEVELS).  Level-wise kinds (down, up, their
+ * level-0 forms) use the level they run on, the bottom uses the deepest level
+ * above it, and the Krylov, refresh, init, mean and persistent kinds level 0. */
+#define GD_PROFILE_LEVELS 32
+int gd_plan_level_times(gd_plan plan, gd_kernel_time *out, int32_t n);
+
 /* Self-test of the bounded waits (no counterpart in the reference).  The
  * streaming kernels wait for their bulk copies on mbarriers with a limit; a
  * wait that gives up sets bit 0 of an error word (a solve then fails with
