@@ -48,7 +48,7 @@ class Params(C.Structure):
                 ("check_every", C.c_int32), ("use_graph", C.c_int32),
                 ("strip_target_warps", C.c_int32), ("bottom_cells", C.c_int32),
                 ("tile_cells", C.c_int32), ("zero_start", C.c_int32),
-                ("persistent_coarse", C.c_int32)]
+                ("persistent_coarse", C.c_int32), ("dependent_launch", C.c_int32)]
 
 
 class Report(C.Structure):

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "gd_coarse.cuh"
@@ -47,6 +48,7 @@ struct gd_plan_s {
   // persistent launch of the coarse levels (gd_coarse.cuh): used when the plan has
   // tile levels below its strips and the device takes cooperative launches
   bool persistent = false;
+  bool dependent_launch = false;  // chain_launch: programmatic dependent launches
   int coarse_from = 0;   // first level index with no strip launch at or below it
   int coarse_grid = 0;   // CTAs of the persistent launch (at most one per SM)
   coarse::Phases phases{};
@@ -191,6 +193,27 @@ void prof_collect(gd_plan p) {
   p->ev_used = 0;
 }
 
+// Launch of a kernel of the solve chain.  With the plan's dependent-launch
+// flag the launch carries the programmatic-serialization attribute: the
+// kernel may be scheduled while the one ahead of it is finishing and waits for
+// it inside (dep_wait), so the launch gap and the kernel's table reads overlap
+// the previous kernel's tail.  Errors are left for cudaGetLastError.
+template <typename... KP, typename... AT>
+void chain_launch(gd_plan p, void (*kernel)(KP...), int grid, int block, size_t smem,
+                  cudaStream_t st, AT &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = p->dependent_launch ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<AT>(args)...);
+}
+
 // Strip geometry of the down / up kernels for a plan's precision and sweeps.
 template <typename T, int S>
 struct StripCfg {
@@ -297,19 +320,19 @@ struct Runner {
   static void down_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->down_count[l] > 0) {
       prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st, l);
-      st::k_down_s<T, S><<<p->down_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-          at_tiles(a, p->down_base[l]));
+      chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kThreads, st::level_smem<T>(),
+                   st, at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     if (p->tdown_count[l] > 0) {
       prof_begin(p, GD_K_DOWN, p->tile_cells[l], st, l);
       if (p->tdown_count[l] < p->sms)
-        tile::k_down_t<T, S, tile::kThreadsSmall>
-            <<<p->tdown_count[l], tile::kThreadsSmall, tile::DownT<T, S>::smem, st>>>(
-                at_tiles(a, p->tdown_base[l]));
+        chain_launch(p, tile::k_down_t<T, S, tile::kThreadsSmall>, p->tdown_count[l],
+                     tile::kThreadsSmall, tile::DownT<T, S>::smem, st,
+                     at_tiles(a, p->tdown_base[l]));
       else
-        tile::k_down_t<T, S><<<p->tdown_count[l], tile::kThreads, tile::DownT<T, S>::smem, st>>>(
-            at_tiles(a, p->tdown_base[l]));
+        chain_launch(p, tile::k_down_t<T, S>, p->tdown_count[l], tile::kThreads,
+                     tile::DownT<T, S>::smem, st, at_tiles(a, p->tdown_base[l]));
       prof_end(p, st);
     }
   }
@@ -319,22 +342,21 @@ struct Runner {
     if (p->tup_count[l] > 0) {
       prof_begin(p, GD_K_UP, p->tile_cells[l], st, l);
       if (p->tup_count[l] < p->sms)
-        tile::k_up_t<T, S, tile::kThreadsSmall>
-            <<<p->tup_count[l], tile::kThreadsSmall, tile::UpT<T, S>::smem, st>>>(
-                at_tiles(a, p->tup_base[l]));
+        chain_launch(p, tile::k_up_t<T, S, tile::kThreadsSmall>, p->tup_count[l],
+                     tile::kThreadsSmall, tile::UpT<T, S>::smem, st, at_tiles(a, p->tup_base[l]));
       else
-        tile::k_up_t<T, S><<<p->tup_count[l], tile::kThreads, tile::UpT<T, S>::smem, st>>>(
-            at_tiles(a, p->tup_base[l]));
+        chain_launch(p, tile::k_up_t<T, S>, p->tup_count[l], tile::kThreads,
+                     tile::UpT<T, S>::smem, st, at_tiles(a, p->tup_base[l]));
       prof_end(p, st);
     }
     if (p->up_count[l] <= 0) return;
     prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st, l);
     if (l == 0)
-      st::k_up_s<T, S, S, true><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-          at_tiles(a, p->up_base[l]));
+      chain_launch(p, st::k_up_s<T, S, S, true>, p->up_count[l], st::kThreads,
+                   st::level_smem<T>(), st, at_tiles(a, p->up_base[l]));
     else
-      st::k_up_s<T, S, S, false><<<p->up_count[l], st::kThreads, st::level_smem<T>(), st>>>(
-          at_tiles(a, p->up_base[l]));
+      chain_launch(p, st::k_up_s<T, S, S, false>, p->up_count[l], st::kThreads,
+                   st::level_smem<T>(), st, at_tiles(a, p->up_base[l]));
     prof_end(p, st);
   }
 
@@ -347,7 +369,7 @@ struct Runner {
     if (!(p->persistent && launch_coarse<S>(p, a, st))) {
       for (int l = top; l < p->depth; ++l) down_level<S>(p, a, st, l);
       prof_begin(p, GD_K_BOTTOM, 0.0, st, p->depth);
-      k_bottom<T, S, S><<<p->n, kBThreads, p->bottom_smem, st>>>(a);
+      chain_launch(p, k_bottom<T, S, S>, p->n, kBThreads, p->bottom_smem, st, a);
       prof_end(p, st);
       for (int l = p->depth - 1; l >= top; --l) up_level<S>(p, a, st, l);
     }
@@ -362,18 +384,20 @@ struct Runner {
     const Args<T> f = at_tiles(a, p->fine_base);
     const double c = p->fine_cells;
     prof_begin(p, GD_K_PUPDATE, c, st);
-    st::k_pupdate_s<T><<<p->fine_count, st::kThreads, st::pupdate_smem<T>(), st>>>(f);
+    chain_launch(p, st::k_pupdate_s<T>, p->fine_count, st::kThreads, st::pupdate_smem<T>(), st,
+                 f);
     prof_end(p, st);
     prof_begin(p, GD_K_CGUPDATE, c, st);
-    st::k_cgupdate_s<T><<<p->fine_count, st::kThreads, st::cgupdate_smem<T>(), st>>>(f);
+    chain_launch(p, st::k_cgupdate_s<T>, p->fine_count, st::kThreads, st::cgupdate_smem<T>(),
+                 st, f);
     prof_end(p, st);
     if (refresh) launch_refresh(p, a, st);
   }
 
   static void launch_refresh(gd_plan p, const Args<T> &a, cudaStream_t st) {
     prof_begin(p, GD_K_RESID, p->fine_cells, st);
-    st::k_refresh_s<T, false><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(
-        at_tiles(a, p->fine_base));
+    chain_launch(p, st::k_refresh_s<T, false>, p->fine_count, st::kThreads,
+                 st::refresh_smem<T>(), st, at_tiles(a, p->fine_base));
     prof_end(p, st);
   }
 
@@ -747,6 +771,10 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
              "gd_plan_create: negative bottom_cells / tile_cells");
   GD_REQUIRE(params->max_iterations >= 0 && params->tolerance >= 0.0, GD_ERR_ARG,
              "gd_plan_create: bad tolerance / iteration budget");
+  GD_REQUIRE(params->persistent_coarse == 0 || params->persistent_coarse == 1, GD_ERR_ARG,
+             "gd_plan_create: persistent_coarse must be 0 or 1");
+  GD_REQUIRE(params->dependent_launch == 0 || params->dependent_launch == 1, GD_ERR_ARG,
+             "gd_plan_create: dependent_launch must be 0 or 1");
   for (int i = 0; i < n; ++i) {
     GD_REQUIRE(grids[i].height > 0 && grids[i].width > 0, GD_ERR_ARG,
                "gd_plan_create: instance %d has an empty grid", i);
@@ -761,8 +789,7 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
   if (p->prm.check_every <= 0) p->prm.check_every = 4;
   if (p->prm.reliable_delta <= 0.0) p->prm.reliable_delta = 1e-4;
   p->fp64 = params->precision == GD_FP64;
-  GD_REQUIRE(params->persistent_coarse == 0 || params->persistent_coarse == 1, GD_ERR_ARG,
-             "gd_plan_create: persistent_coarse must be 0 or 1");
+  p->dependent_launch = params->dependent_launch == 1;
   {
     int dev = 0, sms = 0, coop = 0;
     if (cudaGetDevice(&dev) == cudaSuccess &&
@@ -901,8 +928,9 @@ __global__ void k_refresh_gate(cudaGraphConditionalHandle h, const InstState *st
 template <typename T>
 void launch_init(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_INIT, p->fine_cells, st);
-  k_fmean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  st::k_refresh_s<T, true><<<p->fine_count, st::kThreads, st::refresh_smem<T>(), st>>>(fine);
+  chain_launch(p, k_fmean<T>, p->fine_count, kFThreads, 0, st, fine);
+  chain_launch(p, st::k_refresh_s<T, true>, p->fine_count, st::kThreads, st::refresh_smem<T>(),
+               st, fine);
   prof_end(p, st);
 }
 
@@ -922,8 +950,8 @@ template <typename T>
 void launch_finish(gd_plan p, const Args<T> &fine, cudaStream_t st) {
   prof_begin(p, GD_K_MEAN, p->fine_cells, st);
   if (plan_any_mean(p) && !p->prm.zero_start)
-    k_mean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
-  k_submean<T><<<p->fine_count, kFThreads, 0, st>>>(fine);
+    chain_launch(p, k_mean<T>, p->fine_count, kFThreads, 0, st, fine);
+  chain_launch(p, k_submean<T>, p->fine_count, kFThreads, 0, st, fine);
   prof_end(p, st);
 }
 

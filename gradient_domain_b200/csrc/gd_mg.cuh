@@ -37,6 +37,23 @@ enum : int { FLAG_RU = 1, FLAG_DZERO = 2 };
 // by a kernel whose bounded wait gave up, cleared when a solve starts.
 constexpr int kErrWord = 15;
 
+// Programmatic dependent launch.  The kernels of a solve may be launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, which lets their CTAs be
+// scheduled before the kernel ahead of them in the stream has finished.  Such a
+// kernel reads only the plan's tables that no kernel writes (the tile lists and
+// the level descriptors) before dep_wait(), which returns once the kernel
+// ahead has completed and its writes are visible; then dep_release() lets the
+// next kernel's CTAs be scheduled in turn.  Without the attribute both are
+// no-ops.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void dep_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void dep_enter() {
+  dep_wait();
+  dep_release();
+}
+
 struct LevelInfo {
   int ny, nx, pitch, inst;
   int bc, level, coarse, is_bottom;

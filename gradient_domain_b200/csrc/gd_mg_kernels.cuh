@@ -312,6 +312,7 @@ __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst
 // One CTA per instance.
 template <typename T, int S1, int S2>
 __global__ void __launch_bounds__(kBThreads, 1) k_bottom(Args<T> a) {
+  dep_enter();
   if (a.st[blockIdx.x].status != GD_ACTIVE) return;
   extern __shared__ __align__(16) unsigned char smem[];
   bottom_instance<T, S1, S2>(a, blockIdx.x, smem);
@@ -348,6 +349,7 @@ __device__ __forceinline__ double column_sum(const double *A, long long pitch, i
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_fmean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   if (blockIdx.x == 0 && threadIdx.x == 0) a.counter[kErrWord] = 0u;  // a solve starts
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
@@ -370,6 +372,7 @@ __global__ void __launch_bounds__(kFThreads) k_fmean(Args<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   const InstInfo &I = a.inst[tl.inst];
   double part = 0.0;
   // only solutions no refresh has summed: a caller's x that met the tolerance at once
@@ -399,6 +402,7 @@ __global__ void __launch_bounds__(kFThreads) k_mean(Args<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(kFThreads) k_submean(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   const InstInfo &Ig = a.inst[tl.inst];
   const bool own = a.st[tl.inst].xcur != 0;
   const bool xz = a.st[tl.inst].xzero != 0;

@@ -511,10 +511,11 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_down_s(Arg
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
-  if (a.st[tl.inst].status != GD_ACTIVE) return;
   const LevelInfo L = a.lv[tl.level];
-  fill_table(tab, L.wall);
   const LevelInfo Lc = a.lv[L.coarse];
+  dep_enter();
+  if (a.st[tl.inst].status != GD_ACTIVE) return;
+  fill_table(tab, L.wall);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int RB = L.rows_per_warp;  // even
   const int y_out0 = (tl.ty * kWarps + warp) * RB;
@@ -713,12 +714,13 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) k_up_s(Args<
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
+  const LevelInfo L = a.lv[tl.level];
+  const LevelInfo Lc = a.lv[L.coarse];
+  dep_enter();
   const bool active = a.st[tl.inst].status == GD_ACTIVE;
   double part = 0.0;
   if (active) {
-    const LevelInfo L = a.lv[tl.level];
     fill_table(tab, L.wall);
-    const LevelInfo Lc = a.lv[L.coarse];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int RB = L.rows_per_warp;
     const int y_out0 = (tl.ty * kWarps + warp) * RB;
@@ -845,6 +847,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_pupdate_s(Args<T> a) {
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   const bool active = a.st[tl.inst].status == GD_ACTIVE;
   double part = 0.0;
   if (active) {
@@ -982,6 +985,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_cgupdate_s(Args<T> a) {
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   const bool active = a.st[tl.inst].status == GD_ACTIVE;
   double part = 0.0;
   if (active) {
@@ -1403,6 +1407,7 @@ __device__ __forceinline__ void init_zero_rows(const RefWarp<T> &w, double &part
 template <typename T, bool INIT>
 __global__ void __launch_bounds__(kThreads, 4) k_refresh_s(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   const int flags = a.st[tl.inst].flags;
   const bool work = INIT || (flags & FLAG_RU);
   double part = 0.0, part_f = 0.0;

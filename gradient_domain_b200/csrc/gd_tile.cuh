@@ -392,6 +392,7 @@ __device__ __forceinline__ void up_tile(const Args<T> &a, const Tile tl, unsigne
 template <typename T, int S1, int NT = kThreads>
 __global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   extern __shared__ __align__(16) unsigned char smem[];
   down_tile<T, S1, NT>(a, tl, smem);
@@ -400,6 +401,7 @@ __global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
 template <typename T, int S2, int NT = kThreads>
 __global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  dep_enter();
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   extern __shared__ __align__(16) unsigned char smem[];
   up_tile<T, S2, NT>(a, tl, smem);

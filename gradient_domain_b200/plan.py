@@ -52,6 +52,7 @@ class SolveParams:
     tile_cells: int | None = None    # largest coarse level on shared-memory tiles (0 = 262144)
     zero_start: bool = False      # start from x = 0; x is only written (need not be zeroed)
     persistent_coarse: bool = False  # small coarse levels + bottom in one persistent launch
+    dependent_launch: bool = False   # kernels launched as programmatic dependents
 
     def value(self, name: str):
         """The field's value, with the library default in place of None."""
@@ -68,7 +69,8 @@ class SolveParams:
                            float(p.reliable_delta), int(p.check_every),
                            1 if p.use_graph else 0, int(p.strip_target_warps),
                            int(p.bottom_cells), int(p.tile_cells),
-                           1 if p.zero_start else 0, 1 if p.persistent_coarse else 0)
+                           1 if p.zero_start else 0, 1 if p.persistent_coarse else 0,
+                           1 if p.dependent_launch else 0)
 
 
 @dataclass(frozen=True)

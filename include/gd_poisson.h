@@ -87,6 +87,11 @@ typedef struct gd_params {
                                  where the device or the graph cannot take it); 0 (the
                                  default): one launch per level, measured faster on the
                                  B200 inside the solve graph                            */
+  int32_t dependent_launch;   /* 1: the kernels of a solve are launched as programmatic
+                                 dependents of the kernel ahead of them (each waits for it
+                                 inside), so a launch and its table reads may overlap the
+                                 previous kernel's tail; 0 (the default): plain stream
+                                 order, measured faster on the B200 inside the solve graph */
 } gd_params;
 
 typedef struct gd_report {

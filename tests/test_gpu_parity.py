@@ -652,3 +652,47 @@ def test_persistent_coarse_launch_equals_level_launches(precision):
         assert ia == ib
         for a, b in zip(xa, xb):
             assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_dependent_launch_equals_serial_launch(precision):
+    """Kernels launched as programmatic dependents (each waits for the one ahead
+    before it touches the plan's mutable state) give bitwise the results of plain
+    stream order, on an uneven batch of all boundary types, on direct launches,
+    on the solve graph, with the persistent coarse launch and on the profiled path."""
+    rng = np.random.default_rng(23)
+    shapes = [(1030, 770, "neumann"), (513, 1201, "dirichlet"), (600, 640, "masked"),
+              (257, 129, "neumann"), (40, 72, "dirichlet")]
+    yy, xx = np.mgrid[0:600, 0:640]
+    mask = ((yy - 300.0) ** 2 + (xx - 320.0) ** 2 < 250.0 ** 2).astype(np.uint8)
+    rhs = []
+    for h, w, kind in shapes:
+        f = rng.standard_normal((h, w))
+        if kind == "masked":
+            f = np.where(mask, f, 0.0)
+        rhs.append(torch.as_tensor(f).cuda())
+    insts = [Instance(h, w, kind, kind == "neumann") for h, w, kind in shapes]
+    out = {}
+    for dep in (True, False):
+        for persistent in (False, True):
+            plan = PoissonPlan(insts, SolveParams(precision=precision, tolerance=1e-9,
+                                                  dependent_launch=dep,
+                                                  persistent_coarse=persistent,
+                                                  zero_start=True))
+            plan.set_mask(2, torch.as_tensor(mask).cuda())
+            plan.prepare()
+            sols = []
+            for profiled in (False, False, False, True):  # direct, graph, graph, profiled
+                plan.set_profiling(profiled)
+                x = [torch.empty_like(f) for f in rhs]
+                res = plan.solve(rhs, x, scale=1.0)
+                assert all(r.converged for r in res), res
+                sols.append((x, [r.iterations for r in res]))
+            plan.close()
+            out[(dep, persistent)] = sols
+    ref = out[(False, False)]
+    for key, sols in out.items():
+        for (xa, ia), (xb, ib) in zip(ref, sols):
+            assert ia == ib, key
+            for a, b in zip(xa, xb):
+                assert torch.equal(a, b), key

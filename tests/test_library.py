@@ -52,3 +52,17 @@ def test_smoother_argument_checks_run_on_the_host():
     for sweeps in (0, 5, -1):
         assert fn(u, out, b, 8, 8, 8, 0, 1.0, sweeps, None) == -1
         assert b"sweeps" in _lib.lib().gd_last_error()
+
+
+def test_plan_flags_are_checked_on_the_host():
+    """gd_plan_create rejects launch-mode flags outside {0, 1} before it allocates
+    anything or touches a device."""
+    from gradient_domain_b200.plan import SolveParams
+    grids = (_lib.GridDesc * 1)(_lib.GridDesc(64, 64, _lib.GD_NEUMANN, 1))
+    out = ctypes.c_void_p()
+    for field in ("dependent_launch", "persistent_coarse"):
+        prm = SolveParams(zero_start=True).c_params()
+        setattr(prm, field, 2)
+        rc = _lib.lib().gd_plan_create(grids, 1, ctypes.byref(prm), ctypes.byref(out))
+        assert rc == -1 and not out.value
+        assert field.encode() in _lib.lib().gd_last_error()
