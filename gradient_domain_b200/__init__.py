@@ -20,15 +20,17 @@ from .poisson import (
     solve_masked,
     texture_flatten,
 )
-from .solvers import SOLVERS, SolverReport, solve_neumann, solve_neumann_batch, solve_system
+from .solvers import (SOLVERS, NeumannBatchFuture, SolverReport, solve_neumann,
+                      solve_neumann_batch, solve_neumann_batch_async, solve_system)
 
 __all__ = [
     "SOLVERS", "BenchmarkRecord", "BenchmarkTable", "GuidanceField", "Instance",
-    "MultigridOptions", "MultigridReport", "PoissonPlan", "SolveParams", "SolverReport",
+    "MultigridOptions", "MultigridReport", "NeumannBatchFuture", "PoissonPlan", "SolveParams",
+    "SolverReport",
     "ToneMapConfig", "attenuation_field", "cached_plan", "divergence", "fold_boundary",
     "gradient", "illumination_change", "laplacian", "manufactured_problem", "seamless_clone",
     "solve", "solve_dirichlet", "solve_masked", "solve_neumann", "solve_neumann_batch",
-    "solve_system",
+    "solve_neumann_batch_async", "solve_system",
     "smooth", "solver_scaling", "sparse_laplacian", "texture_flatten", "tone_map", "v_cycle",
 ]
 

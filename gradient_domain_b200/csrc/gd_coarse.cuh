@@ -5,7 +5,8 @@
 // the one-CTA bottom of every instance, the tile levels on the way up - is a
 // phase whose work items (tiles of every instance at that level, or
 // instances) are independent of each other but depend on the previous phase.
-// One cooperative launch of one CTA per SM walks the phases: each CTA takes
+// One cooperative launch of one CTA per SM walks the phases (every tile level
+// here has the small tile shape): each CTA takes
 // the phase's items round-robin, then all CTAs meet at a grid barrier before
 // the next phase.  This replaces one launch per phase (2 x tile levels + 1) and
 // its launch gap and tail; the work of every item is the same device function
@@ -81,9 +82,13 @@ __global__ void __launch_bounds__(kBThreads, 1) k_coarse(Args<T> a, Phases ph) {
         if (a.st[k].status == GD_ACTIVE) bottom_instance<T, S, S>(a, k, smem);
       } else {
         const Tile tl = a.tiles[ph.base[q] + k];
+        const LevelInfo L = a.lv[tl.level];
+        const LevelInfo Lc = a.lv[tl.level + 1];
         if (a.st[tl.inst].status != GD_ACTIVE) continue;
-        if (kind == kPhaseDown) tile::down_tile<T, S, kBThreads>(a, tl, smem);
-        else tile::up_tile<T, S, kBThreads>(a, tl, smem);
+        if (kind == kPhaseDown)
+          tile::down_tile<T, S, kBThreads, tile::kTYs, tile::kTXs>(a, tl, L, Lc, smem);
+        else
+          tile::up_tile<T, S, kBThreads, tile::kTYs, tile::kTXs>(a, tl, L, Lc, smem);
       }
     }
   }

@@ -40,6 +40,7 @@ struct gd_plan_s {
   int fine_base = 0, fine_count = 0, depth = 0;
   std::vector<int> down_base, down_count, up_base, up_count;     // strip maps per level
   std::vector<int> tdown_base, tdown_count, tup_base, tup_count;  // tile maps per level
+  std::vector<char> tsmall;  // per level: tiles of the small shape (fewer large tiles than SMs)
   size_t arena_elems = 0, code_bytes = 0, dense_elems = 0, xs_elems = 0;
   int max_partials = 1;
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
@@ -237,10 +238,10 @@ struct Runner {
                          (int)tile::DownT<T, S>::smem);
     cudaFuncSetAttribute(tile::k_up_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)tile::UpT<T, S>::smem);
-    cudaFuncSetAttribute(tile::k_down_t<T, S, tile::kThreadsSmall>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile::DownT<T, S>::smem);
-    cudaFuncSetAttribute(tile::k_up_t<T, S, tile::kThreadsSmall>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile::UpT<T, S>::smem);
+    cudaFuncSetAttribute(small_down<S>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)SmallDown<S>::smem);
+    cudaFuncSetAttribute(small_up<S>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)SmallUp<S>::smem);
     cudaFuncSetAttribute(st::k_pupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)st::pupdate_smem<T>());
     cudaFuncSetAttribute(st::k_cgupdate_s<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -253,12 +254,26 @@ struct Runner {
                          (int)coarse_smem_max<S>());
   }
 
-  // Shared memory of the persistent coarse launch: the larger of the bottom's
-  // (at most kBottomSmem) and a tile's.
+  // Small-tile forms of the tile kernels (levels with fewer large tiles than SMs).
+  template <int S>
+  using SmallDown = tile::DownT<T, S, tile::kTYs, tile::kTXs>;
+  template <int S>
+  using SmallUp = tile::UpT<T, S, tile::kTYs, tile::kTXs>;
+  template <int S>
+  static constexpr auto small_down() {
+    return tile::k_down_t<T, S, tile::kThreadsSmall, tile::kTYs, tile::kTXs>;
+  }
+  template <int S>
+  static constexpr auto small_up() {
+    return tile::k_up_t<T, S, tile::kThreadsSmall, tile::kTYs, tile::kTXs>;
+  }
+
+  // Shared memory of the persistent coarse launch (whose tile levels are all
+  // small-tile levels): the larger of the bottom's (at most kBottomSmem) and a
+  // small tile's.
   template <int S>
   static constexpr size_t coarse_smem_max() {
-    return std::max<size_t>((size_t)kBottomSmem,
-                            std::max(tile::DownT<T, S>::smem, tile::UpT<T, S>::smem));
+    return std::max<size_t>((size_t)kBottomSmem, std::max(SmallDown<S>::smem, SmallUp<S>::smem));
   }
 
   // The coarse levels and the bottom in one cooperative launch; false when the
@@ -266,8 +281,7 @@ struct Runner {
   // stops using the persistent form).
   template <int S>
   static bool launch_coarse(gd_plan p, const Args<T> &a, cudaStream_t st) {
-    const size_t smem = std::max(p->bottom_smem,
-                                 std::max(tile::DownT<T, S>::smem, tile::UpT<T, S>::smem));
+    const size_t smem = std::max(p->bottom_smem, std::max(SmallDown<S>::smem, SmallUp<S>::smem));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)p->coarse_grid);
     cfg.blockDim = dim3(kBThreads);
@@ -326,10 +340,9 @@ struct Runner {
     }
     if (p->tdown_count[l] > 0) {
       prof_begin(p, GD_K_DOWN, p->tile_cells[l], st, l);
-      if (p->tdown_count[l] < p->sms)
-        chain_launch(p, tile::k_down_t<T, S, tile::kThreadsSmall>, p->tdown_count[l],
-                     tile::kThreadsSmall, tile::DownT<T, S>::smem, st,
-                     at_tiles(a, p->tdown_base[l]));
+      if (p->tsmall[l])
+        chain_launch(p, small_down<S>(), p->tdown_count[l], tile::kThreadsSmall,
+                     SmallDown<S>::smem, st, at_tiles(a, p->tdown_base[l]));
       else
         chain_launch(p, tile::k_down_t<T, S>, p->tdown_count[l], tile::kThreads,
                      tile::DownT<T, S>::smem, st, at_tiles(a, p->tdown_base[l]));
@@ -341,9 +354,9 @@ struct Runner {
   static void up_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->tup_count[l] > 0) {
       prof_begin(p, GD_K_UP, p->tile_cells[l], st, l);
-      if (p->tup_count[l] < p->sms)
-        chain_launch(p, tile::k_up_t<T, S, tile::kThreadsSmall>, p->tup_count[l],
-                     tile::kThreadsSmall, tile::UpT<T, S>::smem, st, at_tiles(a, p->tup_base[l]));
+      if (p->tsmall[l])
+        chain_launch(p, small_up<S>(), p->tup_count[l], tile::kThreadsSmall, SmallUp<S>::smem,
+                     st, at_tiles(a, p->tup_base[l]));
       else
         chain_launch(p, tile::k_up_t<T, S>, p->tup_count[l], tile::kThreads,
                      tile::UpT<T, S>::smem, st, at_tiles(a, p->tup_base[l]));
@@ -578,6 +591,8 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       const long long cells = (long long)ny * nx;
       L.is_bottom = 0;
       const bool coarsest = cells <= kCoarsestCells;
+      // the coarse level is always the next table entry; the smoothing kernels read
+      // it as lv[level + 1] together with the level's own entry
       L.coarse = coarsest ? -1 : (int)p->lv.size() + 1;
       if (coarsest) {
         L.inv_off = (long long)dense;
@@ -639,13 +654,23 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     const LevelInfo &F = p->lv[p->inst[i].level0 + l];
     return l >= 1 && (long long)F.ny * F.nx <= tile_max;
   };
+  p->tsmall.assign(p->depth, 0);
   for (int l = 1; l < p->depth; ++l) {
     p->tdown_base[l] = (int)p->tiles.size();
+    long long large = 0;  // large tiles the level would have
     for (int i = 0; i < p->n; ++i) {
       if (bottoms[i] <= l || !on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[p->inst[i].level0 + l];
-      for (int ty = 0; ty < ceil_div(F.ny, tile::kTY); ++ty)
-        for (int tx = 0; tx < ceil_div(F.nx, tile::kTX); ++tx)
+      large += (long long)ceil_div(F.ny, tile::kTY) * ceil_div(F.nx, tile::kTX);
+    }
+    p->tsmall[l] = large > 0 && large < p->sms;
+    const int ty_cells = p->tsmall[l] ? tile::kTYs : tile::kTY;
+    const int tx_cells = p->tsmall[l] ? tile::kTXs : tile::kTX;
+    for (int i = 0; i < p->n; ++i) {
+      if (bottoms[i] <= l || !on_tiles(i, l)) continue;
+      const LevelInfo &F = p->lv[p->inst[i].level0 + l];
+      for (int ty = 0; ty < ceil_div(F.ny, ty_cells); ++ty)
+        for (int tx = 0; tx < ceil_div(F.nx, tx_cells); ++tx)
           p->tiles.push_back(Tile{p->inst[i].level0 + l, i, ty, tx});
       p->tile_cells[l] += (double)F.ny * F.nx;
     }
@@ -702,12 +727,12 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   // the persistent coarse launch: tile levels below the last strip level, the
   // bottom, and the tile levels again on the way up
   {
-    // below the last strip level, and from the first level whose tiles are fewer
-    // than the SMs (which the per-level path also runs with kBThreads-thread CTAs):
-    // larger tile levels keep their own launch of many smaller CTAs
+    // below the last strip level and the last level of large tiles: the
+    // persistent launch holds only small-tile levels (large tile levels keep
+    // their own launch of many CTAs)
     int top = 0;
     for (int l = 0; l < p->depth; ++l)
-      if (p->down_count[l] > 0 || p->tdown_count[l] >= p->sms) top = l + 1;
+      if (p->down_count[l] > 0 || (p->tdown_count[l] > 0 && !p->tsmall[l])) top = l + 1;
     coarse::Phases ph{};
     auto add = [&](int kind, int base, int items) {
       ph.kind[ph.count] = kind;

@@ -131,42 +131,59 @@ __device__ __forceinline__ int bot_mirror(int f, int n, bool neu) {
   return f;
 }
 
+// The few fields of a bottom level its phases read, staged in shared memory
+// once per launch: every phase after a barrier then finds them at shared-memory
+// latency instead of reloading the level descriptors from global memory.
+struct BotLevel {
+  int ny, nx, px, neu;
+  int sm_b, sm_u, sm_r, sm_c;
+};
+
 // The bottom of one active instance, by the whole CTA (kBThreads threads); the
-// CTA's shared memory is free on entry and may be reused on return.
+// CTA's shared memory is free on entry and may be reused on return.  Every
+// phase runs on all warps: a phase's time is the chain of rows its busiest warp
+// walks, so fewer warps on the small levels were measured slower.
 template <typename T, int S1, int S2>
 __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst,
                                                 unsigned char *smem) {
   InstState &S = a.st[inst];
-  const InstInfo &I = a.inst[inst];
   __shared__ T tdiag[kBottomLevels][8], tdinv[kBottomLevels][8];
-  const int nb = I.coarsest - I.bottom + 1;
+  __shared__ BotLevel bl[kBottomLevels];
+  const int bottom = a.inst[inst].bottom, coarsest = a.inst[inst].coarsest;
+  const bool top_is_fine = bottom == a.inst[inst].level0;
+  const int nb = coarsest - bottom + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = kBThreads / 32;
-  const LevelInfo &Lq = a.lv[I.coarsest];
-  const int nq = Lq.ny * Lq.nx;
-  double *const inv_s = reinterpret_cast<double *>(smem + Lq.sm_d) + kCoarsestCells;
+  const int nq = a.lv[coarsest].ny * a.lv[coarsest].nx;
+  const int sm_d = a.lv[coarsest].sm_d;
+  double *const inv_s = reinterpret_cast<double *>(smem + sm_d) + kCoarsestCells;
   {  // the coarsest inverse travels while the levels above are worked on
-    const double *inv_g = a.dense + Lq.inv_off;
+    const double *inv_g = a.dense + a.lv[coarsest].inv_off;
     for (int k = threadIdx.x; k < nq * nq; k += kBThreads)
       __pipeline_memcpy_async(inv_s + k, inv_g + k, sizeof(double));
     __pipeline_commit();
   }
   {  // zero every padded array up to the inverse (ghost rings stay zero for the whole launch)
-    const int bytes = Lq.sm_d + kCoarsestCells * (int)sizeof(double);
+    const int bytes = sm_d + kCoarsestCells * (int)sizeof(double);
     uint4 *z = reinterpret_cast<uint4 *>(smem);
     for (int k = threadIdx.x; k < bytes / 16; k += kBThreads) z[k] = make_uint4(0, 0, 0, 0);
   }
   for (int q = threadIdx.x; q < nb * 8; q += kBThreads) {
     const int l = q >> 3, c = q & 7;
-    const float w = a.lv[I.bottom + l].wall;
+    const float w = a.lv[bottom + l].wall;
     const double d = c >= 1 && c <= 5 ? class_diag(c, w) : 1.0;
     tdiag[l][c] = (T)d;
     tdinv[l][c] = (c >= 1 && c <= 5 && d > 0.0) ? (T)(1.0 / d) : T(0);
+    if (c == 0) {
+      const LevelInfo &L = a.lv[bottom + l];
+      bl[l] = BotLevel{L.ny, L.nx, L.sm_px, L.bc == BC_NEU ? 1 : 0, L.sm_b, L.sm_u, L.sm_r,
+                       L.sm_c};
+    }
   }
   __syncthreads();
   // classes of every level, and b of the top level
   for (int q = 0; q < nb; ++q) {
-    const LevelInfo &L = a.lv[I.bottom + q];
+    const LevelInfo L = a.lv[bottom + q];
     unsigned char *c = smem + L.sm_c;
     const int px = L.sm_px;
     for (int y = warp; y < L.ny; y += NW)
@@ -174,23 +191,25 @@ __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst
         c[(y + 1) * px + 1 + x] = (unsigned char)cell_class(L, a.codes, y, x);
   }
   {
-    const LevelInfo &L = a.lv[I.bottom];
+    const LevelInfo &L = a.lv[bottom];
     const T *B = a.arena + L.b_off;
-    T *b = reinterpret_cast<T *>(smem + L.sm_b);
-    for (int y = warp; y < L.ny; y += NW)
-      for (int x = lane; x < L.nx; x += 32)
-        b[(y + 1) * L.sm_px + 1 + x] = B[(long long)y * L.pitch + x];
+    const long long pitch = L.pitch;
+    const BotLevel Q = bl[0];
+    T *b = reinterpret_cast<T *>(smem + Q.sm_b);
+    for (int y = warp; y < Q.ny; y += NW)
+      for (int x = lane; x < Q.nx; x += 32)
+        b[(y + 1) * Q.px + 1 + x] = B[(long long)y * pitch + x];
   }
   __syncthreads();
   // down: smooth from zero, residual (into b), restriction
   for (int q = 0; q + 1 < nb; ++q) {
-    const LevelInfo &L = a.lv[I.bottom + q];
-    const LevelInfo &C = a.lv[I.bottom + q + 1];
+    const BotLevel L = bl[q];
+    const BotLevel C = bl[q + 1];
     T *u = reinterpret_cast<T *>(smem + L.sm_u);
     const T *b = reinterpret_cast<const T *>(smem + L.sm_b);
     T *res = reinterpret_cast<T *>(smem + L.sm_r);
     const unsigned char *c = smem + L.sm_c;
-    const int px = L.sm_px;
+    const int px = L.px;
     for (int s = 0; s < S1; ++s) {
       bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 0);
       bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 1);
@@ -207,8 +226,8 @@ __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst
     __syncthreads();
     T *bc = reinterpret_cast<T *>(smem + C.sm_b);
     const unsigned char *cc = smem + C.sm_c;
-    const bool neu = L.bc == BC_NEU;
-    const int cpx = C.sm_px;
+    const bool neu = L.neu != 0;
+    const int cpx = C.px;
     for (int Iy = warp; Iy < C.ny; Iy += NW) {
       int fy[4];
 #pragma unroll
@@ -233,41 +252,56 @@ __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst
     }
     __syncthreads();
   }
+  const BotLevel Lc = bl[nb - 1];
   {  // coarsest: dense FP64 inverse, one warp per row
-    const LevelInfo &L = a.lv[I.coarsest];
-    const int n = L.ny * L.nx;
-    const int px = L.sm_px;
-    double *bd = reinterpret_cast<double *>(smem + L.sm_d);
-    const T *b = reinterpret_cast<const T *>(smem + L.sm_b);
-    T *u = reinterpret_cast<T *>(smem + L.sm_u);
+    const int n = Lc.ny * Lc.nx;
+    const int px = Lc.px;
+    double *bd = reinterpret_cast<double *>(smem + sm_d);
+    const T *b = reinterpret_cast<const T *>(smem + Lc.sm_b);
+    T *u = reinterpret_cast<T *>(smem + Lc.sm_u);
     for (int k = threadIdx.x; k < n; k += kBThreads) {
-      const int y = k / L.nx, x = k - y * L.nx;
+      const int y = k / Lc.nx, x = k - y * Lc.nx;
       bd[k] = (double)b[(y + 1) * px + 1 + x];
     }
     __pipeline_wait_prior(0);
     __syncthreads();
+    // a warp's rows (at most kRowsPerWarp) are summed side by side, so their
+    // shuffle reductions overlap
+    constexpr int kRowsPerWarp = (kCoarsestCells + NW - 1) / NW;
     const double *inv = inv_s;
-    for (int t = warp; t < n; t += NW) {
-      double acc = 0.0;
-      for (int j = lane; j < n; j += 32) acc += inv[(long long)t * n + j] * bd[j];
-      acc = warp_sum(acc);
-      if (lane == 0) {
-        const int y = t / L.nx, x = t - y * L.nx;
-        u[(y + 1) * px + 1 + x] = (T)acc;
+    double acc[kRowsPerWarp];
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) {
+      const int t = warp + r * NW;
+      double v = 0.0;
+      if (t < n)
+        for (int j = lane; j < n; j += 32) v += inv[(long long)t * n + j] * bd[j];
+      acc[r] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = warp_sum(acc[r]);
+    if (lane == 0) {
+#pragma unroll
+      for (int r = 0; r < kRowsPerWarp; ++r) {
+        const int t = warp + r * NW;
+        if (t < n) {
+          const int y = t / Lc.nx, x = t - y * Lc.nx;
+          u[(y + 1) * px + 1 + x] = (T)acc[r];
+        }
       }
     }
     __syncthreads();
   }
   // up: reload b, add the prolonged correction, post-smooth
   for (int q = nb - 2; q >= 0; --q) {
-    const LevelInfo &L = a.lv[I.bottom + q];
-    const LevelInfo &C = a.lv[I.bottom + q + 1];
+    const BotLevel L = bl[q];
+    const BotLevel C = bl[q + 1];
     T *u = reinterpret_cast<T *>(smem + L.sm_u);
     T *b = reinterpret_cast<T *>(smem + L.sm_b);
     const T *e = reinterpret_cast<const T *>(smem + C.sm_u);
     const unsigned char *c = smem + L.sm_c;
-    const bool neu = L.bc == BC_NEU;
-    const int px = L.sm_px, cpx = C.sm_px;
+    const bool neu = L.neu != 0;
+    const int px = L.px, cpx = C.px;
     for (int y = warp; y < L.ny; y += NW) {
       const int row = (y + 1) * px + 1;
       const int cy = y >> 1;
@@ -290,20 +324,22 @@ __device__ __forceinline__ void bottom_instance(const Args<T> &a, const int inst
       bot_sweep(u, b, c, L.ny, L.nx, px, tdinv[q], 0);
     }
   }
-  const LevelInfo &L0 = a.lv[I.bottom];
-  T *U = a.arena + L0.u_off;
+  const BotLevel L0 = bl[0];
+  const LevelInfo &G0 = a.lv[bottom];
+  T *U = a.arena + G0.u_off;
+  const long long pitch0 = G0.pitch;
   const T *u0 = reinterpret_cast<const T *>(smem + L0.sm_u);
   const T *b0 = reinterpret_cast<const T *>(smem + L0.sm_b);
   double part = 0.0;
   for (int y = warp; y < L0.ny; y += NW) {
-    const int row = (y + 1) * L0.sm_px + 1;
+    const int row = (y + 1) * L0.px + 1;
     for (int x = lane; x < L0.nx; x += 32) {
       const T v = u0[row + x];
-      U[(long long)y * L0.pitch + x] = v;
+      U[(long long)y * pitch0 + x] = v;
       part += (double)b0[row + x] * (double)v;
     }
   }
-  if (I.bottom == I.level0) {
+  if (top_is_fine) {
     part = block_sum<kBThreads>(part);
     if (threadIdx.x == 0) finish_rz(S, part);
   }

@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_down_s(Arg
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
   const LevelInfo L = a.lv[tl.level];
-  const LevelInfo Lc = a.lv[L.coarse];
+  const LevelInfo Lc = a.lv[tl.level + 1];  // the next entry: levels are stored finest first
   dep_enter();
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   fill_table(tab, L.wall);
@@ -715,7 +715,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) k_up_s(Args<
   __shared__ ClassTable<T> tab;
   const Tile tl = a.tiles[blockIdx.x];
   const LevelInfo L = a.lv[tl.level];
-  const LevelInfo Lc = a.lv[L.coarse];
+  const LevelInfo Lc = a.lv[tl.level + 1];  // the next entry: levels are stored finest first
   dep_enter();
   const bool active = a.st[tl.inst].status == GD_ACTIVE;
   double part = 0.0;

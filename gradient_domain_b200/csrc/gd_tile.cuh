@@ -27,29 +27,35 @@
 namespace gd {
 namespace tile {
 
-constexpr int kTY = 32, kTX = 64;  // cells of a tile (even: whole coarse cells)
-constexpr int kHX = 8;             // halo columns on each side
-// Threads per CTA: 256 where a level has at least one tile per SM (throughput),
-// 1024 on smaller levels, where each phase then takes one pass per thread
-// instead of four and the CTA's chain of phases is the launch's duration.
-constexpr int kThreads = 256, kThreadsSmall = 1024;
+// Two tile shapes.  Levels with at least one 32 x 64 tile per SM run those
+// tiles on CTAs of 256 threads (throughput).  Smaller levels, where one CTA's
+// chain of phases is the launch's duration, run 16 x 32 tiles on CTAs of 384
+// threads: every phase is one pass per thread, and the level spreads over four
+// times as many SMs, so each SM issues a quarter of the instructions.
+constexpr int kTY = 32, kTX = 64;    // cells of a large tile (even: whole coarse cells)
+constexpr int kTYs = 16, kTXs = 32;  // cells of a small tile
+constexpr int kHX = 8;               // halo columns on each side
+constexpr int kThreads = 256, kThreadsSmall = 384;
 
-template <typename T, int S1>
+template <typename T, int S1, int TY = kTY, int TX = kTX>
 struct DownT {
   static constexpr int H = 2 * S1 + 1;
-  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * kHX, N = RY * RX, GX = RX / 4;
+  static constexpr int RY = TY + 2 * H, RX = TX + 2 * kHX, N = RY * RX, GX = RX / 4;
   static constexpr size_t smem = (size_t)N * (2 * sizeof(T) + 1) + 16;
 };
 
-template <typename T, int S2>
+template <typename T, int S2, int TY = kTY, int TX = kTX>
 struct UpT {
   static constexpr int H = 2 * S2;
-  static constexpr int RY = kTY + 2 * H, RX = kTX + 2 * kHX, N = RY * RX, GX = RX / 4;
+  static constexpr int RY = TY + 2 * H, RX = TX + 2 * kHX, N = RY * RX, GX = RX / 4;
   static constexpr int CY = RY / 2 + 3, CX = RX / 2 + 3, CN = CY * CX;
   static constexpr size_t smem = (size_t)(2 * N + CN) * sizeof(T) + N + 16;
 };
 
-static_assert(kHX % 4 == 0 && kTX % 4 == 0 && kHX >= 7, "tile geometry");
+static_assert(kHX % 4 == 0 && kTX % 4 == 0 && kTXs % 4 == 0 && kHX >= 7, "tile geometry");
+static_assert(kTY % 2 == 0 && kTYs % 2 == 0, "tiles hold whole coarse cells");
+// one group of four cells per thread and phase on small tiles (up to three sweeps)
+static_assert((kTYs + 2 * 7) * ((kTXs + 2 * kHX) / 4) <= kThreadsSmall, "small tile threads");
 
 template <typename T>
 __device__ __forceinline__ void diag_tables(T *tdiag, T *tdinv, float wall) {
@@ -144,19 +150,18 @@ __device__ __forceinline__ int tmirror(int f, int n, bool neu) {
 // residual, restriction (P^T) into the coarse right-hand side.  Called by the
 // whole CTA (NT threads) for an active instance's tile; the CTA's shared
 // memory is free on entry and may be reused on return.
-template <typename T, int S1, int NT>
-__device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, unsigned char *smem) {
-  using G = DownT<T, S1>;
+template <typename T, int S1, int NT, int TY = kTY, int TX = kTX>
+__device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, const LevelInfo &L,
+                                          const LevelInfo &Lc, unsigned char *smem) {
+  using G = DownT<T, S1, TY, TX>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX;
-  const LevelInfo L = a.lv[tl.level];
-  const LevelInfo Lc = a.lv[L.coarse];
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
   unsigned *sc = reinterpret_cast<unsigned *>(su + N);
   __shared__ T tdiag[8], tdinv[8];
   diag_tables(tdiag, tdinv, L.wall);
   __syncthreads();
-  const int y0 = tl.ty * kTY, x0 = tl.tx * kTX;
+  const int y0 = tl.ty * TY, x0 = tl.tx * TX;
   const int gy0 = y0 - H, gx0 = x0 - kHX;
   const int par0 = (gy0 + gx0) & 1;
   {  // load, applying the first half sweep (colour 0 from zero: u = b / d)
@@ -195,14 +200,14 @@ __device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, unsig
   }
   {  // the pre-smoothed iterate of the tile, for the up kernel
     T *W = a.arena + L.w_off;
-    constexpr int TG = kTX / 4, M = kTY * TG;
+    constexpr int TG = TX / 4, M = TY * TG;
     for (int g = threadIdx.x; g < M; g += NT) {
       const int ty = g / TG, q = g - ty * TG;
       store_group(W, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
     }
   }
-  {  // residual on the tile plus one ring, in place into b (groups 1 .. kTX/4 + 2)
-    constexpr int QG = kTX / 4 + 2, M = (kTY + 2) * QG, IT = (M + NT - 1) / NT;
+  {  // residual on the tile plus one ring, in place into b (groups 1 .. TX/4 + 2)
+    constexpr int QG = TX / 4 + 2, M = (TY + 2) * QG, IT = (M + NT - 1) / NT;
     st::V4<T> res[IT];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
@@ -238,7 +243,7 @@ __device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, unsig
   __syncthreads();
   const bool neu = L.bc == BC_NEU;
   T *Bc = a.arena + Lc.b_off;
-  constexpr int CTY = kTY / 2, CTX = kTX / 2;
+  constexpr int CTY = TY / 2, CTX = TX / 2;
   for (int k = threadIdx.x; k < CTY * CTX; k += NT) {
     const int qy = k / CTX, qx = k - qy * CTX;
     const int I = (y0 >> 1) + qy, J = (x0 >> 1) + qx;
@@ -264,19 +269,18 @@ __device__ __forceinline__ void down_tile(const Args<T> &a, const Tile tl, unsig
 // Up on one tile: u = w + P e (bilinear; Neumann clamps at the edge, other
 // boundaries read zero outside), then S2 post-sweeps, colour 1 first.  Same
 // calling convention as down_tile.
-template <typename T, int S2, int NT>
-__device__ __forceinline__ void up_tile(const Args<T> &a, const Tile tl, unsigned char *smem) {
-  using G = UpT<T, S2>;
+template <typename T, int S2, int NT, int TY = kTY, int TX = kTX>
+__device__ __forceinline__ void up_tile(const Args<T> &a, const Tile tl, const LevelInfo &L,
+                                        const LevelInfo &Lc, unsigned char *smem) {
+  using G = UpT<T, S2, TY, TX>;
   constexpr int RY = G::RY, RX = G::RX, H = G::H, N = G::N, GX = G::GX, CX = G::CX;
-  const LevelInfo L = a.lv[tl.level];
-  const LevelInfo Lc = a.lv[L.coarse];
   T *sb = reinterpret_cast<T *>(smem);
   T *su = sb + N;
   T *se = su + N;
   unsigned *sc = reinterpret_cast<unsigned *>(se + G::CN);
   __shared__ T tdiag[8], tdinv[8];
   diag_tables(tdiag, tdinv, L.wall);
-  const int y0 = tl.ty * kTY, x0 = tl.tx * kTX;
+  const int y0 = tl.ty * TY, x0 = tl.tx * TX;
   const int gy0 = y0 - H, gx0 = x0 - kHX;
   const int par0 = (gy0 + gx0) & 1;
   const bool neu = L.bc == BC_NEU;
@@ -381,30 +385,36 @@ __device__ __forceinline__ void up_tile(const Args<T> &a, const Tile tl, unsigne
     tsweep<T, RY, RX, NT>(su, sb, sc, tdinv, 0, par0);
   }
   T *U = a.arena + L.u_off;
-  constexpr int TG = kTX / 4, M = kTY * TG;
+  constexpr int TG = TX / 4, M = TY * TG;
   for (int g = threadIdx.x; g < M; g += NT) {
     const int ty = g / TG, q = g - ty * TG;
     store_group(U, L, y0 + ty, x0 + 4 * q, st::ld4(su + (ty + H) * RX + kHX + 4 * q));
   }
 }
 
-// One launch per level: a CTA per tile.
-template <typename T, int S1, int NT = kThreads>
+// One launch per level: a CTA per tile.  A level's coarse level is the next
+// entry of the level table (levels of an instance are stored finest first), so
+// the status word and both descriptors are requested together.
+template <typename T, int S1, int NT = kThreads, int TY = kTY, int TX = kTX>
 __global__ void __launch_bounds__(NT) k_down_t(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  const LevelInfo L = a.lv[tl.level];
+  const LevelInfo Lc = a.lv[tl.level + 1];
   dep_enter();
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   extern __shared__ __align__(16) unsigned char smem[];
-  down_tile<T, S1, NT>(a, tl, smem);
+  down_tile<T, S1, NT, TY, TX>(a, tl, L, Lc, smem);
 }
 
-template <typename T, int S2, int NT = kThreads>
+template <typename T, int S2, int NT = kThreads, int TY = kTY, int TX = kTX>
 __global__ void __launch_bounds__(NT) k_up_t(Args<T> a) {
   const Tile tl = a.tiles[blockIdx.x];
+  const LevelInfo L = a.lv[tl.level];
+  const LevelInfo Lc = a.lv[tl.level + 1];
   dep_enter();
   if (a.st[tl.inst].status != GD_ACTIVE) return;
   extern __shared__ __align__(16) unsigned char smem[];
-  up_tile<T, S2, NT>(a, tl, smem);
+  up_tile<T, S2, NT, TY, TX>(a, tl, L, Lc, smem);
 }
 
 }  // namespace tile

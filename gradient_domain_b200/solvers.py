@@ -46,7 +46,8 @@ from .autotune import resolve
 from .multigrid import MultigridOptions, RefWorkspace
 from .plan import Instance, PoissonPlan, SolveParams, cached_plan
 
-__all__ = ["SolverReport", "SOLVERS", "solve_system", "solve_neumann", "solve_neumann_batch"]
+__all__ = ["SolverReport", "SOLVERS", "solve_system", "solve_neumann", "solve_neumann_batch",
+           "solve_neumann_batch_async", "NeumannBatchFuture"]
 
 
 @dataclass
@@ -379,14 +380,15 @@ _PIPELINE_LOCK = threading.Lock()
 def _take_pipeline(h: int, w: int, params: SolveParams, n: int):
     """``n`` single-instance plans, each with its own stream and device buffers.
 
-    A pipeline is removed from the cache while in use, so concurrent callers of
-    the same shape each get their own.
+    A pipeline is removed from the pool while in use, so concurrent callers of
+    the same shape (or calls still in flight) each get their own.
     """
     key = (h, w, params, n)
     with _PIPELINE_LOCK:
-        pipe = _PIPELINES.pop(key, None)
-    if pipe is not None:
-        return key, pipe
+        idle = _PIPELINES.get(key)
+        if idle:
+            _PIPELINES.move_to_end(key)
+            return key, idle.pop()
     dev = _lib.device()
     pipe = []
     inst = Instance(h, w, "neumann", True)
@@ -401,23 +403,58 @@ def _take_pipeline(h: int, w: int, params: SolveParams, n: int):
     return key, pipe
 
 
+_PIPELINES_KEPT = 8  # idle pipelines kept over all shapes
+
+
 def _return_pipeline(key, pipe) -> None:
+    closing = []
     with _PIPELINE_LOCK:
-        if key in _PIPELINES:
+        _PIPELINES.setdefault(key, []).append(pipe)
+        _PIPELINES.move_to_end(key)
+        while sum(len(v) for v in _PIPELINES.values()) > _PIPELINES_KEPT:
+            old_key = next(iter(_PIPELINES))
+            closing.append(_PIPELINES[old_key].pop(0))
+            if not _PIPELINES[old_key]:
+                del _PIPELINES[old_key]
+    for old in closing:
+        for plan, *_ in old:
+            plan.close()
+
+
+class NeumannBatchFuture:
+    """A :func:`solve_neumann_batch_async` call in flight.  ``result()`` waits for
+    its solves and downloads and returns ``out``; ``reports`` then holds one
+    result per right-hand side."""
+
+    def __init__(self, out: torch.Tensor, key, pipe):
+        self.out = out
+        self.reports: list = []
+        self._key, self._pipe = key, pipe
+
+    def done(self) -> bool:
+        return self._pipe is None
+
+    def result(self) -> torch.Tensor:
+        if self._pipe is None:
+            return self.out
+        pipe, self._pipe = self._pipe, None
+        try:
+            for plan, stream, f, x in pipe:
+                self.reports.extend(plan.finish())
+                stream.synchronize()
+        except BaseException:
             for plan, *_ in pipe:
                 plan.close()
-            return
-        _PIPELINES[key] = pipe
-        while len(_PIPELINES) > 4:
-            _, old = _PIPELINES.popitem(last=False)
-            for plan, *_ in old:
-                plan.close()
+            raise
+        _return_pipeline(self._key, pipe)
+        return self.out
 
 
-def _pipelined_neumann(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
+def _launch_pipelined(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
     """Channel k's upload, solve and download run on stream k: the copy of one
     channel overlaps the solves of the others (copy engines and SMs work at the
-    same time), and each solve is one graph with a device-side loop."""
+    same time), and each solve is one graph with a device-side loop.  Returns
+    without waiting."""
     n, h, w = b.shape
     key, pipe = _take_pipeline(h, w, params, n)
     try:
@@ -428,13 +465,34 @@ def _pipelined_neumann(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
                 f.copy_(b[k], non_blocking=True)
                 plan.solve_async([f], [x], scale=-1.0)
                 out[k].copy_(x, non_blocking=True)
-        results = []
-        for plan, stream, f, x in pipe:
-            results.extend(plan.finish())
-            stream.synchronize()
     except BaseException:
         for plan, *_ in pipe:
             plan.close()
         raise
-    _return_pipeline(key, pipe)
-    return results
+    return NeumannBatchFuture(out, key, pipe)
+
+
+def _pipelined_neumann(b: torch.Tensor, out: torch.Tensor, params: SolveParams):
+    fut = _launch_pipelined(b, out, params)
+    fut.result()
+    return fut.reports
+
+
+def solve_neumann_batch_async(b: torch.Tensor, out: torch.Tensor,
+                              tolerance: float = NEUMANN_EXACT_TOLERANCE,
+                              max_iterations: int = 2000,
+                              precision: str = "mixed") -> NeumannBatchFuture:
+    """:func:`solve_neumann_batch` without waiting, for callers that keep several
+    batches in flight (the next batch's uploads then overlap this one's solves
+    and downloads).  ``b`` and ``out`` are pinned FP64 CPU tensors of one shape
+    ``(n, h, w)``; neither may be touched until ``result()`` has returned.  The
+    solutions are bitwise those of :func:`solve_neumann_batch`."""
+    if not (isinstance(b, torch.Tensor) and isinstance(out, torch.Tensor) and b.dim() == 3
+            and b.dtype == torch.float64 and out.dtype == torch.float64
+            and b.device.type == "cpu" and out.device.type == "cpu" and b.is_pinned()
+            and out.is_pinned() and out.shape == b.shape):
+        raise ValueError("solve_neumann_batch_async takes pinned FP64 CPU tensors b and out "
+                         "of one (n, h, w) shape")
+    params = SolveParams(precision=precision, tolerance=tolerance,
+                         max_iterations=max_iterations, zero_start=True)
+    return _launch_pipelined(b, out, params)

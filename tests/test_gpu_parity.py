@@ -417,6 +417,23 @@ def test_async_solve_and_pipelined_batch():
         assert got is host_out
         assert np.array_equal(host_out.numpy(), want)
         assert all(r.converged for r in gd.solve_neumann_batch.last_results)
+    # several batches in flight (later uploads overlap earlier solves): each one
+    # bitwise the synchronous result, also with a shape change in between
+    stacks = [stack, -stack, stack[:, :48, :80].copy()]
+    for k in range(2):
+        stacks[2 - k] -= stacks[2 - k].mean(axis=(1, 2), keepdims=True)
+    wants = [gd.solve_neumann_batch(s, tolerance=1e-12) for s in stacks]
+    futs = []
+    for rep in range(2):
+        for s_np in stacks:
+            b = torch.as_tensor(s_np).pin_memory()
+            futs.append((gd.solve_neumann_batch_async(b, torch.empty_like(b).pin_memory(),
+                                                      tolerance=1e-12), b))
+    for k, (fut, _) in enumerate(futs):
+        out = fut.result()
+        assert fut.done() and fut.result() is out
+        assert np.array_equal(out.numpy(), wants[k % len(stacks)])
+        assert len(fut.reports) == 3 and all(r.converged for r in fut.reports)
 
 
 def _device_field_div(target, kind, window, source=None, select=None, weights=None,
@@ -696,3 +713,31 @@ def test_dependent_launch_equals_serial_launch(precision):
             assert ia == ib, key
             for a, b in zip(xa, xb):
                 assert torch.equal(a, b), key
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_tile_shape_does_not_change_results(precision):
+    """Level 1 of a 990 x 1000 instance (495 x 500 cells) has 128 large tiles: alone it
+    runs on small tiles (fewer large tiles than SMs), in a batch of two on large
+    tiles.  Every tile recomputes its halo exactly, so the solutions are bitwise the
+    same either way, on direct launches and on the solve graph."""
+    rng = np.random.default_rng(41)
+    shapes = [(990, 1000, "neumann"), (1000, 980, "dirichlet")]
+    rhs = [torch.as_tensor(rng.standard_normal(s[:2])).cuda() for s in shapes]
+    params = SolveParams(precision=precision, tolerance=1e-9, zero_start=True)
+    insts = [Instance(h, w, b, b == "neumann") for h, w, b in shapes]
+    batch = PoissonPlan(insts, params)
+    got = []
+    for _ in range(2):
+        xb = [torch.empty_like(r) for r in rhs]
+        rb = batch.solve(rhs, xb, scale=1.0)
+        got.append((xb, [r.iterations for r in rb]))
+    batch.close()
+    for k in range(len(shapes)):
+        alone = PoissonPlan([insts[k]], params)
+        for xb, its in got:
+            xa = torch.empty_like(rhs[k])
+            (ra,) = alone.solve([rhs[k]], [xa], scale=1.0)
+            assert ra.converged and ra.iterations == its[k]
+            assert torch.equal(xa, xb[k])
+        alone.close()

@@ -258,3 +258,16 @@ def test_serving_mix_equals_alone():
             plan.solve(f, x)
             ref = np.stack([t.cpu().numpy() for t in x])
         assert np.abs(got.x - ref).max() <= 1e-6 * max(np.abs(ref).max(), 1e-12), name
+
+
+def test_async_batch_rejects_pageable_or_mismatched_buffers():
+    """solve_neumann_batch_async checks its buffers on the host before any copy."""
+    import torch
+    from gradient_domain_b200 import solve_neumann_batch_async
+    b = torch.zeros((2, 8, 8), dtype=torch.float64)
+    with pytest.raises(ValueError):
+        solve_neumann_batch_async(b, torch.zeros_like(b))          # not pinned
+    with pytest.raises(ValueError):
+        solve_neumann_batch_async(b.numpy(), torch.zeros_like(b))  # not a tensor
+    with pytest.raises(ValueError):
+        solve_neumann_batch_async(b[0], torch.zeros_like(b[0]))    # not a stack
