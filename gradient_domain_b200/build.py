@@ -13,6 +13,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -27,7 +28,6 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC,-O3",
     "--expt-relaxed-constexpr",
-    "-shared",
 ]
 
 
@@ -52,15 +52,36 @@ def nvcc() -> str:
 
 
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
-    """Compile every ``csrc/*.cu`` into ``libgd_poisson.so``; returns its path."""
+    """Compile every ``csrc/*.cu`` into ``libgd_poisson.so``; returns its path.
+
+    The translation units share no device code, so each compiles to its own
+    object in parallel (under ``_build/``) and one nvcc call links them.
+    """
     if not force and not _stale():
         return LIB
-    tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"),
-           "-o", tmp, *sources(), *LINK]
+    objdir = os.path.join(ROOT, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(src)[:-3] + ".o") for src in srcs]
+    cmds = [[nvcc(), *NVCC_FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"),
+             "-c", "-o", obj, src] for src, obj in zip(srcs, objs)]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        for cmd in cmds:
+            print(" ".join(cmd), flush=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for cmd, res in zip(cmds, results):
+        if res.stdout or res.stderr:
+            sys.stdout.write(res.stdout)
+            sys.stderr.write(res.stderr)
+        if res.returncode != 0:
+            raise subprocess.CalledProcessError(res.returncode, cmd)
+    tmp = LIB + ".tmp"
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+            "-o", tmp, *objs, *LINK]
+    if verbose:
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -41,6 +41,9 @@ struct gd_plan_s {
   std::vector<int> down_base, down_count, up_base, up_count;     // strip maps per level
   std::vector<int> tdown_base, tdown_count, tup_base, tup_count;  // tile maps per level
   std::vector<char> tsmall;  // per level: tiles of the small shape (fewer large tiles than SMs)
+  // per strip level: some strip instance is masked (at the level or the next) or
+  // too large for 32-bit row offsets, so the launch needs the general strips
+  std::vector<char> strip_any;
   size_t arena_elems = 0, code_bytes = 0, dense_elems = 0, xs_elems = 0;
   int max_partials = 1;
   size_t o_lv = 0, o_inst = 0, o_st = 0, o_tiles = 0, o_arena = 0, o_codes = 0, o_dense = 0,
@@ -228,12 +231,21 @@ struct Runner {
   static void set_attrs() {
     cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kBottomSmem);
-    const int lvl = (int)st::level_smem<T>();
+    const int lvl = (int)st::strip_smem<T, S>();
     cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, lvl);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          lvl);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          lvl);
+    if constexpr (sizeof(T) == 4) {
+      const int fast = (int)st::strip_smem<T, S, false>();
+      cudaFuncSetAttribute(st::k_down_s<T, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           fast);
+      cudaFuncSetAttribute(st::k_up_s<T, S, S, true, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, fast);
+      cudaFuncSetAttribute(st::k_up_s<T, S, S, false, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, fast);
+    }
     cudaFuncSetAttribute(tile::k_down_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)tile::DownT<T, S>::smem);
     cudaFuncSetAttribute(tile::k_up_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -330,12 +342,20 @@ struct Runner {
     return a;
   }
 
+  // Levels whose strip instances are all rectangles run the rectangle-only
+  // strip kernels (FP32), which fit more CTAs per SM.
+  static bool rect_only(gd_plan p, int l) { return sizeof(T) == 4 && !p->strip_any[l]; }
+
   template <int S>
   static void down_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->down_count[l] > 0) {
       prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st, l);
-      chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kThreads, st::level_smem<T>(),
-                   st, at_tiles(a, p->down_base[l]));
+      if (rect_only(p, l))
+        chain_launch(p, st::k_down_s<T, S, false>, p->down_count[l], st::kThreads,
+                     st::strip_smem<T, S, false>(), st, at_tiles(a, p->down_base[l]));
+      else
+        chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kThreads,
+                     st::strip_smem<T, S>(), st, at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     if (p->tdown_count[l] > 0) {
@@ -364,12 +384,17 @@ struct Runner {
     }
     if (p->up_count[l] <= 0) return;
     prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st, l);
-    if (l == 0)
-      chain_launch(p, st::k_up_s<T, S, S, true>, p->up_count[l], st::kThreads,
-                   st::level_smem<T>(), st, at_tiles(a, p->up_base[l]));
-    else
-      chain_launch(p, st::k_up_s<T, S, S, false>, p->up_count[l], st::kThreads,
-                   st::level_smem<T>(), st, at_tiles(a, p->up_base[l]));
+    const Args<T> at = at_tiles(a, p->up_base[l]);
+    const int n = p->up_count[l];
+    if (rect_only(p, l)) {
+      const size_t sm = st::strip_smem<T, S, false>();
+      if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true, false>, n, st::kThreads, sm, st, at);
+      else chain_launch(p, st::k_up_s<T, S, S, false, false>, n, st::kThreads, sm, st, at);
+    } else {
+      const size_t sm = st::strip_smem<T, S>();
+      if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true>, n, st::kThreads, sm, st, at);
+      else chain_launch(p, st::k_up_s<T, S, S, false>, n, st::kThreads, sm, st, at);
+    }
     prof_end(p, st);
   }
 
@@ -678,6 +703,16 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     p->tup_base[l] = p->tdown_base[l];  // the up kernel uses the same tiles
     p->tup_count[l] = p->tdown_count[l];
   }
+  p->strip_any.assign(std::max(p->depth, 1), 0);
+  for (int l = 0; l < p->depth; ++l)
+    for (int i = 0; i < p->n; ++i) {
+      if (bottoms[i] <= l || on_tiles(i, l)) continue;
+      const LevelInfo &F = p->lv[p->inst[i].level0 + l];
+      const LevelInfo &Fc = p->lv[p->inst[i].level0 + l + 1];
+      if (F.code_off >= 0 || Fc.code_off >= 0 ||
+          (long long)(F.ny + 16) * F.pitch >= (1LL << 31))
+        p->strip_any[l] = 1;
+    }
   for (int l = 0; l < p->depth; ++l) {
     p->down_base[l] = (int)p->tiles.size();
     for (int i = 0; i < p->n; ++i) {
@@ -1169,6 +1204,9 @@ int collect_reports(gd_plan p, gd_report *reports) {
              "the solution is not valid", err);
   GD_REQUIRE(!(err & coarse::kErrBarrier), GD_ERR_CUDA,
              "solve: a grid barrier of the persistent coarse launch gave up (error word %#x); "
+             "the solution is not valid", err);
+  GD_REQUIRE(!(err & st::kErrStrip), GD_ERR_CUDA,
+             "solve: a rectangle-only strip kernel met a masked level (error word %#x); "
              "the solution is not valid", err);
   GD_REQUIRE(err == 0, GD_ERR_CUDA, "solve: device error word %#x; the solution is not valid",
              err);

@@ -310,18 +310,100 @@ struct Coef {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Arithmetic of the smoothing kernels.  Every cell value is one fixed sequence
+// of round-to-nearest operations (nothing left to the compiler's contraction),
+// written once per cell for the general strips (FP32 and FP64) and once per
+// pair of cells for the FP32 interior strips, which evaluate it with the paired
+// FP32 instructions of sm_100 (two cells per instruction).  Both give the same
+// bits, so which strip computes a cell never changes its value.
+//
+// A lane's four columns x0 .. x0+3 (x0 a multiple of 4) are held by the
+// interior strips as two pairs, E = (v0, v2) and O = (v1, v3): the cells of a
+// pair have the same colour on every row, so a red-black half sweep updates
+// exactly one pair of each lane.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Sum of a cell's four neighbours and its right-hand side: nbA is the
+// horizontal neighbour inside the lane's four columns on the side of the
+// cell's pair partner (the right one for even columns, the left one for odd
+// columns), nbB the other one; dn, the row a pipelined sweep updated last, is
+// added last so that it ends the dependency chain.
+template <typename T>
+__device__ __forceinline__ T nsum1(T up, T nbA, T nbB, T b, T dn) {
+  return add_rn(add_rn(add_rn(add_rn(up, nbA), nbB), b), dn);
+}
+// Prolongation of a coarse correction onto a fine cell: w + 3/4 near + 1/4 far.
+template <typename T>
+__device__ __forceinline__ T prolong1(T w, T near, T far) {
+  return fma_rn(T(0.25), far, fma_rn(T(0.75), near, w));
+}
+// Full weighting along one axis: 1/4 a + 3/4 b + 3/4 c + 1/4 d.
+template <typename T>
+__device__ __forceinline__ T weigh1(T a, T b, T c, T d) {
+  return fma_rn(T(0.25), d, fma_rn(T(0.75), c, fma_rn(T(0.75), b, mul_rn(T(0.25), a))));
+}
+// Linear interpolation 3/4 near + 1/4 far.
+template <typename T>
+__device__ __forceinline__ T interp1(T near, T far) {
+  return fma_rn(T(0.25), far, mul_rn(T(0.75), near));
+}
+// Dot product of a lane's four cells.
+template <typename T>
+__device__ __forceinline__ T dot1(const V4<T> &b, const V4<T> &v) {
+  return add_rn(fma_rn(b.v[1], v.v[1], mul_rn(b.v[0], v.v[0])),
+                fma_rn(b.v[3], v.v[3], mul_rn(b.v[2], v.v[2])));
+}
+
+// Paired forms (element-wise the scalar ones above).
+struct P4 {
+  float2 e, o;  // (v0, v2), (v1, v3)
+};
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 nsum2(float2 up, float2 nbA, float2 nbB, float2 b, float2 dn) {
+  return add2(add2(add2(add2(up, nbA), nbB), b), dn);
+}
+__device__ __forceinline__ P4 split4(const float4 &q) {
+  return P4{make_float2(q.x, q.z), make_float2(q.y, q.w)};
+}
+__device__ __forceinline__ float4 join4(const P4 &p) {
+  return make_float4(p.e.x, p.o.x, p.e.y, p.o.y);
+}
+__device__ __forceinline__ P4 zero_p4() { return P4{make_float2(0.f, 0.f), make_float2(0.f, 0.f)}; }
+
+// Half sweep of the even pair (J0 = 0) or the odd pair (J0 = 1) of a row of an
+// interior strip, diagonal inverse `inv` for every cell.
+template <int J0>
+__device__ __forceinline__ void psweep(P4 &u, const P4 &up, const P4 &dn, const P4 &b, float2 inv) {
+  if constexpr (J0 == 0) {
+    const float left = shfl_up1(u.o.y);
+    u.e = mul2(nsum2(up.e, u.o, make_float2(left, u.o.x), b.e, dn.e), inv);
+  } else {
+    const float right = shfl_dn1(u.e.x);
+    u.o = mul2(nsum2(up.o, u.e, make_float2(u.e.y, right), b.o, dn.o), inv);
+  }
+}
+
 // Half sweep on one row; J0 (first updated cell of the lane) is compile-time.
 template <int J0, typename T, bool INT>
 __device__ __forceinline__ void hsweep(V4<T> &u, const V4<T> &up, const V4<T> &dn,
                                        const V4<T> &b, unsigned c, const Coef<T, INT> &K) {
   if constexpr (J0 == 0) {
     const T left = shfl_up1(u.v[3]);
-    u.v[0] = (b.v[0] + up.v[0] + dn.v[0] + left + u.v[1]) * K.inv(c, 0);
-    u.v[2] = (b.v[2] + up.v[2] + dn.v[2] + u.v[1] + u.v[3]) * K.inv(c, 2);
+    u.v[0] = mul_rn(nsum1(up.v[0], u.v[1], left, b.v[0], dn.v[0]), K.inv(c, 0));
+    u.v[2] = mul_rn(nsum1(up.v[2], u.v[3], u.v[1], b.v[2], dn.v[2]), K.inv(c, 2));
   } else {
     const T right = shfl_dn1(u.v[0]);
-    u.v[1] = (b.v[1] + up.v[1] + dn.v[1] + u.v[0] + u.v[2]) * K.inv(c, 1);
-    u.v[3] = (b.v[3] + up.v[3] + dn.v[3] + u.v[2] + right) * K.inv(c, 3);
+    u.v[1] = mul_rn(nsum1(up.v[1], u.v[0], u.v[2], b.v[1], dn.v[1]), K.inv(c, 1));
+    u.v[3] = mul_rn(nsum1(up.v[3], u.v[2], right, b.v[3], dn.v[3]), K.inv(c, 3));
   }
 }
 
@@ -329,7 +411,7 @@ template <int J0, typename T, bool INT>
 __device__ __forceinline__ void hsweep_zero(V4<T> &u, const V4<T> &b, unsigned c,
                                             const Coef<T, INT> &K) {
 #pragma unroll
-  for (int j = 0; j < 4; ++j) u.v[j] = ((j & 1) == J0) ? b.v[j] * K.inv(c, j) : T(0);
+  for (int j = 0; j < 4; ++j) u.v[j] = ((j & 1) == J0) ? mul_rn(b.v[j], K.inv(c, j)) : T(0);
 }
 
 // A u on a row (zero where there is no unknown).
@@ -440,11 +522,18 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
       const T left = shfl_up1(uK.v[3]);
       const T right = shfl_dn1(uK.v[0]);
       const unsigned cK = Cw[wslot<U>(ph, K)];
-      const V4<T> au = arow(uK, Uw[wslot<U>(ph, K + 1)], Uw[wslot<U>(ph, K - 1)], left, right, cK, C);
       const V4<T> &bK = Bw[wslot<U>(ph, K)];
+      const V4<T> &upK = Uw[wslot<U>(ph, K + 1)], &dnK = Uw[wslot<U>(ph, K - 1)];
+      const T lf[4] = {left, uK.v[0], uK.v[1], uK.v[2]};
+      const T rt[4] = {uK.v[1], uK.v[2], uK.v[3], right};
       V4<T> res;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) res.v[j] = C.on(cK, j) ? bK.v[j] - au.v[j] : T(0);
+      for (int j = 0; j < 4; ++j) {
+        // b - A u = (b + neighbours) - d u, neighbours summed as in the sweeps
+        const T s = (j & 1) ? nsum1(upK.v[j], lf[j], rt[j], bK.v[j], dnK.v[j])
+                            : nsum1(upK.v[j], rt[j], lf[j], bK.v[j], dnK.v[j]);
+        res.v[j] = C.on(cK, j) ? fma_rn(-C.d(cK, j), uK.v[j], s) : T(0);
+      }
       T e[6];
       e[0] = shfl_up1(res.v[3]);
       e[1] = res.v[0]; e[2] = res.v[1]; e[3] = res.v[2]; e[4] = res.v[3];
@@ -458,8 +547,8 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
         }
       }
       V4<T> &Fr = F[wslot<U>(ph, K)];
-      Fr.v[0] = T(0.25) * e[0] + T(0.75) * e[1] + T(0.75) * e[2] + T(0.25) * e[3];
-      Fr.v[1] = T(0.25) * e[2] + T(0.75) * e[3] + T(0.75) * e[4] + T(0.25) * e[5];
+      Fr.v[0] = weigh1(e[0], e[1], e[2], e[3]);
+      Fr.v[1] = weigh1(e[2], e[3], e[4], e[5]);
       // coarse row I = yr / 2 - 1 from residual rows 2I-1 .. 2I+2 (yr even <=> ph even)
       if ((ph & 1) == 0) {
         const int I = (yr >> 1) - 1;
@@ -484,8 +573,7 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
             for (int q = 0; q < 2; ++q) {
               const int J = J0 + q;
               if (J >= 0 && J < Lc.nx) {
-                T v = T(0.25) * rows[0][q] + T(0.75) * rows[1][q] + T(0.75) * rows[2][q] +
-                      T(0.25) * rows[3][q];
+                T v = weigh1(rows[0][q], rows[1][q], rows[2][q], rows[3][q]);
                 if (!INT && Lc.code_off >= 0 && !a.codes[Lc.code_off + (long long)I * Lc.pitch + J])
                   v = T(0);
                 Bc[(long long)I * Lc.pitch + J] = v;
@@ -499,14 +587,293 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
   __pipeline_wait_prior(0);  // no copy may land after this warp's shared memory is released
 }
 
+// Phases of one unrolled pass of the interior strips: a multiple of the window
+// length U and at least 6, so that the ring slot (P slots, P - 1 rows in
+// flight per lane) and every window and coarse slot is a compile-time index.
+template <int U>
+struct FastGeom {
+  static constexpr int P = U >= 6 ? U : 2 * U;
+  // Ring slots per array (P - 1 rows in flight; 2P, alternating between the two
+  // halves, was measured no faster).
+  static constexpr int R = P;
+  static_assert(P % U == 0 && P % 2 == 0 && (R == P || R == 2 * P), "interior strip pass");
+};
+
+// Dynamic shared memory of the down / up kernels: the general strips' rings or
+// the fast FP32 strips' rings, whichever is larger (ANY), or the fast strips'
+// alone.
+// Coarse-row ring of the fast up strips: per slot 8 bytes per lane (the lane's
+// two coarse columns) and 8 bytes per warp (the columns just outside it).
+template <int R>
+constexpr size_t coarse_ring_bytes() { return (size_t)R * (kThreads * 8 + kWarps * 8); }
+
+template <typename T, int S, bool ANY = true>
+constexpr size_t strip_smem() {
+  constexpr int R = FastGeom<2 * S + 2>::R;
+  const size_t fast = sizeof(T) == 4 ? (size_t)2 * R * kThreads * 16 + coarse_ring_bytes<R>() : 0;
+  if (!ANY) return fast;
+  return level_smem<T>() > fast ? level_smem<T>() : fast;
+}
+
+// Per-lane constants of the fast strips on rectangle levels in any position
+// (RECT): which of the lane's four columns are in the grid, and the diagonal
+// inverse and negated diagonal of its cells, as same-colour pairs, for each
+// kind of row: 0, 1 or 2 walls (2: a level one row high).  Rows outside the
+// grid (kind 3) have no unknowns.  Values come from the class table, as in the
+// general strips.
+struct LaneRect {
+  P4 inv[3], negd[3];
+  unsigned on;  // bit j: column x0 + j is in the grid
+};
+
+__device__ __forceinline__ LaneRect lane_rect(const LevelInfo &L, const ClassTable<float> &tab,
+                                              int x0) {
+  LaneRect r;
+  r.on = 0u;
+  float iv[3][4], nd[3][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int x = x0 + j;
+    const bool in = x >= 0 && x < L.nx;
+    const int wx = (x == 0) + (x == L.nx - 1);
+    if (in) r.on |= 1u << j;
+#pragma unroll
+    for (int wy = 0; wy < 3; ++wy) {
+      const int c = in ? 1 + wy + wx : 0;
+      iv[wy][j] = tab.inv[c];
+      nd[wy][j] = -tab.d[c];
+    }
+  }
+#pragma unroll
+  for (int wy = 0; wy < 3; ++wy) {
+    r.inv[wy] = P4{make_float2(iv[wy][0], iv[wy][2]), make_float2(iv[wy][1], iv[wy][3])};
+    r.negd[wy] = P4{make_float2(nd[wy][0], nd[wy][2]), make_float2(nd[wy][1], nd[wy][3])};
+  }
+  return r;
+}
+
+// Kind of row y: walls (0, 1, 2), or 3 outside the grid.
+__device__ __forceinline__ int row_kind(const LevelInfo &L, int y) {
+  return (y < 0 || y >= L.ny) ? 3 : (y == 0) + (y == L.ny - 1);
+}
+
+__device__ __forceinline__ P4 pick(const P4 (&t)[3], int kind) {
+  return kind == 0 ? t[0] : kind == 1 ? t[1] : kind == 2 ? t[2] : zero_p4();
+}
+
+// Zero the cells of a row that have no unknown (rows outside the grid, columns
+// outside it).
+__device__ __forceinline__ P4 mask_on(const P4 &v, unsigned on, int kind) {
+  if (kind == 3) return zero_p4();
+  return P4{make_float2((on & 1u) ? v.e.x : 0.f, (on & 4u) ? v.e.y : 0.f),
+            make_float2((on & 2u) ? v.o.x : 0.f, (on & 8u) ? v.o.y : 0.f)};
+}
+
+// Down on an FP32 strip of an unmasked level whose next level is unmasked: the
+// same cells as down_strip<float, S1, INT>, bit for bit, with ring slots and
+// window slots fixed per unrolled phase, running row offsets and the
+// arithmetic on same-colour cell pairs.  RECT = false: every row and column
+// the strip loads is an interior cell (no walls, no bounds tests); RECT = true:
+// any strip of a rectangle level (copies outside the grid are zero-filled,
+// walls take their cells' diagonals, Neumann restriction mirrors its ghosts).
+template <int S1, bool RECT>
+__device__ __forceinline__ void down_strip_fast(const Args<float> &a, const LevelInfo &L,
+                                                const LevelInfo &Lc, const ClassTable<float> &tab,
+                                                int x0, bool out_lane, int y_start, int y_last,
+                                                int y_out0, int y_out1, int I_begin, int I_end,
+                                                unsigned char *smem) {
+  constexpr int U = DownGeom<float, S1>::U;
+  constexpr int P = FastGeom<U>::P, R = FastGeom<U>::R;
+  constexpr int K = 2 * S1;       // window index of the residual row
+  constexpr int KP = 2 * S1 - 1;  // window index of the row written as w
+  const float2 q25 = splat2(0.25f), q75 = splat2(0.75f);
+  const float *B = a.arena + L.b_off;
+  float *Bc = a.arena + Lc.b_off;
+  float *Wp = a.arena + L.w_off + x0;
+  const int pitch = L.pitch;
+  float *ring = reinterpret_cast<float *>(smem) + threadIdx.x * 4;
+  constexpr int kSlot = kThreads * 4;  // floats between two slots of a lane
+  // interior: one diagonal for every cell
+  const P4 inv_i{splat2(tab.inv[1]), splat2(tab.inv[1])};
+  const float2 negd_i = splat2(-tab.d[1]);
+  LaneRect lr;
+  bool lane_in = true, full = true, neu = false;
+  int J0 = x0 >> 1;  // x0 is a multiple of 4, so this is exact for negative x0 too
+  bool st0 = true, st1 = true;  // coarse columns J0, J0 + 1 are in the coarse grid
+  if constexpr (RECT) {
+    lr = lane_rect(L, tab, x0);
+    lane_in = x0 >= 0 && x0 < L.nx;
+    full = x0 + 3 < L.nx;
+    neu = L.bc == BC_NEU;
+    st0 = J0 >= 0 && J0 < Lc.nx;
+    st1 = J0 + 1 >= 0 && J0 + 1 < Lc.nx;
+  }
+  P4 Bw[U], Uw[U];
+  float2 F[U];
+  int Kw[U];  // row kinds of the window rows (RECT)
+#pragma unroll
+  for (int k = 0; k < U; ++k) {
+    Bw[k] = zero_p4(); Uw[k] = zero_p4(); F[k] = make_float2(0.f, 0.f); Kw[k] = 3;
+  }
+  auto issue = [&](float *dst, int y, int gofs) {
+    if constexpr (RECT) {
+      const bool ok = lane_in && y >= 0 && y < L.ny;
+      __pipeline_memcpy_async(dst, ok ? B + gofs : B, 16, ok ? 0 : 16);
+    } else {
+      __pipeline_memcpy_async(dst, B + gofs, 16);
+    }
+  };
+  int gofs = y_start * pitch + x0;  // row offset of the next row to copy
+#pragma unroll
+  for (int q = 0; q < R - 1; ++q) {
+    issue(ring + q * kSlot, y_start + q, gofs);
+    __pipeline_commit();
+    gofs += pitch;
+  }
+  int wofs = (y_start - KP) * pitch;  // row offset of the w row written this step
+  int half = 0;  // ring slot of this pass's first row (0 or P when R == 2P)
+  for (int base = y_start; base <= y_last; base += P) {
+    float *cur = ring + half * kSlot;
+    float *prev = ring + (R == P ? 0 : (half ^ P)) * kSlot;  // half the slot before ph = 0 is in
+#pragma unroll
+    for (int ph = 0; ph < P; ++ph) {
+      const int y = base + ph;
+      if (y > y_last) break;
+      __pipeline_wait_prior(R - 2);
+      const float4 qb = *reinterpret_cast<const float4 *>(cur + ph * kSlot);
+      if (y + R - 1 <= y_last)  // no copy of rows past the strip; the slot read one step ago
+        issue(ph > 0 ? cur + (ph - 1) * kSlot : prev + (P - 1) * kSlot, y + R - 1, gofs);
+      __pipeline_commit();
+      gofs += pitch;
+      P4 &b0 = Bw[wslot<U>(ph, 0)];
+      b0 = split4(qb);
+      if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
+      auto inv_of = [&](int k) -> P4 {
+        if constexpr (RECT) return pick(lr.inv, Kw[wslot<U>(ph, k)]);
+        else return inv_i;
+      };
+      // first half sweep (colour 0) from a zero iterate on row y
+      if ((ph & 1) == 0) {
+        Uw[wslot<U>(ph, 0)].e = mul2(b0.e, inv_of(0).e);
+        Uw[wslot<U>(ph, 0)].o = make_float2(0.f, 0.f);
+      } else {
+        Uw[wslot<U>(ph, 0)].o = mul2(b0.o, inv_of(0).o);
+        Uw[wslot<U>(ph, 0)].e = make_float2(0.f, 0.f);
+      }
+      // half sweep h on row y - (h - 1); its updated pair is the parity of y
+#pragma unroll
+      for (int h = 2; h <= 2 * S1; ++h) {
+        const int k = h - 1;
+        if ((ph & 1) == 0)
+          psweep<0>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                    Bw[wslot<U>(ph, k)], inv_of(k).e);
+        else
+          psweep<1>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                    Bw[wslot<U>(ph, k)], inv_of(k).o);
+      }
+      {  // row y - KP has seen every pre-sweep: keep it for the up kernel
+        const int yw = y - KP;
+        if (out_lane && lane_in && yw >= y_out0 && yw < y_out1) {
+          const float4 v = join4(Uw[wslot<U>(ph, KP)]);
+          if (full) {
+            *reinterpret_cast<float4 *>(Wp + wofs) = v;
+          } else {
+            const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (x0 + j < L.nx) Wp[wofs + j] = vv[j];
+          }
+        }
+        wofs += pitch;
+      }
+      // residual of row y - K and its horizontal restriction
+      const P4 &uK = Uw[wslot<U>(ph, K)], &upK = Uw[wslot<U>(ph, K + 1)];
+      const P4 &dnK = Uw[wslot<U>(ph, K - 1)], &bK = Bw[wslot<U>(ph, K)];
+      const float left = shfl_up1(uK.o.y), right = shfl_dn1(uK.e.x);
+      P4 nd;
+      if constexpr (RECT) nd = pick(lr.negd, Kw[wslot<U>(ph, K)]);
+      else nd = P4{negd_i, negd_i};
+      P4 r;
+      r.e = fma2(nd.e, uK.e, nsum2(upK.e, uK.o, make_float2(left, uK.o.x), bK.e, dnK.e));
+      r.o = fma2(nd.o, uK.o, nsum2(upK.o, uK.e, make_float2(uK.e.y, right), bK.o, dnK.o));
+      if constexpr (RECT) r = mask_on(r, lr.on, Kw[wslot<U>(ph, K)]);
+      float e0 = shfl_up1(r.o.y), e5 = shfl_dn1(r.e.x);
+      float2 fA = make_float2(e0, r.o.x), fB = r.e, fC = r.o, fD = make_float2(r.e.y, e5);
+      if constexpr (RECT) {
+        if (neu) {  // Neumann ghosts of the restriction mirror the edge cells
+          float e[6] = {e0, r.e.x, r.o.x, r.e.y, r.o.y, e5};
+          if (x0 == 0) e[0] = e[1];
+          if (!(L.nx & 1)) {
+            const int mr = L.nx - x0;
+#pragma unroll
+            for (int m = 0; m <= 4; ++m)
+              if (m == mr) e[m + 1] = e[m];
+          }
+          fA = make_float2(e[0], e[2]); fB = make_float2(e[1], e[3]);
+          fC = make_float2(e[2], e[4]); fD = make_float2(e[3], e[5]);
+        }
+      }
+      // (weigh1(e0, e1, e2, e3), weigh1(e2, e3, e4, e5))
+      F[wslot<U>(ph, K)] = fma2(q25, fD, fma2(q75, fC, fma2(q75, fB, mul2(q25, fA))));
+      // coarse row I = (y - K) / 2 - 1 from the restricted rows 2I-1 .. 2I+2
+      if ((ph & 1) == 0) {
+        const int I = ((y - K) >> 1) - 1;
+        if (out_lane && I >= I_begin && I < I_end) {
+          float2 rows[4] = {F[wslot<U>(ph, K + 3)], F[wslot<U>(ph, K + 2)],
+                            F[wslot<U>(ph, K + 1)], F[wslot<U>(ph, K)]};
+          if constexpr (RECT) {
+            if (neu) {
+              if (I == 0) rows[0] = rows[1];
+              if (!(L.ny & 1)) {
+#pragma unroll
+                for (int q = 1; q < 4; ++q)
+                  if (2 * I - 1 + q == L.ny) rows[q] = rows[q - 1];
+              }
+            }
+          }
+          const float2 v =
+              fma2(q25, rows[3], fma2(q75, rows[2], fma2(q75, rows[1], mul2(q25, rows[0]))));
+          float *dst = Bc + I * Lc.pitch + J0;
+          if (st0 && st1) {
+            *reinterpret_cast<float2 *>(dst) = v;
+          } else {
+            if (st0) dst[0] = v.x;
+            if (st1) dst[1] = v.y;
+          }
+        }
+      }
+    }
+    if constexpr (R != P) half ^= P;
+  }
+  __pipeline_wait_prior(0);  // no copy may land after this warp's shared memory is released
+}
+
 // Is every cell a strip loads an interior cell of an unmasked level?
 __device__ __forceinline__ bool strip_interior(const LevelInfo &L, int y_lo, int y_hi, int x_lo,
                                                int x_hi) {
   return L.code_off < 0 && y_lo >= 1 && y_hi <= L.ny - 2 && x_lo >= 1 && x_hi <= L.nx - 2;
 }
 
-template <typename T, int S1>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_down_s(Args<T> a) {
+// The fast FP32 strips take unmasked levels whose next level is unmasked and
+// whose row offsets fit 32 bits.
+__device__ __forceinline__ bool fast_levels(const LevelInfo &L, const LevelInfo &Lc) {
+  return L.code_off < 0 && Lc.code_off < 0 && (long long)(L.ny + 16) * L.pitch < (1LL << 31);
+}
+
+// Error word bit: a rectangle-only strip kernel met a level it does not handle
+// (the host launches those kernels only for levels without masked instances).
+constexpr unsigned kErrStrip = 8u;
+
+// CTAs per SM the strip kernels are compiled for: FP32 kernels with the
+// general (masked) strips need up to 128 (down) / 168 (up) registers; the
+// rectangle-only forms (ANY = false) fit more CTAs.
+template <typename T, bool ANY, bool UP>
+constexpr int strip_min_ctas() {
+  return sizeof(T) != 4 ? 1 : UP ? 3 : 4;  // four up CTAs (128 registers) spill: slower
+}
+
+template <typename T, int S1, bool ANY = true>
+__global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, false>()) k_down_s(Args<T> a) {
   using G = DownGeom<T, S1>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -529,12 +896,28 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 4 : 1) k_down_s(Arg
   const int y_start = (y_out0 - 1 - 2 * S1) & ~1;  // even, at least the rows the sweeps need
   const int y_last = max(2 * I_end + 2 * S1, y_out1 - 1 + 2 * S1 - 1);
   extern __shared__ __align__(16) unsigned char smem[];
-  if (strip_interior(L, y_start, y_last, xl, xl + 127))
-    down_strip<T, S1, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
-                            I_begin, I_end, smem);
-  else
-    down_strip<T, S1, false>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
-                             I_begin, I_end, smem);
+  const bool interior = strip_interior(L, y_start, y_last, xl, xl + 127);
+  if constexpr (sizeof(T) == 4) {
+    if (fast_levels(L, Lc)) {
+      if (interior)
+        down_strip_fast<S1, false>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0,
+                                   y_out1, I_begin, I_end, smem);
+      else
+        down_strip_fast<S1, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0,
+                                  y_out1, I_begin, I_end, smem);
+      return;
+    }
+  }
+  if constexpr (ANY) {
+    if (interior)
+      down_strip<T, S1, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
+                              I_begin, I_end, smem);
+    else
+      down_strip<T, S1, false>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0, y_out1,
+                               I_begin, I_end, smem);
+  } else if (lane == 0) {
+    atomicOr(a.counter + kErrWord, kErrStrip);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -593,10 +976,10 @@ __device__ __forceinline__ V4<T> coarse_interp(const Pair<T> &c) {
   if (lane == 0) lft = c.outer;
   if (lane == 31) rgt = c.outer;
   V4<T> h;
-  h.v[0] = T(0.75) * v0 + T(0.25) * lft;
-  h.v[1] = T(0.75) * v0 + T(0.25) * v1;
-  h.v[2] = T(0.75) * v1 + T(0.25) * v0;
-  h.v[3] = T(0.75) * v1 + T(0.25) * rgt;
+  h.v[0] = interp1(v0, lft);
+  h.v[1] = interp1(v0, v1);
+  h.v[2] = interp1(v1, v0);
+  h.v[3] = interp1(v1, rgt);
   return h;
 }
 
@@ -664,7 +1047,7 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
         const V4<T> &oth = (ph & 1) ? Ce[2] : Ce[0];  // y odd <=> ph odd (y_start even)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          u.v[j] = C.on(c, j) ? u.v[j] + T(0.75) * Ce[1].v[j] + T(0.25) * oth.v[j] : T(0);
+          u.v[j] = C.on(c, j) ? prolong1(u.v[j], Ce[1].v[j], oth.v[j]) : T(0);
         Uw[wslot<U>(ph, 0)] = u;
       }
       // post half sweep g runs on row y - g with colour g & 1, so its first
@@ -694,10 +1077,7 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
         }
         if (LEVEL0) {
           const V4<T> &bO = Bw[wslot<U>(ph, O)];
-          T acc = T(0);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc += bO.v[j] * v.v[j];
-          part += (double)acc;
+          part += (double)dot1(bO, v);
         }
       }
     }
@@ -706,10 +1086,195 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
   return part;
 }
 
+// Up on an FP32 strip of an unmasked level whose next level is unmasked: the
+// same cells and the same r.z partial as up_strip<float, S1, S2, LEVEL0, INT>,
+// bit for bit, laid out like down_strip_fast (RECT as there).  The coarse
+// correction's rows travel through the copy ring too: coarse row Y/2 + 1 is
+// copied in the commit group of fine row Y (Y even), so it has landed when
+// row Y is processed and is interpolated then.  The interpolated rows live in
+// a circular window of NC slots indexed by the coarse row's distance from the
+// strip's first one, so they rotate without moves.
+template <int S1, int S2, bool LEVEL0, bool RECT>
+__device__ __forceinline__ double up_strip_fast(const Args<float> &a, const LevelInfo &L,
+                                                const LevelInfo &Lc, const ClassTable<float> &tab,
+                                                int x0, bool out_lane, int y_start, int y_out0,
+                                                int y_out1, unsigned char *smem) {
+  using G = UpGeom<float, S1, S2>;
+  constexpr int U = G::U, O = G::O;
+  constexpr int P = FastGeom<U>::P, R = FastGeom<U>::R;
+  constexpr int NC = P / 2;  // coarse rows per pass; at least 3
+  static_assert(NC >= 3 && R == P, "coarse window");
+  const float2 q25 = splat2(0.25f), q75 = splat2(0.75f);
+  const P4 inv_i{splat2(tab.inv[1]), splat2(tab.inv[1])};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float *B = a.arena + L.b_off;
+  const float *Wp = a.arena + L.w_off;
+  const int c0 = x0 >> 1;  // x0 is a multiple of 4, so this is exact for negative x0 too
+  const float *E = a.arena + Lc.u_off;
+  float *Uo = a.arena + L.u_off + x0;
+  const int pitch = L.pitch;
+  const int y_last = y_out1 - 1 + O;
+  const bool edge_lane = lane == 0 || lane == 31;
+  const int outer_c = c0 + (lane == 0 ? -1 : 2);
+  LaneRect lr;
+  bool lane_in = true, full = true, neu = false, pair_in = true;
+  if constexpr (RECT) {
+    lr = lane_rect(L, tab, x0);
+    lane_in = x0 >= 0 && x0 < L.nx;
+    full = x0 + 3 < L.nx;
+    neu = L.bc == BC_NEU;
+    pair_in = c0 >= 0 && c0 + 1 < Lc.nx;
+  }
+  constexpr int kSlot = kThreads * 4;
+  float *rb = reinterpret_cast<float *>(smem) + threadIdx.x * 4;
+  float *rw = rb + R * kSlot;
+  // coarse ring: slot q holds the lane's two coarse columns and the warp's two
+  // outer columns of the coarse row copied with fine slot q
+  float2 *rc = reinterpret_cast<float2 *>(smem + (size_t)2 * R * kSlot * 4) + threadIdx.x;
+  float *ro = reinterpret_cast<float *>(smem + (size_t)2 * R * kSlot * 4 + (size_t)R * kThreads * 8) +
+              warp * 2 + (lane == 31);
+  constexpr int kCSlot = kThreads;  // float2 between two coarse slots of a lane
+  constexpr int kOSlot = kWarps * 2;
+  // copy of one coarse column into the ring: Neumann ghosts mirror the edge,
+  // Dirichlet ghosts and rows outside are zero
+  auto ccopy1 = [&](float *dst, const float *row, bool row_ok, int c) {
+    if (neu) c = min(max(c, 0), Lc.nx - 1);
+    const bool ok = row_ok && c >= 0 && c < Lc.nx;
+    __pipeline_memcpy_async(dst, ok ? row + c : E, 4, ok ? 0 : 4);
+  };
+  auto cissue = [&](int q, int cy) {
+    float2 *dv = rc + q * kCSlot;
+    float *dout = ro + q * kOSlot;
+    if constexpr (RECT) {
+      const int yy = neu ? min(max(cy, 0), Lc.ny - 1) : cy;
+      const bool row_ok = yy >= 0 && yy < Lc.ny;
+      const float *row = E + (row_ok ? yy : 0) * Lc.pitch;
+      if (pair_in) {
+        __pipeline_memcpy_async(dv, row_ok ? row + c0 : E, 8, row_ok ? 0 : 8);
+      } else {
+        ccopy1(reinterpret_cast<float *>(dv), row, row_ok, c0);
+        ccopy1(reinterpret_cast<float *>(dv) + 1, row, row_ok, c0 + 1);
+      }
+      if (edge_lane) ccopy1(dout, row, row_ok, outer_c);
+    } else {
+      // interior strips: every coarse row they use is in the grid; rows past the
+      // last are clamped and never used
+      const float *row = E + min(cy, Lc.ny - 1) * Lc.pitch;
+      __pipeline_memcpy_async(dv, row + c0, 8);
+      if (edge_lane) __pipeline_memcpy_async(dout, row + outer_c, 4);
+    }
+  };
+  auto cread = [&](int q) {
+    const float2 v = rc[q * kCSlot];
+    const float outer = edge_lane ? ro[q * kOSlot] : 0.f;
+    float lft = shfl_up1(v.y), rgt = shfl_dn1(v.x);
+    if (lane == 0) lft = outer;
+    if (lane == 31) rgt = outer;
+    const float2 m = mul2(q75, v);  // interp1(near, far) on both pairs
+    return P4{fma2(q25, make_float2(lft, v.x), m), fma2(q25, make_float2(v.y, rgt), m)};
+  };
+  auto issue = [&](int q, int y, int gofs) {
+    float *db = rb + q * kSlot, *dw = rw + q * kSlot;
+    if constexpr (RECT) {
+      const bool ok = lane_in && y >= 0 && y < L.ny;
+      __pipeline_memcpy_async(db, ok ? B + gofs + x0 : B, 16, ok ? 0 : 16);
+      __pipeline_memcpy_async(dw, ok ? Wp + gofs + x0 : Wp, 16, ok ? 0 : 16);
+    } else {
+      __pipeline_memcpy_async(db, B + gofs + x0, 16);
+      __pipeline_memcpy_async(dw, Wp + gofs + x0, 16);
+    }
+    if (!(y & 1)) cissue(q, (y >> 1) + 1);  // the coarse row interpolated at row y
+  };
+  P4 Bw[U], Uw[U], H[NC];
+  int Kw[U];  // row kinds of the window rows (RECT)
+#pragma unroll
+  for (int k = 0; k < U; ++k) { Bw[k] = zero_p4(); Uw[k] = zero_p4(); Kw[k] = 3; }
+  // coarse rows relative to cy0 = y_start / 2: window slot of row cy0 + k is
+  // k mod NC.  Rows cy0 - 1 and cy0 come through coarse slots 1 and 3, which
+  // the loop never uses (a coarse row travels with an even fine row, and even
+  // rows take even slots).
+  const int cy0 = y_start >> 1;
+  cissue(1, cy0 - 1);
+  cissue(3, cy0);
+  __pipeline_commit();
+  int gofs = y_start * pitch;
+#pragma unroll
+  for (int q = 0; q < R - 1; ++q) {
+    issue(q, y_start + q, gofs);
+    __pipeline_commit();
+    gofs += pitch;
+  }
+  __pipeline_wait_prior(R - 1);
+  H[NC - 1] = cread(1);
+  H[0] = cread(3);
+  int oofs = (y_start - O) * pitch;  // row offset of the output row of this step
+  double part = 0.0;
+  for (int base = y_start; base <= y_last; base += P) {
+#pragma unroll
+    for (int ph = 0; ph < P; ++ph) {
+      const int y = base + ph;
+      if (y > y_last) break;
+      __pipeline_wait_prior(R - 2);
+      const float4 qb = *reinterpret_cast<const float4 *>(rb + ph * kSlot);
+      const float4 qw = *reinterpret_cast<const float4 *>(rw + ph * kSlot);
+      const int c = ph >> 1;  // coarse row of y relative to the pass's first
+      if ((ph & 1) == 0) H[(c + 1) % NC] = cread(ph);  // coarse row c + 1 for rows 2c, 2c + 1
+      if (y + R - 1 <= y_last)  // no copy of rows past the strip; the slot read one step ago
+        issue((ph + P - 1) % P, y + R - 1, gofs);
+      __pipeline_commit();
+      gofs += pitch;
+      Bw[wslot<U>(ph, 0)] = split4(qb);
+      if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
+      auto inv_of = [&](int k) -> P4 {
+        if constexpr (RECT) return pick(lr.inv, Kw[wslot<U>(ph, k)]);
+        else return inv_i;
+      };
+      const P4 &hn = H[c % NC];
+      const P4 &hf = (ph & 1) ? H[(c + 1) % NC] : H[(c + NC - 1) % NC];
+      const P4 w = split4(qw);
+      P4 &u = Uw[wslot<U>(ph, 0)];
+      u.e = fma2(q25, hf.e, fma2(q75, hn.e, w.e));  // prolong1 on both pairs
+      u.o = fma2(q25, hf.o, fma2(q75, hn.o, w.o));
+      if constexpr (RECT) u = mask_on(u, lr.on, Kw[wslot<U>(ph, 0)]);
+      // post half sweep g on row y - g; its updated pair is the parity of y
+#pragma unroll
+      for (int g = 1; g <= 2 * S2; ++g) {
+        if ((ph & 1) == 0)
+          psweep<0>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                    Bw[wslot<U>(ph, g)], inv_of(g).e);
+        else
+          psweep<1>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                    Bw[wslot<U>(ph, g)], inv_of(g).o);
+      }
+      if (out_lane && y - O >= y_out0) {
+        P4 v = Uw[wslot<U>(ph, O)];
+        if constexpr (RECT) v = mask_on(v, lr.on, Kw[wslot<U>(ph, O)]);
+        const float4 q = join4(v);
+        if (full) {
+          *reinterpret_cast<float4 *>(Uo + oofs) = q;
+        } else {
+          const float vv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (x0 + j < L.nx) Uo[oofs + j] = vv[j];
+        }
+        if (LEVEL0) {
+          const P4 &bo = Bw[wslot<U>(ph, O)];
+          const float2 t = fma2(bo.o, v.o, mul2(bo.e, v.e));  // dot1
+          part += (double)__fadd_rn(t.x, t.y);
+        }
+      }
+      oofs += pitch;
+    }
+  }
+  __pipeline_wait_prior(0);
+  return part;
+}
+
 // FP32: three CTAs per SM (above 170 registers only two fit, which was measured
 // slower); the FP64 form needs more registers than that and is left unbounded.
-template <typename T, int S1, int S2, bool LEVEL0>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) k_up_s(Args<T> a) {
+template <typename T, int S1, int S2, bool LEVEL0, bool ANY = true>
+__global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, true>()) k_up_s(Args<T> a) {
   using G = UpGeom<T, S1, S2>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -732,12 +1297,29 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1) k_up_s(Args<
       const int y_start = (y_out0 - 2 * S2) & ~1;
       const int y_last = y_out1 - 1 + G::O;
       extern __shared__ __align__(16) unsigned char smem[];
-      if (strip_interior(L, y_start, y_last, xl, xl + 127))
-        part = up_strip<T, S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
-                                                 y_out1, smem);
-      else
-        part = up_strip<T, S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
-                                                  y_out1, smem);
+      const bool interior = strip_interior(L, y_start, y_last, xl, xl + 127);
+      bool fast = false;
+      if constexpr (sizeof(T) == 4) {
+        fast = fast_levels(L, Lc);
+        if (fast && interior)
+          part = up_strip_fast<S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start,
+                                                      y_out0, y_out1, smem);
+        else if (fast)
+          part = up_strip_fast<S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start,
+                                                     y_out0, y_out1, smem);
+      }
+      if constexpr (ANY) {
+        if (fast) {
+          // done above
+        } else if (interior)
+          part = up_strip<T, S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start,
+                                                   y_out0, y_out1, smem);
+        else
+          part = up_strip<T, S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start,
+                                                    y_out0, y_out1, smem);
+      } else if (!fast && lane == 0) {
+        atomicOr(a.counter + kErrWord, kErrStrip);
+      }
     }
   }
   if (!LEVEL0) return;

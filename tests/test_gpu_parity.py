@@ -167,6 +167,51 @@ def test_fp32_vcycle_matches_model(sweeps):
         assert _rel(z, ref) < 2e-5
 
 
+@pytest.mark.parametrize("sweeps", [1, 2, 3])
+def test_strip_height_does_not_change_the_vcycle(sweeps):
+    """The strip height decides which rows near the top and bottom edges a strip
+    on the interior path computes and which a strip on the general path does, so
+    with interior and general arithmetic defined per cell identically, V-cycles
+    with different strip heights give the same bits (two strip levels here:
+    1500 x 1400 and 750 x 700), FP32 and FP64."""
+    rng = np.random.default_rng(100 + sweeps)
+    shape = (1500, 1400)
+    r = torch.as_tensor(rng.standard_normal(shape))
+    for boundary in ("neumann", "dirichlet"):
+        for precision in ("mixed", "fp64"):
+            outs = []
+            for warps in (64, 1000, 1 << 20):  # level 0 on 64-, 16- and 8-row strips
+                plan = PoissonPlan([Instance(*shape, boundary)],
+                                   SolveParams(precision=precision, sweeps=sweeps,
+                                               strip_target_warps=warps))
+                outs.append(plan.apply_vcycle(0, r))
+                plan.close()
+            ref = M.vcycle(M.build_levels(shape, boundary), r.numpy(), sweeps=sweeps)
+            tol = 2e-5 if precision == "mixed" else 1e-11
+            assert _rel(outs[0].cpu().numpy(), ref) < tol, (boundary, precision)
+            for z in outs[1:]:
+                assert torch.equal(z, outs[0]), (boundary, precision)
+
+
+@pytest.mark.parametrize("shape", [(1500, 1400), (301, 517), (130, 90)])
+def test_full_mask_equals_dirichlet_rectangle(shape):
+    """A masked instance whose mask covers the whole rectangle is the Dirichlet
+    rectangle's system (walls of coefficient 1 on the finest level, 2 below), so
+    its V-cycle, which runs on the masked (general) strips, gives the same bits as
+    the rectangle's, which runs on the rectangle and interior strips."""
+    rng = np.random.default_rng(shape[0])
+    r = torch.as_tensor(rng.standard_normal(shape))
+    for precision in ("mixed", "fp64"):
+        rect = PoissonPlan([Instance(*shape, "dirichlet")], SolveParams(precision=precision))
+        z_rect = rect.apply_vcycle(0, r)
+        rect.close()
+        masked = PoissonPlan([Instance(*shape, "masked")], SolveParams(precision=precision))
+        masked.set_mask(0, torch.ones(shape, dtype=torch.uint8, device="cuda"))
+        z_mask = masked.apply_vcycle(0, r)
+        masked.close()
+        assert torch.equal(z_rect, z_mask), precision
+
+
 @pytest.mark.parametrize("bottom_cells", [64, 1024, 16384])
 def test_bottom_sizes_give_the_same_vcycle(bottom_cells):
     """Whichever level the one-CTA bottom starts at, the V-cycle is the same."""
