@@ -231,20 +231,21 @@ struct Runner {
   static void set_attrs() {
     cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kBottomSmem);
-    const int lvl = (int)st::strip_smem<T, S>();
-    cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, lvl);
+    const int dsm = (int)st::strip_smem<T, S, false>(), usm = (int)st::strip_smem<T, S, true>();
+    cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         lvl);
+                         usm);
     cudaFuncSetAttribute(st::k_up_s<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         lvl);
+                         usm);
     if constexpr (sizeof(T) == 4) {
-      const int fast = (int)st::strip_smem<T, S, false>();
+      const int fd = (int)st::strip_smem<T, S, false, false>();
+      const int fu = (int)st::strip_smem<T, S, true, false>();
       cudaFuncSetAttribute(st::k_down_s<T, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           fast);
+                           fd);
       cudaFuncSetAttribute(st::k_up_s<T, S, S, true, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, fast);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, fu);
       cudaFuncSetAttribute(st::k_up_s<T, S, S, false, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, fast);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, fu);
     }
     cudaFuncSetAttribute(tile::k_down_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)tile::DownT<T, S>::smem);
@@ -352,10 +353,10 @@ struct Runner {
       prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st, l);
       if (rect_only(p, l))
         chain_launch(p, st::k_down_s<T, S, false>, p->down_count[l], st::kThreads,
-                     st::strip_smem<T, S, false>(), st, at_tiles(a, p->down_base[l]));
+                     st::strip_smem<T, S, false, false>(), st, at_tiles(a, p->down_base[l]));
       else
         chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kThreads,
-                     st::strip_smem<T, S>(), st, at_tiles(a, p->down_base[l]));
+                     st::strip_smem<T, S, false>(), st, at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     if (p->tdown_count[l] > 0) {
@@ -387,11 +388,11 @@ struct Runner {
     const Args<T> at = at_tiles(a, p->up_base[l]);
     const int n = p->up_count[l];
     if (rect_only(p, l)) {
-      const size_t sm = st::strip_smem<T, S, false>();
+      const size_t sm = st::strip_smem<T, S, true, false>();
       if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true, false>, n, st::kThreads, sm, st, at);
       else chain_launch(p, st::k_up_s<T, S, S, false, false>, n, st::kThreads, sm, st, at);
     } else {
-      const size_t sm = st::strip_smem<T, S>();
+      const size_t sm = st::strip_smem<T, S, true>();
       if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true>, n, st::kThreads, sm, st, at);
       else chain_launch(p, st::k_up_s<T, S, S, false>, n, st::kThreads, sm, st, at);
     }

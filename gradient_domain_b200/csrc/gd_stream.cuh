@@ -593,8 +593,8 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
 template <int U>
 struct FastGeom {
   static constexpr int P = U >= 6 ? U : 2 * U;
-  // Ring slots per array (P - 1 rows in flight; 2P, alternating between the two
-  // halves, was measured no faster).
+  // Ring slots per array (P - 1 rows in flight per lane; 2P slots, the passes
+  // alternating between the two halves, was measured no faster).
   static constexpr int R = P;
   static_assert(P % U == 0 && P % 2 == 0 && (R == P || R == 2 * P), "interior strip pass");
 };
@@ -607,58 +607,70 @@ struct FastGeom {
 template <int R>
 constexpr size_t coarse_ring_bytes() { return (size_t)R * (kThreads * 8 + kWarps * 8); }
 
-template <typename T, int S, bool ANY = true>
+// The up kernels stream two arrays and the coarse rows, the down kernels one array.
+template <typename T, int S, bool UP, bool ANY = true>
 constexpr size_t strip_smem() {
   constexpr int R = FastGeom<2 * S + 2>::R;
-  const size_t fast = sizeof(T) == 4 ? (size_t)2 * R * kThreads * 16 + coarse_ring_bytes<R>() : 0;
+  const size_t fast = sizeof(T) != 4 ? 0
+                      : UP       ? (size_t)2 * R * kThreads * 16 + coarse_ring_bytes<R>()
+                                 : (size_t)R * kThreads * 16;
   if (!ANY) return fast;
   return level_smem<T>() > fast ? level_smem<T>() : fast;
 }
 
 // Per-lane constants of the fast strips on rectangle levels in any position
-// (RECT): which of the lane's four columns are in the grid, and the diagonal
-// inverse and negated diagonal of its cells, as same-colour pairs, for each
-// kind of row: 0, 1 or 2 walls (2: a level one row high).  Rows outside the
-// grid (kind 3) have no unknowns.  Values come from the class table, as in the
-// general strips.
+// (RECT): which of the lane's four columns are in the grid and how many walls
+// each has, and the diagonal inverse and negated diagonal of its cells in rows
+// without a wall, as same-colour pairs.  Rows with walls (1, or 2 on a level
+// one row high) look their cells' values up in the class table; rows outside
+// the grid (kind 3) have no unknowns.  Values come from the class table, as in
+// the general strips.
 struct LaneRect {
-  P4 inv[3], negd[3];
+  P4 inv0, negd0;
   unsigned on;  // bit j: column x0 + j is in the grid
+  unsigned wx;  // bits 2j, 2j + 1: walls of column x0 + j
 };
 
 __device__ __forceinline__ LaneRect lane_rect(const LevelInfo &L, const ClassTable<float> &tab,
                                               int x0) {
   LaneRect r;
   r.on = 0u;
-  float iv[3][4], nd[3][4];
+  r.wx = 0u;
+  float iv[4], nd[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int x = x0 + j;
     const bool in = x >= 0 && x < L.nx;
     const int wx = (x == 0) + (x == L.nx - 1);
     if (in) r.on |= 1u << j;
-#pragma unroll
-    for (int wy = 0; wy < 3; ++wy) {
-      const int c = in ? 1 + wy + wx : 0;
-      iv[wy][j] = tab.inv[c];
-      nd[wy][j] = -tab.d[c];
-    }
+    r.wx |= (unsigned)wx << (2 * j);
+    const int c = in ? 1 + wx : 0;
+    iv[j] = tab.inv[c];
+    nd[j] = -tab.d[c];
   }
-#pragma unroll
-  for (int wy = 0; wy < 3; ++wy) {
-    r.inv[wy] = P4{make_float2(iv[wy][0], iv[wy][2]), make_float2(iv[wy][1], iv[wy][3])};
-    r.negd[wy] = P4{make_float2(nd[wy][0], nd[wy][2]), make_float2(nd[wy][1], nd[wy][3])};
-  }
+  r.inv0 = P4{make_float2(iv[0], iv[2]), make_float2(iv[1], iv[3])};
+  r.negd0 = P4{make_float2(nd[0], nd[2]), make_float2(nd[1], nd[3])};
   return r;
+}
+
+// Diagonal inverse (NEG = false) or negated diagonal (NEG = true) of the lane's
+// cells in a row of kind `kind`.
+template <bool NEG>
+__device__ __forceinline__ P4 rect_diag(const LaneRect &lr, const ClassTable<float> &tab,
+                                        int kind) {
+  if (kind == 0) return NEG ? lr.negd0 : lr.inv0;
+  float v[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = (kind < 3 && ((lr.on >> j) & 1u)) ? 1 + kind + (int)((lr.wx >> (2 * j)) & 3u) : 0;
+    v[j] = NEG ? -tab.d[c] : tab.inv[c];
+  }
+  return P4{make_float2(v[0], v[2]), make_float2(v[1], v[3])};
 }
 
 // Kind of row y: walls (0, 1, 2), or 3 outside the grid.
 __device__ __forceinline__ int row_kind(const LevelInfo &L, int y) {
   return (y < 0 || y >= L.ny) ? 3 : (y == 0) + (y == L.ny - 1);
-}
-
-__device__ __forceinline__ P4 pick(const P4 (&t)[3], int kind) {
-  return kind == 0 ? t[0] : kind == 1 ? t[1] : kind == 2 ? t[2] : zero_p4();
 }
 
 // Zero the cells of a row that have no unknown (rows outside the grid, columns
@@ -700,6 +712,9 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
   bool lane_in = true, full = true, neu = false;
   int J0 = x0 >> 1;  // x0 is a multiple of 4, so this is exact for negative x0 too
   bool st0 = true, st1 = true;  // coarse columns J0, J0 + 1 are in the coarse grid
+  // the warp's 128 columns are all interior columns (no wall, none outside)
+  const int xl = x0 - 4 * (int)(threadIdx.x & 31);
+  const bool cols_plain = xl >= 1 && xl + 127 <= L.nx - 2;
   if constexpr (RECT) {
     lr = lane_rect(L, tab, x0);
     lane_in = x0 >= 0 && x0 < L.nx;
@@ -748,28 +763,68 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
       P4 &b0 = Bw[wslot<U>(ph, 0)];
       b0 = split4(qb);
       if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
-      auto inv_of = [&](int k) -> P4 {
-        if constexpr (RECT) return pick(lr.inv, Kw[wslot<U>(ph, k)]);
-        else return inv_i;
-      };
-      // first half sweep (colour 0) from a zero iterate on row y
-      if ((ph & 1) == 0) {
-        Uw[wslot<U>(ph, 0)].e = mul2(b0.e, inv_of(0).e);
-        Uw[wslot<U>(ph, 0)].o = make_float2(0.f, 0.f);
-      } else {
-        Uw[wslot<U>(ph, 0)].o = mul2(b0.o, inv_of(0).o);
-        Uw[wslot<U>(ph, 0)].e = make_float2(0.f, 0.f);
-      }
-      // half sweep h on row y - (h - 1); its updated pair is the parity of y
+      // rectangle strips: every row the step touches (y - U + 1 .. y) has no wall
+      // and is in the grid (kv = 0, per-lane constants), or some row is special
+      // (kv = 1, per-row kinds); one copy runs, chosen by a warp-uniform branch
+      const bool rows_plain = !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
 #pragma unroll
-      for (int h = 2; h <= 2 * S1; ++h) {
-        const int k = h - 1;
-        if ((ph & 1) == 0)
-          psweep<0>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
-                    Bw[wslot<U>(ph, k)], inv_of(k).e);
-        else
-          psweep<1>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
-                    Bw[wslot<U>(ph, k)], inv_of(k).o);
+      for (int kv = 0; kv < (RECT ? 2 : 1); ++kv) {
+        if ((kv == 1) == rows_plain) continue;
+        const bool kinds = kv == 1;
+        auto inv_of = [&](int k) -> P4 {
+          if constexpr (RECT) return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
+          else return inv_i;
+        };
+        // first half sweep (colour 0) from a zero iterate on row y
+        if ((ph & 1) == 0) {
+          Uw[wslot<U>(ph, 0)].e = mul2(b0.e, inv_of(0).e);
+          Uw[wslot<U>(ph, 0)].o = make_float2(0.f, 0.f);
+        } else {
+          Uw[wslot<U>(ph, 0)].o = mul2(b0.o, inv_of(0).o);
+          Uw[wslot<U>(ph, 0)].e = make_float2(0.f, 0.f);
+        }
+        // half sweep h on row y - (h - 1); its updated pair is the parity of y
+#pragma unroll
+        for (int h = 2; h <= 2 * S1; ++h) {
+          const int k = h - 1;
+          if ((ph & 1) == 0)
+            psweep<0>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                      Bw[wslot<U>(ph, k)], inv_of(k).e);
+          else
+            psweep<1>(Uw[wslot<U>(ph, k)], Uw[wslot<U>(ph, k + 1)], Uw[wslot<U>(ph, k - 1)],
+                      Bw[wslot<U>(ph, k)], inv_of(k).o);
+        }
+        // residual of row y - K and its horizontal restriction
+        const P4 &uK = Uw[wslot<U>(ph, K)], &upK = Uw[wslot<U>(ph, K + 1)];
+        const P4 &dnK = Uw[wslot<U>(ph, K - 1)], &bK = Bw[wslot<U>(ph, K)];
+        const float left = shfl_up1(uK.o.y), right = shfl_dn1(uK.e.x);
+        P4 nd{negd_i, negd_i};
+        if constexpr (RECT) nd = kinds ? rect_diag<true>(lr, tab, Kw[wslot<U>(ph, K)]) : lr.negd0;
+        P4 r;
+        r.e = fma2(nd.e, uK.e, nsum2(upK.e, uK.o, make_float2(left, uK.o.x), bK.e, dnK.e));
+        r.o = fma2(nd.o, uK.o, nsum2(upK.o, uK.e, make_float2(uK.e.y, right), bK.o, dnK.o));
+        if constexpr (RECT) {
+          if (kinds) r = mask_on(r, lr.on, Kw[wslot<U>(ph, K)]);
+          else if (!cols_plain) r = mask_on(r, lr.on, 0);
+        }
+        const float e0 = shfl_up1(r.o.y), e5 = shfl_dn1(r.e.x);
+        float2 fA = make_float2(e0, r.o.x), fB = r.e, fC = r.o, fD = make_float2(r.e.y, e5);
+        if constexpr (RECT) {
+          if (neu && !cols_plain) {  // Neumann ghosts of the restriction mirror the edge cells
+            float e[6] = {e0, r.e.x, r.o.x, r.e.y, r.o.y, e5};
+            if (x0 == 0) e[0] = e[1];
+            if (!(L.nx & 1)) {
+              const int mr = L.nx - x0;
+#pragma unroll
+              for (int m = 0; m <= 4; ++m)
+                if (m == mr) e[m + 1] = e[m];
+            }
+            fA = make_float2(e[0], e[2]); fB = make_float2(e[1], e[3]);
+            fC = make_float2(e[2], e[4]); fD = make_float2(e[3], e[5]);
+          }
+        }
+        // (weigh1(e0, e1, e2, e3), weigh1(e2, e3, e4, e5))
+        F[wslot<U>(ph, K)] = fma2(q25, fD, fma2(q75, fC, fma2(q75, fB, mul2(q25, fA))));
       }
       {  // row y - KP has seen every pre-sweep: keep it for the up kernel
         const int yw = y - KP;
@@ -786,35 +841,6 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
         }
         wofs += pitch;
       }
-      // residual of row y - K and its horizontal restriction
-      const P4 &uK = Uw[wslot<U>(ph, K)], &upK = Uw[wslot<U>(ph, K + 1)];
-      const P4 &dnK = Uw[wslot<U>(ph, K - 1)], &bK = Bw[wslot<U>(ph, K)];
-      const float left = shfl_up1(uK.o.y), right = shfl_dn1(uK.e.x);
-      P4 nd;
-      if constexpr (RECT) nd = pick(lr.negd, Kw[wslot<U>(ph, K)]);
-      else nd = P4{negd_i, negd_i};
-      P4 r;
-      r.e = fma2(nd.e, uK.e, nsum2(upK.e, uK.o, make_float2(left, uK.o.x), bK.e, dnK.e));
-      r.o = fma2(nd.o, uK.o, nsum2(upK.o, uK.e, make_float2(uK.e.y, right), bK.o, dnK.o));
-      if constexpr (RECT) r = mask_on(r, lr.on, Kw[wslot<U>(ph, K)]);
-      float e0 = shfl_up1(r.o.y), e5 = shfl_dn1(r.e.x);
-      float2 fA = make_float2(e0, r.o.x), fB = r.e, fC = r.o, fD = make_float2(r.e.y, e5);
-      if constexpr (RECT) {
-        if (neu) {  // Neumann ghosts of the restriction mirror the edge cells
-          float e[6] = {e0, r.e.x, r.o.x, r.e.y, r.o.y, e5};
-          if (x0 == 0) e[0] = e[1];
-          if (!(L.nx & 1)) {
-            const int mr = L.nx - x0;
-#pragma unroll
-            for (int m = 0; m <= 4; ++m)
-              if (m == mr) e[m + 1] = e[m];
-          }
-          fA = make_float2(e[0], e[2]); fB = make_float2(e[1], e[3]);
-          fC = make_float2(e[2], e[4]); fD = make_float2(e[3], e[5]);
-        }
-      }
-      // (weigh1(e0, e1, e2, e3), weigh1(e2, e3, e4, e5))
-      F[wslot<U>(ph, K)] = fma2(q25, fD, fma2(q75, fC, fma2(q75, fB, mul2(q25, fA))));
       // coarse row I = (y - K) / 2 - 1 from the restricted rows 2I-1 .. 2I+2
       if ((ph & 1) == 0) {
         const int I = ((y - K) >> 1) - 1;
@@ -1103,7 +1129,7 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
   constexpr int U = G::U, O = G::O;
   constexpr int P = FastGeom<U>::P, R = FastGeom<U>::R;
   constexpr int NC = P / 2;  // coarse rows per pass; at least 3
-  static_assert(NC >= 3 && R == P, "coarse window");
+  static_assert(NC >= 3, "coarse window");
   const float2 q25 = splat2(0.25f), q75 = splat2(0.75f);
   const P4 inv_i{splat2(tab.inv[1]), splat2(tab.inv[1])};
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1118,6 +1144,9 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
   const int outer_c = c0 + (lane == 0 ? -1 : 2);
   LaneRect lr;
   bool lane_in = true, full = true, neu = false, pair_in = true;
+  // the warp's 128 columns are all interior columns (no wall, none outside)
+  const int xl = x0 - 4 * lane;
+  const bool cols_plain = xl >= 1 && xl + 127 <= L.nx - 2;
   if constexpr (RECT) {
     lr = lane_rect(L, tab, x0);
     lane_in = x0 >= 0 && x0 < L.nx;
@@ -1209,46 +1238,64 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
   H[0] = cread(3);
   int oofs = (y_start - O) * pitch;  // row offset of the output row of this step
   double part = 0.0;
+  int half = 0;  // ring slot of this pass's first row (0 or P when R == 2P)
   for (int base = y_start; base <= y_last; base += P) {
+    const int prev = R == P ? 0 : (half ^ P);  // half the slot before ph = 0 is in
 #pragma unroll
     for (int ph = 0; ph < P; ++ph) {
       const int y = base + ph;
       if (y > y_last) break;
       __pipeline_wait_prior(R - 2);
-      const float4 qb = *reinterpret_cast<const float4 *>(rb + ph * kSlot);
-      const float4 qw = *reinterpret_cast<const float4 *>(rw + ph * kSlot);
+      const float4 qb = *reinterpret_cast<const float4 *>(rb + (half + ph) * kSlot);
+      const float4 qw = *reinterpret_cast<const float4 *>(rw + (half + ph) * kSlot);
       const int c = ph >> 1;  // coarse row of y relative to the pass's first
-      if ((ph & 1) == 0) H[(c + 1) % NC] = cread(ph);  // coarse row c + 1 for rows 2c, 2c + 1
+      if ((ph & 1) == 0) H[(c + 1) % NC] = cread(half + ph);  // row c + 1 for rows 2c, 2c + 1
       if (y + R - 1 <= y_last)  // no copy of rows past the strip; the slot read one step ago
-        issue((ph + P - 1) % P, y + R - 1, gofs);
+        issue(ph > 0 ? half + ph - 1 : prev + P - 1, y + R - 1, gofs);
       __pipeline_commit();
       gofs += pitch;
       Bw[wslot<U>(ph, 0)] = split4(qb);
       if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
-      auto inv_of = [&](int k) -> P4 {
-        if constexpr (RECT) return pick(lr.inv, Kw[wslot<U>(ph, k)]);
-        else return inv_i;
-      };
       const P4 &hn = H[c % NC];
       const P4 &hf = (ph & 1) ? H[(c + 1) % NC] : H[(c + NC - 1) % NC];
       const P4 w = split4(qw);
-      P4 &u = Uw[wslot<U>(ph, 0)];
-      u.e = fma2(q25, hf.e, fma2(q75, hn.e, w.e));  // prolong1 on both pairs
-      u.o = fma2(q25, hf.o, fma2(q75, hn.o, w.o));
-      if constexpr (RECT) u = mask_on(u, lr.on, Kw[wslot<U>(ph, 0)]);
-      // post half sweep g on row y - g; its updated pair is the parity of y
+      // rectangle strips: per-lane constants when every row the step touches
+      // (y - U + 1 .. y) has no wall and is in the grid (kv = 0), per-row kinds
+      // otherwise (kv = 1); one copy runs, chosen by a warp-uniform branch
+      const bool rows_plain = !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
+      P4 v;  // the output row y - O
 #pragma unroll
-      for (int g = 1; g <= 2 * S2; ++g) {
-        if ((ph & 1) == 0)
-          psweep<0>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
-                    Bw[wslot<U>(ph, g)], inv_of(g).e);
-        else
-          psweep<1>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
-                    Bw[wslot<U>(ph, g)], inv_of(g).o);
+      for (int kv = 0; kv < (RECT ? 2 : 1); ++kv) {
+        if ((kv == 1) == rows_plain) continue;
+        const bool kinds = kv == 1;
+        auto inv_of = [&](int k) -> P4 {
+          if constexpr (RECT) return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
+          else return inv_i;
+        };
+        P4 &u = Uw[wslot<U>(ph, 0)];
+        u.e = fma2(q25, hf.e, fma2(q75, hn.e, w.e));  // prolong1 on both pairs
+        u.o = fma2(q25, hf.o, fma2(q75, hn.o, w.o));
+        if constexpr (RECT) {
+          if (kinds) u = mask_on(u, lr.on, Kw[wslot<U>(ph, 0)]);
+          else if (!cols_plain) u = mask_on(u, lr.on, 0);
+        }
+        // post half sweep g on row y - g; its updated pair is the parity of y
+#pragma unroll
+        for (int g = 1; g <= 2 * S2; ++g) {
+          if ((ph & 1) == 0)
+            psweep<0>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                      Bw[wslot<U>(ph, g)], inv_of(g).e);
+          else
+            psweep<1>(Uw[wslot<U>(ph, g)], Uw[wslot<U>(ph, g + 1)], Uw[wslot<U>(ph, g - 1)],
+                      Bw[wslot<U>(ph, g)], inv_of(g).o);
+        }
+        v = Uw[wslot<U>(ph, O)];
+        if constexpr (RECT) {
+          if (kinds) v = mask_on(v, lr.on, Kw[wslot<U>(ph, O)]);
+          else if (!cols_plain) v = mask_on(v, lr.on, 0);
+        }
       }
       if (out_lane && y - O >= y_out0) {
-        P4 v = Uw[wslot<U>(ph, O)];
-        if constexpr (RECT) v = mask_on(v, lr.on, Kw[wslot<U>(ph, O)]);
         const float4 q = join4(v);
         if (full) {
           *reinterpret_cast<float4 *>(Uo + oofs) = q;
@@ -1266,6 +1313,7 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
       }
       oofs += pitch;
     }
+    if constexpr (R != P) half ^= P;
   }
   __pipeline_wait_prior(0);
   return part;
