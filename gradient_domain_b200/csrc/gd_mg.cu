@@ -231,21 +231,19 @@ struct Runner {
   static void set_attrs() {
     cudaFuncSetAttribute(k_bottom<T, S, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kBottomSmem);
-    const int dsm = (int)st::strip_smem<T, S, false>(), usm = (int)st::strip_smem<T, S, true>();
-    cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
+    cudaFuncSetAttribute(st::k_down_s<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)down_smem<S>(false));
     cudaFuncSetAttribute(st::k_up_s<T, S, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         usm);
+                         (int)up_smem<S, true>(false));
     cudaFuncSetAttribute(st::k_up_s<T, S, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         usm);
+                         (int)up_smem<S, false>(false));
     if constexpr (sizeof(T) == 4) {
-      const int fd = (int)st::strip_smem<T, S, false, false>();
-      const int fu = (int)st::strip_smem<T, S, true, false>();
       cudaFuncSetAttribute(st::k_down_s<T, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           fd);
+                           (int)down_smem<S>(true));
       cudaFuncSetAttribute(st::k_up_s<T, S, S, true, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, fu);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem<S, true>(true));
       cudaFuncSetAttribute(st::k_up_s<T, S, S, false, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, fu);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem<S, false>(true));
     }
     cudaFuncSetAttribute(tile::k_down_t<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)tile::DownT<T, S>::smem);
@@ -347,16 +345,27 @@ struct Runner {
   // strip kernels (FP32), which fit more CTAs per SM.
   static bool rect_only(gd_plan p, int l) { return sizeof(T) == 4 && !p->strip_any[l]; }
 
+  // Dynamic shared memory of the strip kernels (rectangle-only forms or not).
+  template <int S>
+  static size_t down_smem(bool rect) {
+    return rect ? st::strip_smem<T, S, false, false>() : st::strip_smem<T, S, false>();
+  }
+  template <int S, bool LEVEL0>
+  static size_t up_smem(bool rect) {
+    constexpr int NT = st::UpCta<LEVEL0>::NT;
+    return rect ? st::strip_smem<T, S, true, false, NT>() : st::strip_smem<T, S, true, true, NT>();
+  }
+
   template <int S>
   static void down_level(gd_plan p, const Args<T> &a, cudaStream_t st, int l) {
     if (p->down_count[l] > 0) {
       prof_begin(p, l == 0 ? GD_K_DOWN0 : GD_K_DOWN, p->launch_cells[2 * l], st, l);
       if (rect_only(p, l))
-        chain_launch(p, st::k_down_s<T, S, false>, p->down_count[l], st::kThreads,
-                     st::strip_smem<T, S, false, false>(), st, at_tiles(a, p->down_base[l]));
+        chain_launch(p, st::k_down_s<T, S, false>, p->down_count[l], st::kSThreads,
+                     down_smem<S>(true), st, at_tiles(a, p->down_base[l]));
       else
-        chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kThreads,
-                     st::strip_smem<T, S, false>(), st, at_tiles(a, p->down_base[l]));
+        chain_launch(p, st::k_down_s<T, S>, p->down_count[l], st::kSThreads,
+                     down_smem<S>(false), st, at_tiles(a, p->down_base[l]));
       prof_end(p, st);
     }
     if (p->tdown_count[l] > 0) {
@@ -387,15 +396,16 @@ struct Runner {
     prof_begin(p, l == 0 ? GD_K_UP0 : GD_K_UP, p->launch_cells[2 * l + 1], st, l);
     const Args<T> at = at_tiles(a, p->up_base[l]);
     const int n = p->up_count[l];
-    if (rect_only(p, l)) {
-      const size_t sm = st::strip_smem<T, S, true, false>();
-      if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true, false>, n, st::kThreads, sm, st, at);
-      else chain_launch(p, st::k_up_s<T, S, S, false, false>, n, st::kThreads, sm, st, at);
-    } else {
-      const size_t sm = st::strip_smem<T, S, true>();
-      if (l == 0) chain_launch(p, st::k_up_s<T, S, S, true>, n, st::kThreads, sm, st, at);
-      else chain_launch(p, st::k_up_s<T, S, S, false>, n, st::kThreads, sm, st, at);
-    }
+    constexpr int NT0 = st::UpCta<true>::NT, NT1 = st::UpCta<false>::NT;
+    const bool rect = rect_only(p, l);
+    if (rect && l == 0)
+      chain_launch(p, st::k_up_s<T, S, S, true, false>, n, NT0, up_smem<S, true>(true), st, at);
+    else if (rect)
+      chain_launch(p, st::k_up_s<T, S, S, false, false>, n, NT1, up_smem<S, false>(true), st, at);
+    else if (l == 0)
+      chain_launch(p, st::k_up_s<T, S, S, true>, n, NT0, up_smem<S, true>(false), st, at);
+    else
+      chain_launch(p, st::k_up_s<T, S, S, false>, n, NT1, up_smem<S, false>(false), st, at);
     prof_end(p, st);
   }
 
@@ -719,7 +729,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     for (int i = 0; i < p->n; ++i) {
       if (bottoms[i] <= l || on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[p->inst[i].level0 + l];
-      const int rows = st::kWarps * F.rows_per_warp;
+      const int rows = st::kSWarps * F.rows_per_warp;
       for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
         for (int tx = 0; tx < ceil_div(F.nx, down_ow); ++tx)
           p->tiles.push_back(Tile{p->inst[i].level0 + l, i, ty, tx});
@@ -732,7 +742,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       InstInfo &I = p->inst[i];
       if (bottoms[i] <= l || on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[I.level0 + l];
-      const int rows = st::kWarps * F.rows_per_warp;
+      const int rows = (l == 0 ? st::UpCta<true>::W : st::UpCta<false>::W) * F.rows_per_warp;
       if (l == 0) I.up0_begin = (int)p->tiles.size() - p->up_base[0];
       for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
         for (int tx = 0; tx < ceil_div(F.nx, up_ow); ++tx)

@@ -25,8 +25,21 @@ namespace gd {
 namespace st {
 
 constexpr int kLanes = 32;
-constexpr int kWarps = 4;          // warps per CTA
+constexpr int kWarps = 4;          // warps per CTA of the Krylov and refresh kernels
 constexpr int kThreads = kWarps * kLanes;
+// The down / up kernels run one warp (one strip) per CTA: the block scheduler
+// then spreads a launch's strips evenly over the SMs (a launch of four-warp
+// CTAs that fits one wave left some SMs one CTA short of others).
+constexpr int kSWarps = 1;
+constexpr int kSThreads = kSWarps * kLanes;
+// ... except the level-0 up kernel, whose CTAs each add an r.z partial and
+// take a ticket for the last-CTA reduction: four warps per CTA keep those
+// fences and atomics four times fewer (one warp per CTA was measured slower).
+template <bool LEVEL0>
+struct UpCta {
+  static constexpr int W = LEVEL0 ? 4 : 1;
+  static constexpr int NT = W * kLanes;
+};
 constexpr int kKrylovRows = 16;    // rows per warp in the Krylov kernels
 constexpr int kKrylovCols = 128;   // columns per warp (and per CTA)
 
@@ -191,11 +204,11 @@ __device__ __forceinline__ void shift(unsigned (&w)[N]) {
 // (FP32) contiguous bytes per slot, free of bank conflicts.
 constexpr int kRing = 8;
 
-template <typename T>
+template <typename T, int NT = kThreads>
 struct Ring {
   T *base;
   __device__ __forceinline__ explicit Ring(T *smem) : base(smem + threadIdx.x * 4) {}
-  __device__ __forceinline__ T *slot(int s) const { return base + (s & (kRing - 1)) * kThreads * 4; }
+  __device__ __forceinline__ T *slot(int s) const { return base + (s & (kRing - 1)) * NT * 4; }
   // Copy A[y, x0 .. x0 + 3] into slot s, or zeros when the row or lane is outside the grid.
   __device__ __forceinline__ void issue(int s, const T *A, const LevelInfo &L, int y, int x0) const {
     const bool ok = y >= 0 && y < L.ny && x0 >= 0 && x0 < L.nx;
@@ -211,11 +224,12 @@ struct Ring {
 };
 
 // Per-lane ring of packed cell classes of masked levels (4 bytes per row).
+template <int NT = kThreads>
 struct CodeRing {
   unsigned *base;
   __device__ __forceinline__ explicit CodeRing(unsigned *smem) : base(smem + threadIdx.x) {}
   __device__ __forceinline__ unsigned *slot(int s) const {
-    return base + (s & (kRing - 1)) * kThreads;
+    return base + (s & (kRing - 1)) * NT;
   }
   __device__ __forceinline__ void issue(int s, const LevelInfo &L, const unsigned char *codes,
                                         int y, int x0) const {
@@ -242,17 +256,20 @@ struct EdgeRing {
 };
 
 // Cell classes of row y: computed for rectangles, from the ring for masks.
-__device__ __forceinline__ unsigned classes_at(const LevelInfo &L, const CodeRing &cr, int s,
+template <int NT>
+__device__ __forceinline__ unsigned classes_at(const LevelInfo &L, const CodeRing<NT> &cr, int s,
                                                int y, int x0) {
   if (L.code_off >= 0) return cr.read(s);
   return row_classes(L, nullptr, y, x0);
 }
 
 // Dynamic shared memory of the streaming kernels (rings).
-template <typename T>
-constexpr size_t ring_bytes() { return (size_t)kRing * kThreads * 4 * sizeof(T); }
-template <typename T>
-constexpr size_t level_smem() { return 2 * ring_bytes<T>() + (size_t)kRing * kThreads * 4; }
+template <typename T, int NT = kThreads>
+constexpr size_t ring_bytes() { return (size_t)kRing * NT * 4 * sizeof(T); }
+template <typename T, int NT = kSThreads>
+constexpr size_t level_smem() {
+  return 2 * ring_bytes<T, NT>() + (size_t)kRing * NT * 4;
+}
 template <typename T>
 constexpr size_t edge_bytes() { return (size_t)kRing * kThreads * sizeof(T); }
 
@@ -459,8 +476,8 @@ __device__ __forceinline__ void down_strip(const Args<T> &a, const LevelInfo &L,
   T *Bc = a.arena + Lc.b_off;
   T *Wp = a.arena + L.w_off;
   const bool store_lane = out_lane && x0 >= 0 && x0 < L.nx;
-  const Ring<T> ring(reinterpret_cast<T *>(smem));
-  const CodeRing cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T>()));
+  const Ring<T, kSThreads> ring(reinterpret_cast<T *>(smem));
+  const CodeRing<kSThreads> cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T, kSThreads>()));
   V4<T> Bw[U], Uw[U], F[U];
   unsigned Cw[U];
 #pragma unroll
@@ -604,18 +621,19 @@ struct FastGeom {
 // alone.
 // Coarse-row ring of the fast up strips: per slot 8 bytes per lane (the lane's
 // two coarse columns) and 8 bytes per warp (the columns just outside it).
-template <int R>
-constexpr size_t coarse_ring_bytes() { return (size_t)R * (kThreads * 8 + kWarps * 8); }
+template <int R, int NT>
+constexpr size_t coarse_ring_bytes() { return (size_t)R * (NT * 8 + (NT / kLanes) * 8); }
 
-// The up kernels stream two arrays and the coarse rows, the down kernels one array.
-template <typename T, int S, bool UP, bool ANY = true>
+// The up kernels stream two arrays and the coarse rows, the down kernels one
+// array; NT threads per CTA.
+template <typename T, int S, bool UP, bool ANY = true, int NT = kSThreads>
 constexpr size_t strip_smem() {
   constexpr int R = FastGeom<2 * S + 2>::R;
   const size_t fast = sizeof(T) != 4 ? 0
-                      : UP       ? (size_t)2 * R * kThreads * 16 + coarse_ring_bytes<R>()
-                                 : (size_t)R * kThreads * 16;
+                      : UP       ? (size_t)2 * R * NT * 16 + coarse_ring_bytes<R, NT>()
+                                 : (size_t)R * NT * 16;
   if (!ANY) return fast;
-  return level_smem<T>() > fast ? level_smem<T>() : fast;
+  return level_smem<T, NT>() > fast ? level_smem<T, NT>() : fast;
 }
 
 // Per-lane constants of the fast strips on rectangle levels in any position
@@ -704,7 +722,7 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
   float *Wp = a.arena + L.w_off + x0;
   const int pitch = L.pitch;
   float *ring = reinterpret_cast<float *>(smem) + threadIdx.x * 4;
-  constexpr int kSlot = kThreads * 4;  // floats between two slots of a lane
+  constexpr int kSlot = kSThreads * 4;  // floats between two slots of a lane
   // interior: one diagonal for every cell
   const P4 inv_i{splat2(tab.inv[1]), splat2(tab.inv[1])};
   const float2 negd_i = splat2(-tab.d[1]);
@@ -893,13 +911,15 @@ constexpr unsigned kErrStrip = 8u;
 // CTAs per SM the strip kernels are compiled for: FP32 kernels with the
 // general (masked) strips need up to 128 (down) / 168 (up) registers; the
 // rectangle-only forms (ANY = false) fit more CTAs.
-template <typename T, bool ANY, bool UP>
+template <typename T, bool UP, int NT>
 constexpr int strip_min_ctas() {
-  return sizeof(T) != 4 ? 1 : UP ? 3 : 4;  // four up CTAs (128 registers) spill: slower
+  // FP32: 12 up warps per SM (16 at 128 registers spilled: slower), 16 down warps
+  return sizeof(T) != 4 ? 1 : (UP ? 12 : 16) * kLanes / NT;
 }
 
 template <typename T, int S1, bool ANY = true>
-__global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, false>()) k_down_s(Args<T> a) {
+__global__ void __launch_bounds__(kSThreads, strip_min_ctas<T, false, kSThreads>())
+    k_down_s(Args<T> a) {
   using G = DownGeom<T, S1>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -911,7 +931,7 @@ __global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, false>()) k_d
   fill_table(tab, L.wall);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int RB = L.rows_per_warp;  // even
-  const int y_out0 = (tl.ty * kWarps + warp) * RB;
+  const int y_out0 = (tl.ty * kSWarps + warp) * RB;
   if (y_out0 >= L.ny) return;
   const int xl = tl.tx * H::OW - 4 * H::HL;
   const int x0 = xl + 4 * lane;
@@ -1033,9 +1053,10 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
   for (int q = 0; q < 3; ++q) Ce[q] = coarse_interp(coarse_pair(E, Lc, ce_top + q, x0, neu));
   Pair<T> next0 = coarse_pair(E, Lc, ce_top + 3, x0, neu);
   Pair<T> next1 = coarse_pair(E, Lc, ce_top + 4, x0, neu);
-  const Ring<T> rb(reinterpret_cast<T *>(smem));
-  const Ring<T> rw(reinterpret_cast<T *>(smem) + kRing * kThreads * 4);
-  const CodeRing cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T>()));
+  constexpr int NT = UpCta<LEVEL0>::NT;
+  const Ring<T, NT> rb(reinterpret_cast<T *>(smem));
+  const Ring<T, NT> rw(reinterpret_cast<T *>(smem) + kRing * NT * 4);
+  const CodeRing<NT> cring(reinterpret_cast<unsigned *>(smem + 2 * ring_bytes<T, NT>()));
   for (int q = 0; q < kRing - 1; ++q) {
     rb.issue(q, B, L, y_start + q, x0);
     rw.issue(q, Wp, L, y_start + q, x0);
@@ -1154,16 +1175,17 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
     neu = L.bc == BC_NEU;
     pair_in = c0 >= 0 && c0 + 1 < Lc.nx;
   }
-  constexpr int kSlot = kThreads * 4;
+  constexpr int NT = UpCta<LEVEL0>::NT;
+  constexpr int kSlot = NT * 4;
   float *rb = reinterpret_cast<float *>(smem) + threadIdx.x * 4;
   float *rw = rb + R * kSlot;
   // coarse ring: slot q holds the lane's two coarse columns and the warp's two
   // outer columns of the coarse row copied with fine slot q
   float2 *rc = reinterpret_cast<float2 *>(smem + (size_t)2 * R * kSlot * 4) + threadIdx.x;
-  float *ro = reinterpret_cast<float *>(smem + (size_t)2 * R * kSlot * 4 + (size_t)R * kThreads * 8) +
+  float *ro = reinterpret_cast<float *>(smem + (size_t)2 * R * kSlot * 4 + (size_t)R * NT * 8) +
               warp * 2 + (lane == 31);
-  constexpr int kCSlot = kThreads;  // float2 between two coarse slots of a lane
-  constexpr int kOSlot = kWarps * 2;
+  constexpr int kCSlot = NT;  // float2 between two coarse slots of a lane
+  constexpr int kOSlot = (NT / kLanes) * 2;
   // copy of one coarse column into the ring: Neumann ghosts mirror the edge,
   // Dirichlet ghosts and rows outside are zero
   auto ccopy1 = [&](float *dst, const float *row, bool row_ok, int c) {
@@ -1322,7 +1344,8 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
 // FP32: three CTAs per SM (above 170 registers only two fit, which was measured
 // slower); the FP64 form needs more registers than that and is left unbounded.
 template <typename T, int S1, int S2, bool LEVEL0, bool ANY = true>
-__global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, true>()) k_up_s(Args<T> a) {
+__global__ void __launch_bounds__(UpCta<LEVEL0>::NT, strip_min_ctas<T, true, UpCta<LEVEL0>::NT>())
+    k_up_s(Args<T> a) {
   using G = UpGeom<T, S1, S2>;
   using H = typename G::H;
   __shared__ ClassTable<T> tab;
@@ -1336,7 +1359,7 @@ __global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, true>()) k_up
     fill_table(tab, L.wall);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int RB = L.rows_per_warp;
-    const int y_out0 = (tl.ty * kWarps + warp) * RB;
+    const int y_out0 = (tl.ty * UpCta<LEVEL0>::W + warp) * RB;
     if (y_out0 < L.ny) {
       const int y_out1 = min(y_out0 + RB, L.ny);
       const int xl = tl.tx * H::OW - 4 * H::HL;
@@ -1371,7 +1394,7 @@ __global__ void __launch_bounds__(kThreads, strip_min_ctas<T, ANY, true>()) k_up
     }
   }
   if (!LEVEL0) return;
-  part = block_sum<kThreads>(part);
+  part = block_sum<UpCta<LEVEL0>::NT>(part);
   if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
   if (!last_block(a.counter + 3)) return;
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
