@@ -4,7 +4,10 @@
 Default workload (one GPU): tone-mapping-style Neumann integration of a
 4096 x 4096 x 3 radiance map (16.8 MP per channel, three channels solved as
 one batched plan), mixed precision (FP32 V-cycle, FP64 residual refresh and
-accumulator) to a true relative residual of 1e-8.  One step = one batched
+accumulator) to a true relative residual of 1e-8.  The plan's sweeps and kernel
+geometry come from the project's autotuner, run on the plan's own right-hand
+sides before the measurement (``--no-tune``: ``--sweeps`` and the default
+geometry; the choice is in ``config.autotuned``).  One step = one batched
 solve of the three channels from x0 = 0.  ``value`` is whole-job Mpix/s
 (channels x pixels / step time, device-timed, inputs resident in HBM);
 ``e2e`` repeats the measurement through the public API with pinned host
@@ -24,6 +27,7 @@ ranks of the device time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -212,9 +216,18 @@ def ours(args) -> None:
     x = torch.empty_like(f)
     insts = [Instance(size, size, "neumann", zero_mean=True) for _ in range(n_ch)]
     # every solve starts from zero (as the reference's solve_neumann); x is only written
-    plan = PoissonPlan(insts, SolveParams(precision="mixed", tolerance=args.tol,
-                                          sweeps=args.sweeps, reliable_delta=args.delta,
-                                          zero_start=True))
+    params = SolveParams(precision="mixed", tolerance=args.tol, sweeps=args.sweeps,
+                         reliable_delta=args.delta, zero_start=True)
+    tuning = None
+    if not args.no_tune:
+        # the plan's sweeps and kernel geometry come from the autotuner, timed on this
+        # plan's own right-hand sides before the measurement (untimed)
+        from gradient_domain_b200 import autotune
+        t0 = time.perf_counter()
+        params = autotune.tune(insts, params, rhs=list(f), reps=3, force=True, scale=-1.0)
+        tuning = {name: getattr(params, name) for name, _ in autotune.SPACE}
+        tuning["seconds"] = round(time.perf_counter() - t0, 2)
+    plan = PoissonPlan(insts, params)
     stream = torch.cuda.current_stream()
 
     def step(p):
@@ -283,8 +296,7 @@ def ours(args) -> None:
         extra["oracle_seconds"] = time.perf_counter() - t0
 
     # FP64 MGPCG on the same workload (the precision baseline)
-    plan64 = PoissonPlan(insts, SolveParams(precision="fp64", tolerance=args.tol,
-                                            sweeps=args.sweeps, zero_start=True))
+    plan64 = PoissonPlan(insts, dataclasses.replace(params, precision="fp64"))
     for _ in range(2):  # the second solve builds the plan's graph
         step(plan64)
     barrier()
@@ -460,7 +472,7 @@ def ours(args) -> None:
     refreshes = max(r.refreshes for r in results)
     launches = args.steps * (2 + 1 + max(its) * (per_iter + 2) + refreshes + 1)
 
-    smoother = smoother_gate(size, hbm, kinds, args.sweeps) if rank == 0 else None
+    smoother = smoother_gate(size, hbm, kinds, params.sweeps) if rank == 0 else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
@@ -468,7 +480,8 @@ def ours(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32/fp64-mixed", "data": "synthetic",
         "config": {"workload": f"tonemap-neumann {size}x{size}x{n_ch}", "tolerance": args.tol,
-                   "sweeps": args.sweeps, "reliable_delta": args.delta, "instances_per_gpu": n_ch,
+                   "sweeps": params.sweeps, "autotuned": tuning, "reliable_delta": args.delta,
+                   "instances_per_gpu": n_ch,
                    "l2": "inputs larger than L2 (3 x 134 MB rhs + solution + hierarchy)",
                    "parallelism": f"replicas x{world}"},
         "clocks": clock,
@@ -877,6 +890,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the oracle and CPU baseline")
     ap.add_argument("--no-port", action="store_true",
                     help="skip the literal GPU port of the reference mgcg")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="headline plan with --sweeps and default geometry instead of the "
+                         "autotuner's choice")
     ap.add_argument("--channels", type=int, default=3)
     ap.add_argument("--solve-only", action="store_true",
                     help="only the mixed-precision solves (small profiling runs): no FP64 plan, "

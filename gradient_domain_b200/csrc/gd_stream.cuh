@@ -911,14 +911,15 @@ constexpr unsigned kErrStrip = 8u;
 // CTAs per SM the strip kernels are compiled for: FP32 kernels with the
 // general (masked) strips need up to 128 (down) / 168 (up) registers; the
 // rectangle-only forms (ANY = false) fit more CTAs.
-template <typename T, bool UP, int NT>
+template <typename T, bool UP, int NT, int S>
 constexpr int strip_min_ctas() {
-  // FP32: 12 up warps per SM (16 at 128 registers spilled: slower), 16 down warps
-  return sizeof(T) != 4 ? 1 : (UP ? 12 : 16) * kLanes / NT;
+  // FP32: 12 up warps per SM (16 at 128 registers spilled: slower), 16 down
+  // warps (12 with three sweeps, whose longer window needs more registers)
+  return sizeof(T) != 4 ? 1 : (UP || S > 2 ? 12 : 16) * kLanes / NT;
 }
 
 template <typename T, int S1, bool ANY = true>
-__global__ void __launch_bounds__(kSThreads, strip_min_ctas<T, false, kSThreads>())
+__global__ void __launch_bounds__(kSThreads, strip_min_ctas<T, false, kSThreads, S1>())
     k_down_s(Args<T> a) {
   using G = DownGeom<T, S1>;
   using H = typename G::H;
@@ -1344,7 +1345,8 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
 // FP32: three CTAs per SM (above 170 registers only two fit, which was measured
 // slower); the FP64 form needs more registers than that and is left unbounded.
 template <typename T, int S1, int S2, bool LEVEL0, bool ANY = true>
-__global__ void __launch_bounds__(UpCta<LEVEL0>::NT, strip_min_ctas<T, true, UpCta<LEVEL0>::NT>())
+__global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
+                                  strip_min_ctas<T, true, UpCta<LEVEL0>::NT, S2>())
     k_up_s(Args<T> a) {
   using G = UpGeom<T, S1, S2>;
   using H = typename G::H;
