@@ -5,8 +5,10 @@ after the coarse correction); the B200 solver exposes the knobs that set how
 its kernels tile the work, and the best values depend on the level sizes, the
 number of instances in a plan and the boundary type:
 
-* ``strip_target_warps`` - the height of the register-streaming strips (the
-  tallest of 64/32/16/8 rows that still gives this many warps per launch);
+* ``strip_target_warps`` - the height of the register-streaming strips: 0 (the
+  default) chooses the height with the fewest waves x rows per launch, a
+  positive value the tallest of 64/32/16/8 rows that still gives this many
+  warps per launch;
 * ``tile_cells`` - the largest coarse level run on shared-memory tiles rather
   than strips;
 * ``bottom_cells`` - the largest level solved inside the one-CTA bottom kernel;
@@ -48,7 +50,7 @@ from .plan import Instance, PoissonPlan, SolveParams
 # (parameter, candidate values); the first value of each is the default of SolveParams
 SPACE: tuple[tuple[str, tuple[int, ...]], ...] = (
     ("sweeps", (2, 1, 3)),
-    ("strip_target_warps", (1800, 900, 3600)),
+    ("strip_target_warps", (0, 900, 3600)),
     ("tile_cells", (262144, 65536, 1048576)),
     ("bottom_cells", (4096, 1024, 16384)),
 )

@@ -455,6 +455,46 @@ struct Runner {
     else if (s == 2) set_attrs<2>();
     else set_attrs<3>();
   }
+
+  // What one wave of the strip kernels holds on the whole GPU: down warps,
+  // level-0 up CTAs (of UpCta<true>::W warps) and coarse up warps; the
+  // rectangle-only forms when `rect`.  Zero where the occupancy query failed.
+  template <int S>
+  static void strip_capacity(gd_plan p, bool rect, long long cap[3]) {
+    auto occ = [&](const void *kernel, int threads, size_t smem) -> long long {
+      int blocks = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        blocks = 0;
+      }
+      return (long long)blocks * p->sms;
+    };
+    constexpr int NT0 = st::UpCta<true>::NT, NT1 = st::UpCta<false>::NT;
+    bool done = false;
+    if constexpr (sizeof(T) == 4) {
+      if (rect) {
+        cap[0] = occ((const void *)st::k_down_s<T, S, false>, st::kSThreads, down_smem<S>(true));
+        cap[1] = occ((const void *)st::k_up_s<T, S, S, true, false>, NT0, up_smem<S, true>(true));
+        cap[2] = occ((const void *)st::k_up_s<T, S, S, false, false>, NT1,
+                     up_smem<S, false>(true));
+        done = true;
+      }
+    }
+    if (!done) {
+      cap[0] = occ((const void *)st::k_down_s<T, S>, st::kSThreads, down_smem<S>(false));
+      cap[1] = occ((const void *)st::k_up_s<T, S, S, true>, NT0, up_smem<S, true>(false));
+      cap[2] = occ((const void *)st::k_up_s<T, S, S, false>, NT1, up_smem<S, false>(false));
+    }
+    cap[0] *= st::kSWarps;
+    cap[2] *= st::UpCta<false>::W;
+  }
+  static void dispatch_capacity(gd_plan p, bool rect, long long cap[3]) {
+    const int s = p->prm.pre_sweeps;
+    if (s == 1) strip_capacity<1>(p, rect, cap);
+    else if (s == 2) strip_capacity<2>(p, rect, cap);
+    else strip_capacity<3>(p, rect, cap);
+  }
   static void dispatch_iteration(gd_plan p, const Args<T> &a, cudaStream_t st,
                                  bool refresh = true) {
     const int s = p->prm.pre_sweeps;
@@ -533,24 +573,65 @@ int choose_bottom(gd_plan p, int level0, int last, size_t es) {
   return last;
 }
 
-// Strip height of level l: the tallest of 64, 32, 16, 8 rows that still gives
-// `target` warps over the level-l strips of all instances (one launch), else 8.
-// Taller strips amortise the warm-up rows; shorter ones keep enough warps in
-// flight on small levels and in plans with few instances, where the strips'
-// per-warp row chain would otherwise set the launch time.
-int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int ow, int target) {
+// Strip height (rows per warp, even) of level l.
+//
+// target > 0: the tallest of 64, 32, 16, 8 rows that still gives `target` warps
+// over the level-l strips of all instances (one launch), else 8.
+//
+// target == 0 (the default): the height that minimises the launch time modelled
+// as waves x rows a warp walks, for the down and the up launch together.  A
+// strip walks its rows plus its warm-up rows (4 S + 2 for down, 4 S for up);
+// a wave is what the GPU holds at once (cap: down warps, level-0 up CTAs of
+// UpCta<true>::W warps, coarse up warps; resident warps each walk their strip
+// in parallel).  A launch that overflows a wave by a few strips pays a whole
+// second wave, and a launch of few tall strips leaves each warp a long row
+// chain; the model avoids both (e.g. 2048 x 2048 x 3: 68 rows and one wave
+// instead of 64 rows and 1.03 waves).  `only` >= 0: that instance alone.
+int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int down_ow, int up_ow,
+               const long long cap[3], int target, int only = -1) {
   const long long tile_max = p->prm.tile_cells > 0 ? p->prm.tile_cells : kTileCells;
-  for (int rb = 64; rb >= 8; rb >>= 1) {
-    long long warps = 0;
-    for (int i = 0; i < p->n; ++i) {
-      if (l >= bottoms[i]) continue;
-      const LevelInfo &L = p->lv[p->inst[i].level0 + l];
-      if (l >= 1 && (long long)L.ny * L.nx <= tile_max) continue;  // on the tile kernels
-      warps += (long long)ceil_div(L.nx, ow) * ceil_div(L.ny, rb);
+  auto strip_level = [&](int i) {
+    if (only >= 0 && i != only) return false;
+    if (l >= bottoms[i]) return false;
+    const LevelInfo &L = p->lv[p->inst[i].level0 + l];
+    return !(l >= 1 && (long long)L.ny * L.nx <= tile_max);  // else on the tile kernels
+  };
+  if (target > 0) {
+    const int ow = std::min(down_ow, up_ow);
+    for (int rb = 64; rb >= 8; rb >>= 1) {
+      long long warps = 0;
+      for (int i = 0; i < p->n; ++i) {
+        if (!strip_level(i)) continue;
+        const LevelInfo &L = p->lv[p->inst[i].level0 + l];
+        warps += (long long)ceil_div(L.nx, ow) * ceil_div(L.ny, rb);
+      }
+      if (warps >= target) return rb;
     }
-    if (warps >= target) return rb;
+    return 8;
   }
-  return 8;
+  const int s = p->prm.pre_sweeps;
+  const long long cd = cap[0] > 0 ? cap[0] : 12LL * p->sms;
+  const int upw = l == 0 ? st::UpCta<true>::W : st::UpCta<false>::W;
+  const long long cu = l == 0 ? (cap[1] > 0 ? cap[1] : 3LL * p->sms)
+                              : (cap[2] > 0 ? cap[2] : 12LL * p->sms);
+  long long best_cost = -1;
+  int best = 8;
+  for (int rb = 256; rb >= 8; rb -= 2) {
+    long long sd = 0, su = 0;
+    for (int i = 0; i < p->n; ++i) {
+      if (!strip_level(i)) continue;
+      const LevelInfo &L = p->lv[p->inst[i].level0 + l];
+      sd += (long long)ceil_div(L.nx, down_ow) * ceil_div(L.ny, rb);
+      su += (long long)ceil_div(L.nx, up_ow) * ceil_div(L.ny, upw * rb);
+    }
+    if (sd == 0) return 8;
+    const long long cost = ((sd + cd - 1) / cd) * (rb + 4 * s + 2) + ((su + cu - 1) / cu) * (rb + 4 * s);
+    if (best_cost < 0 || cost < best_cost) {  // ties keep the taller strips
+      best_cost = cost;
+      best = rb;
+    }
+  }
+  return best;
 }
 
 template <typename T>
@@ -659,11 +740,24 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
   }
   int down_ow = 0, up_ow = 0;
   strip_widths(p, &down_ow, &up_ow);
-  const int target_warps = p->prm.strip_target_warps > 0 ? p->prm.strip_target_warps : 1800;
+  const int target_warps = std::max(p->prm.strip_target_warps, 0);
+  long long cap[3] = {0, 0, 0};
+  {
+    bool any_masked = false;
+    for (int i = 0; i < p->n; ++i) any_masked = any_masked || p->inst[i].bc == BC_MASK;
+    if (p->fp64) Runner<double>::dispatch_capacity(p, false, cap);
+    else Runner<float>::dispatch_capacity(p, !any_masked, cap);
+  }
   for (int l = 0; l < p->depth; ++l) {
-    const int rb = strip_rows(p, bottoms, l, std::min(down_ow, up_ow), target_warps);
+    // Level 0's strip height sets how the r.z partial sums are grouped, so it
+    // depends on the instance alone: an instance gives the same bits in any
+    // batch.  Coarse levels have no reduction and share the launch's height.
+    const bool own = l == 0 && target_warps == 0;
+    const int rb = own ? 0 : strip_rows(p, bottoms, l, down_ow, up_ow, cap, target_warps);
     for (int i = 0; i < p->n; ++i)
-      if (l < bottoms[i]) p->lv[p->inst[i].level0 + l].rows_per_warp = rb;
+      if (l < bottoms[i])
+        p->lv[p->inst[i].level0 + l].rows_per_warp =
+            own ? strip_rows(p, bottoms, l, down_ow, up_ow, cap, 0, i) : rb;
   }
   p->fine_base = (int)p->tiles.size();
   for (int i = 0; i < p->n; ++i) {
@@ -872,9 +966,10 @@ extern "C" int gd_plan_create(const gd_grid_desc *grids, int32_t n, const gd_par
     p->persistent = params->persistent_coarse == 1 && coop != 0;
   }
   p->mask_set.assign(n, 0);
-  build_plan(p, grids);
+  // kernel attributes first: the strip heights depend on the kernels' occupancy
   if (p->fp64) Runner<double>::dispatch_attrs(p->prm.pre_sweeps);
   else Runner<float>::dispatch_attrs(p->prm.pre_sweeps);
+  build_plan(p, grids);
   // the limits above are constants every plan sets alike; a failure (no device in a
   // CPU-only check) must not stay behind as this thread's last error, where a later
   // launch check would report it as its own

@@ -27,7 +27,7 @@ BOUNDARIES = {"dirichlet": GD_DIRICHLET, "neumann": GD_NEUMANN, "masked": GD_MAS
 
 # values of the SolveParams fields that None leaves to the library (or to the autotuner's
 # cached choice for the plan's shape class, see autotune.resolve)
-DEFAULTS = {"precision": "mixed", "sweeps": 2, "strip_target_warps": 1800, "bottom_cells": 0,
+DEFAULTS = {"precision": "mixed", "sweeps": 2, "strip_target_warps": 0, "bottom_cells": 0,
             "tile_cells": 0}
 
 
@@ -47,7 +47,7 @@ class SolveParams:
     reliable_delta: float = 1e-4  # residual drop between FP64 residual refreshes
     check_every: int = 4          # host poll interval of solves on direct launches
     use_graph: bool = True        # from a plan's second solve on: one graph, device-side loop
-    strip_target_warps: int | None = None  # smoother strip height: warps per level launch (1800)
+    strip_target_warps: int | None = None  # strip height: 0 = fewest waves x rows, else warps per launch
     bottom_cells: int | None = None  # largest level solved inside the one-CTA bottom (0 = 4096)
     tile_cells: int | None = None    # largest coarse level on shared-memory tiles (0 = 262144)
     zero_start: bool = False      # start from x = 0; x is only written (need not be zeroed)
