@@ -573,12 +573,15 @@ int choose_bottom(gd_plan p, int level0, int last, size_t es) {
   return last;
 }
 
-// Strip height (rows per warp, even) of level l.
+// Level 0's default strip rule: warps per launch.
+constexpr int kLevel0TargetWarps = 1800;
+
+// Strip height (rows per warp, a multiple of st::kRzRows) of level l.
 //
 // target > 0: the tallest of 64, 32, 16, 8 rows that still gives `target` warps
 // over the level-l strips of all instances (one launch), else 8.
 //
-// target == 0 (the default): the height that minimises the launch time modelled
+// target == 0 (the default on coarse levels): the height that minimises the launch time modelled
 // as waves x rows a warp walks, for the down and the up launch together.  A
 // strip walks its rows plus its warm-up rows (4 S + 2 for down, 4 S for up);
 // a wave is what the GPU holds at once (cap: down warps, level-0 up CTAs of
@@ -586,12 +589,11 @@ int choose_bottom(gd_plan p, int level0, int last, size_t es) {
 // in parallel).  A launch that overflows a wave by a few strips pays a whole
 // second wave, and a launch of few tall strips leaves each warp a long row
 // chain; the model avoids both (e.g. 2048 x 2048 x 3: 68 rows and one wave
-// instead of 64 rows and 1.03 waves).  `only` >= 0: that instance alone.
+// instead of 64 rows and 1.03 waves).
 int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int down_ow, int up_ow,
-               const long long cap[3], int target, int only = -1) {
+               const long long cap[3], int target) {
   const long long tile_max = p->prm.tile_cells > 0 ? p->prm.tile_cells : kTileCells;
   auto strip_level = [&](int i) {
-    if (only >= 0 && i != only) return false;
     if (l >= bottoms[i]) return false;
     const LevelInfo &L = p->lv[p->inst[i].level0 + l];
     return !(l >= 1 && (long long)L.ny * L.nx <= tile_max);  // else on the tile kernels
@@ -616,7 +618,7 @@ int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int down
                               : (cap[2] > 0 ? cap[2] : 12LL * p->sms);
   long long best_cost = -1;
   int best = 8;
-  for (int rb = 256; rb >= 8; rb -= 2) {
+  for (int rb = 256; rb >= st::kRzRows; rb -= st::kRzRows) {
     long long sd = 0, su = 0;
     for (int i = 0; i < p->n; ++i) {
       if (!strip_level(i)) continue;
@@ -749,15 +751,13 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     else Runner<float>::dispatch_capacity(p, !any_masked, cap);
   }
   for (int l = 0; l < p->depth; ++l) {
-    // Level 0's strip height sets how the r.z partial sums are grouped, so it
-    // depends on the instance alone: an instance gives the same bits in any
-    // batch.  Coarse levels have no reduction and share the launch's height.
-    const bool own = l == 0 && target_warps == 0;
-    const int rb = own ? 0 : strip_rows(p, bottoms, l, down_ow, up_ow, cap, target_warps);
+    // level 0 keeps the warps-per-launch rule by default: one wave of tall strips
+    // was measured slower there (4096 x 4096 x 3: 256 rows, up0 170 -> 295 us per
+    // launch) than several waves of 64-row strips
+    const int target = (l == 0 && target_warps == 0) ? kLevel0TargetWarps : target_warps;
+    const int rb = strip_rows(p, bottoms, l, down_ow, up_ow, cap, target);
     for (int i = 0; i < p->n; ++i)
-      if (l < bottoms[i])
-        p->lv[p->inst[i].level0 + l].rows_per_warp =
-            own ? strip_rows(p, bottoms, l, down_ow, up_ow, cap, 0, i) : rb;
+      if (l < bottoms[i]) p->lv[p->inst[i].level0 + l].rows_per_warp = rb;
   }
   p->fine_base = (int)p->tiles.size();
   for (int i = 0; i < p->n; ++i) {
@@ -830,6 +830,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     }
     p->down_count[l] = (int)p->tiles.size() - p->down_base[l];
   }
+  int rz_parts = 0;
   for (int l = 0; l < p->depth; ++l) {
     p->up_base[l] = (int)p->tiles.size();
     for (int i = 0; i < p->n; ++i) {
@@ -837,15 +838,18 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       if (bottoms[i] <= l || on_tiles(i, l)) continue;
       const LevelInfo &F = p->lv[I.level0 + l];
       const int rows = (l == 0 ? st::UpCta<true>::W : st::UpCta<false>::W) * F.rows_per_warp;
-      if (l == 0) I.up0_begin = (int)p->tiles.size() - p->up_base[0];
+      if (l == 0) {  // the instance's r.z group partials (st::RzGroups)
+        I.up0_begin = rz_parts;
+        rz_parts += ceil_div(F.ny, st::kRzRows) * ceil_div(F.nx, up_ow);
+        I.up0_end = rz_parts;
+      }
       for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)
         for (int tx = 0; tx < ceil_div(F.nx, up_ow); ++tx)
           p->tiles.push_back(Tile{I.level0 + l, i, ty, tx});
-      if (l == 0) I.up0_end = (int)p->tiles.size() - p->up_base[0];
     }
     p->up_count[l] = (int)p->tiles.size() - p->up_base[l];
   }
-  p->max_partials = std::max(1, std::max(p->fine_count, p->depth > 0 ? p->up_count[0] : 0));
+  p->max_partials = std::max(1, std::max(p->fine_count, rz_parts));
   p->launch_cells.assign(2 * std::max(p->depth, 1), 0.0);
   p->fine_cells = 0;
   for (int i = 0; i < p->n; ++i) {

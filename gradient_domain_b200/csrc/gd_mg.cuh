@@ -77,7 +77,7 @@ struct InstInfo {
   long long r_off, p_off, d_off, z_off, q_off;  // p is double-buffered: p_off / q_off
   long long xs_off;  // the plan's own FP64 copy of the solution (element offset, row pitch `pitch`)
   int fine_begin, fine_end;  // tile range in the fine map
-  int up0_begin, up0_end;    // tile range in the level-0 up map (empty if bottom is level 0)
+  int up0_begin, up0_end;    // range of its r.z group partials (empty if bottom is level 0)
   int zero_mean, pad;
   // set per solve
   const double *f;

@@ -80,33 +80,6 @@ __device__ __forceinline__ V4<T> zero4() {
   return r;
 }
 
-// Per-level constants: 1/d and d for each wall count 0..4 (classes 1..5).
-template <typename T>
-struct Diag {
-  T d[5], inv[5];
-  __device__ __forceinline__ void init(float wall) {
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double dd = 4.0 - (double)k * (1.0 - (double)wall);
-      d[k] = (T)dd;
-      inv[k] = dd > 0.0 ? (T)(1.0 / dd) : T(0);
-    }
-  }
-  // class 0 (no unknown) -> 0
-  __device__ __forceinline__ T inv_of(int c) const {
-    T r = T(0);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) r = (c == k + 1) ? inv[k] : r;
-    return r;
-  }
-  __device__ __forceinline__ T d_of(int c) const {
-    T r = T(0);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) r = (c == k + 1) ? d[k] : r;
-    return r;
-  }
-};
-
 // Classes of the 4 cells x0..x0+3 of row y, packed one byte each.
 __device__ __forceinline__ unsigned row_classes(const LevelInfo &L, const unsigned char *codes,
                                                 int y, int x0) {
@@ -130,71 +103,10 @@ __device__ __forceinline__ unsigned row_classes(const LevelInfo &L, const unsign
 
 __device__ __forceinline__ int cls(unsigned packed, int j) { return (packed >> (8 * j)) & 0xff; }
 
-// Row of T values at (y, x0..x0+3); zero outside the grid.
-template <typename T>
-__device__ __forceinline__ V4<T> load_row(const T *A, const LevelInfo &L, int y, int x0) {
-  if (y < 0 || y >= L.ny || x0 < 0 || x0 >= L.nx) return zero4<T>();
-  return ld4(A + (long long)y * L.pitch + x0);
-}
-
 template <typename T>
 __device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 template <typename T>
 __device__ __forceinline__ T shfl_dn1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
-
-// One red-black half sweep of colour `colour` on row window U[k] (row y_k):
-// cells j with (y_k + x0 + j) odd/even = colour; x0 is a multiple of 4.
-template <typename T>
-__device__ __forceinline__ void half_sweep(V4<T> &u, const V4<T> &up, const V4<T> &dn,
-                                           const V4<T> &b, unsigned c, const Diag<T> &D,
-                                           int yk, int colour) {
-  const int j0 = (colour + yk) & 1;  // warp-uniform
-  if (j0 == 0) {
-    const T left = shfl_up1(u.v[3]);
-    u.v[0] = (b.v[0] + up.v[0] + dn.v[0] + left + u.v[1]) * D.inv_of(cls(c, 0));
-    u.v[2] = (b.v[2] + up.v[2] + dn.v[2] + u.v[1] + u.v[3]) * D.inv_of(cls(c, 2));
-  } else {
-    const T right = shfl_dn1(u.v[0]);
-    u.v[1] = (b.v[1] + up.v[1] + dn.v[1] + u.v[0] + u.v[2]) * D.inv_of(cls(c, 1));
-    u.v[3] = (b.v[3] + up.v[3] + dn.v[3] + u.v[2] + right) * D.inv_of(cls(c, 3));
-  }
-}
-
-// First half sweep from a zero iterate: only the cells of the colour change.
-template <typename T>
-__device__ __forceinline__ void half_sweep_from_zero(V4<T> &u, const V4<T> &b, unsigned c,
-                                                     const Diag<T> &D, int yk) {
-  const int j0 = yk & 1;  // colour 0
-#pragma unroll
-  for (int j = 0; j < 4; ++j) u.v[j] = ((j & 1) == j0) ? b.v[j] * D.inv_of(cls(c, j)) : T(0);
-}
-
-// A u on one row: d u - (up + down + left + right), zero where there is no unknown.
-template <typename T>
-__device__ __forceinline__ V4<T> apply_row(const V4<T> &u, const V4<T> &up, const V4<T> &dn,
-                                           T left, T right, unsigned c, const Diag<T> &D) {
-  V4<T> r;
-  const T lf[4] = {left, u.v[0], u.v[1], u.v[2]};
-  const T rt[4] = {u.v[1], u.v[2], u.v[3], right};
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int cj = cls(c, j);
-    r.v[j] = cj ? D.d_of(cj) * u.v[j] - (up.v[j] + dn.v[j] + lf[j] + rt[j]) : T(0);
-  }
-  return r;
-}
-
-template <typename T, int N>
-__device__ __forceinline__ void shift(V4<T> (&w)[N]) {
-#pragma unroll
-  for (int k = N - 1; k > 0; --k) w[k] = w[k - 1];
-}
-
-template <int N>
-__device__ __forceinline__ void shift(unsigned (&w)[N]) {
-#pragma unroll
-  for (int k = N - 1; k > 0; --k) w[k] = w[k - 1];
-}
 
 // Per-lane ring of RS row slices (4 elements each) in shared memory, filled
 // with cp.async so that RS - 1 rows per lane are in flight while the current
@@ -254,14 +166,6 @@ struct EdgeRing {
   }
   __device__ __forceinline__ T read(int s) const { return *slot(s); }
 };
-
-// Cell classes of row y: computed for rectangles, from the ring for masks.
-template <int NT>
-__device__ __forceinline__ unsigned classes_at(const LevelInfo &L, const CodeRing<NT> &cr, int s,
-                                               int y, int x0) {
-  if (L.code_off >= 0) return cr.read(s);
-  return row_classes(L, nullptr, y, x0);
-}
 
 // Dynamic shared memory of the streaming kernels (rings).
 template <typename T, int NT = kThreads>
@@ -978,6 +882,28 @@ struct UpGeom {
   static constexpr int U = O + 2;    // rows in every circular window (even)
 };
 
+// r.z partials of the level-0 up kernel: one per kRzRows-row group and column
+// strip, at a fixed place (the instance's base + group x column strips +
+// column strip), so their grouping does not depend on the strip height (strip
+// heights are multiples of kRzRows): a warp adds its lanes' products over the
+// group's rows and writes the group's warp sum when the group ends.  The last
+// CTA of the launch sums an instance's partials in index order, so an instance
+// gives the same r.z whatever strip heights its batch chose.
+constexpr int kRzRows = 8;
+struct RzGroups {
+  double *base;  // partial of group 0 of this column strip
+  int stride;    // column strips of the instance
+  double acc;    // this lane's share of the open group
+  __device__ __forceinline__ void add(double v) { acc += v; }
+  __device__ __forceinline__ void row_done(int yo, int y_out1) {
+    if ((yo & (kRzRows - 1)) == kRzRows - 1 || yo == y_out1 - 1) {
+      const double sum = warp_sum(acc);  // xor tree: the same sum in every lane
+      if ((threadIdx.x & 31) == 0) base[(yo / kRzRows) * stride] = sum;
+      acc = 0.0;
+    }
+  }
+};
+
 // The lane's two coarse values (columns x0/2, x0/2 + 1) of coarse row cy, with
 // Neumann ghosts mirrored and Dirichlet ghosts zero.
 // Lanes 0 and 31 also load the coarse column just outside the warp (c0 - 1,
@@ -1031,10 +957,10 @@ __device__ __forceinline__ V4<T> coarse_interp(const Pair<T> &c) {
 }
 
 template <typename T, int S1, int S2, bool LEVEL0, bool INT>
-__device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
-                                           const LevelInfo &Lc, const ClassTable<T> &tab, int x0,
-                                           bool out_lane, int y_start, int y_out0, int y_out1,
-                                           unsigned char *smem) {
+__device__ __forceinline__ void up_strip(const Args<T> &a, const LevelInfo &L,
+                                         const LevelInfo &Lc, const ClassTable<T> &tab, int x0,
+                                         bool out_lane, int y_start, int y_out0, int y_out1,
+                                         RzGroups &rz, unsigned char *smem) {
   using G = UpGeom<T, S1, S2>;
   constexpr int U = G::U, O = G::O;
   const Coef<T, INT> C{tab, tab.d[1], tab.inv[1]};
@@ -1064,7 +990,6 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
     if (!INT && masked) cring.issue(q, L, a.codes, y_start + q, x0);
     __pipeline_commit();
   }
-  double part = 0.0;
   for (int base = y_start; base <= y_last; base += U) {
 #pragma unroll
     for (int ph = 0; ph < U; ++ph) {
@@ -1110,28 +1035,27 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
                             Bw[wslot<U>(ph, g)], Cw[wslot<U>(ph, g)], C);
       }
       const int yo = y - O;
-      if (yo >= y_out0 && yo < y_out1 && out_lane) {
-        V4<T> v = Uw[wslot<U>(ph, O)];
-        const unsigned c = Cw[wslot<U>(ph, O)];
+      if (yo >= y_out0 && yo < y_out1) {
+        if (out_lane) {
+          V4<T> v = Uw[wslot<U>(ph, O)];
+          const unsigned c = Cw[wslot<U>(ph, O)];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v.v[j] = C.on(c, j) ? v.v[j] : T(0);
-        T *dst = Uo + (long long)yo * L.pitch + x0;
-        if (x0 + 3 < L.nx) {
-          st4(dst, v);
-        } else {
+          for (int j = 0; j < 4; ++j) v.v[j] = C.on(c, j) ? v.v[j] : T(0);
+          T *dst = Uo + (long long)yo * L.pitch + x0;
+          if (x0 + 3 < L.nx) {
+            st4(dst, v);
+          } else {
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (x0 + j < L.nx) dst[j] = v.v[j];
+            for (int j = 0; j < 4; ++j)
+              if (x0 + j < L.nx) dst[j] = v.v[j];
+          }
+          if (LEVEL0) rz.add((double)dot1(Bw[wslot<U>(ph, O)], v));
         }
-        if (LEVEL0) {
-          const V4<T> &bO = Bw[wslot<U>(ph, O)];
-          part += (double)dot1(bO, v);
-        }
+        if (LEVEL0) rz.row_done(yo, y_out1);
       }
     }
   }
   __pipeline_wait_prior(0);
-  return part;
 }
 
 // Up on an FP32 strip of an unmasked level whose next level is unmasked: the
@@ -1143,10 +1067,10 @@ __device__ __forceinline__ double up_strip(const Args<T> &a, const LevelInfo &L,
 // a circular window of NC slots indexed by the coarse row's distance from the
 // strip's first one, so they rotate without moves.
 template <int S1, int S2, bool LEVEL0, bool RECT>
-__device__ __forceinline__ double up_strip_fast(const Args<float> &a, const LevelInfo &L,
-                                                const LevelInfo &Lc, const ClassTable<float> &tab,
-                                                int x0, bool out_lane, int y_start, int y_out0,
-                                                int y_out1, unsigned char *smem) {
+__device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelInfo &L,
+                                              const LevelInfo &Lc, const ClassTable<float> &tab,
+                                              int x0, bool out_lane, int y_start, int y_out0,
+                                              int y_out1, RzGroups &rz, unsigned char *smem) {
   using G = UpGeom<float, S1, S2>;
   constexpr int U = G::U, O = G::O;
   constexpr int P = FastGeom<U>::P, R = FastGeom<U>::R;
@@ -1260,7 +1184,6 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
   H[NC - 1] = cread(1);
   H[0] = cread(3);
   int oofs = (y_start - O) * pitch;  // row offset of the output row of this step
-  double part = 0.0;
   int half = 0;  // ring slot of this pass's first row (0 or P when R == 2P)
   for (int base = y_start; base <= y_last; base += P) {
     const int prev = R == P ? 0 : (half ^ P);  // half the slot before ph = 0 is in
@@ -1318,28 +1241,30 @@ __device__ __forceinline__ double up_strip_fast(const Args<float> &a, const Leve
           else if (!cols_plain) v = mask_on(v, lr.on, 0);
         }
       }
-      if (out_lane && y - O >= y_out0) {
-        const float4 q = join4(v);
-        if (full) {
-          *reinterpret_cast<float4 *>(Uo + oofs) = q;
-        } else {
-          const float vv[4] = {q.x, q.y, q.z, q.w};
+      if (y - O >= y_out0) {
+        if (out_lane) {
+          const float4 q = join4(v);
+          if (full) {
+            *reinterpret_cast<float4 *>(Uo + oofs) = q;
+          } else {
+            const float vv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (x0 + j < L.nx) Uo[oofs + j] = vv[j];
+            for (int j = 0; j < 4; ++j)
+              if (x0 + j < L.nx) Uo[oofs + j] = vv[j];
+          }
+          if (LEVEL0) {
+            const P4 &bo = Bw[wslot<U>(ph, O)];
+            const float2 t = fma2(bo.o, v.o, mul2(bo.e, v.e));  // dot1
+            rz.add((double)__fadd_rn(t.x, t.y));
+          }
         }
-        if (LEVEL0) {
-          const P4 &bo = Bw[wslot<U>(ph, O)];
-          const float2 t = fma2(bo.o, v.o, mul2(bo.e, v.e));  // dot1
-          part += (double)__fadd_rn(t.x, t.y);
-        }
+        if (LEVEL0) rz.row_done(y - O, y_out1);
       }
       oofs += pitch;
     }
     if constexpr (R != P) half ^= P;
   }
   __pipeline_wait_prior(0);
-  return part;
 }
 
 // FP32: three CTAs per SM (above 170 registers only two fit, which was measured
@@ -1356,12 +1281,12 @@ __global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
   const LevelInfo Lc = a.lv[tl.level + 1];  // the next entry: levels are stored finest first
   dep_enter();
   const bool active = a.st[tl.inst].status == GD_ACTIVE;
-  double part = 0.0;
   if (active) {
     fill_table(tab, L.wall);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int RB = L.rows_per_warp;
+    const int RB = L.rows_per_warp;  // a multiple of kRzRows
     const int y_out0 = (tl.ty * UpCta<LEVEL0>::W + warp) * RB;
+    RzGroups rz{a.part0 + a.inst[tl.inst].up0_begin + tl.tx, (L.nx + H::OW - 1) / H::OW, 0.0};
     if (y_out0 < L.ny) {
       const int y_out1 = min(y_out0 + RB, L.ny);
       const int xl = tl.tx * H::OW - 4 * H::HL;
@@ -1375,29 +1300,28 @@ __global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
       if constexpr (sizeof(T) == 4) {
         fast = fast_levels(L, Lc);
         if (fast && interior)
-          part = up_strip_fast<S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start,
-                                                      y_out0, y_out1, smem);
+          up_strip_fast<S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
+                                               y_out1, rz, smem);
         else if (fast)
-          part = up_strip_fast<S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start,
-                                                     y_out0, y_out1, smem);
+          up_strip_fast<S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
+                                              y_out1, rz, smem);
       }
       if constexpr (ANY) {
         if (fast) {
           // done above
         } else if (interior)
-          part = up_strip<T, S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start,
-                                                   y_out0, y_out1, smem);
+          up_strip<T, S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start, y_out0, y_out1,
+                                            rz, smem);
         else
-          part = up_strip<T, S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start,
-                                                    y_out0, y_out1, smem);
+          up_strip<T, S1, S2, LEVEL0, false>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
+                                             y_out1, rz, smem);
       } else if (!fast && lane == 0) {
         atomicOr(a.counter + kErrWord, kErrStrip);
       }
     }
   }
   if (!LEVEL0) return;
-  part = block_sum<UpCta<LEVEL0>::NT>(part);
-  if (threadIdx.x == 0) a.part0[blockIdx.x] = part;
+  __threadfence();  // this CTA's group partials are visible before it takes its ticket
   if (!last_block(a.counter + 3)) return;
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int i = warp; i < a.ninst; i += nw) {

@@ -193,6 +193,30 @@ def test_strip_height_does_not_change_the_vcycle(sweeps):
                 assert torch.equal(z, outs[0]), (boundary, precision)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_strip_height_does_not_change_the_solve(precision):
+    """The r.z partials of the level-0 up kernel are summed per fixed 8-row group
+    and column strip, so whole solves (V-cycles and every reduction) give the same
+    bits and iteration counts whatever strip heights the plan chose."""
+    rng = np.random.default_rng(7)
+    shapes = [(1500, 1400, "neumann"), (700, 900, "dirichlet")]
+    rhs = [torch.as_tensor(rng.standard_normal(s[:2])).cuda() for s in shapes]
+    insts = [Instance(h, w, b, b == "neumann") for h, w, b in shapes]
+    outs = []
+    for warps in (0, 64, 1000, 1 << 20):
+        plan = PoissonPlan(insts, SolveParams(precision=precision, tolerance=1e-9,
+                                              strip_target_warps=warps, zero_start=True))
+        xs = [torch.empty_like(r) for r in rhs]
+        res = plan.solve(rhs, xs, scale=1.0)
+        plan.close()
+        assert all(r.converged for r in res)
+        outs.append((xs, [r.iterations for r in res]))
+    for xs, its in outs[1:]:
+        assert its == outs[0][1]
+        for a, b in zip(xs, outs[0][0]):
+            assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("shape", [(1500, 1400), (301, 517), (130, 90)])
 def test_full_mask_equals_dirichlet_rectangle(shape):
     """A masked instance whose mask covers the whole rectangle is the Dirichlet
