@@ -589,11 +589,12 @@ constexpr int kLevel0TargetWarps = 1800;
 // in parallel).  A launch that overflows a wave by a few strips pays a whole
 // second wave, and a launch of few tall strips leaves each warp a long row
 // chain; the model avoids both (e.g. 2048 x 2048 x 3: 68 rows and one wave
-// instead of 64 rows and 1.03 waves).
+// instead of 64 rows and 1.03 waves).  `only` >= 0: that instance alone.
 int strip_rows(const gd_plan p, const std::vector<int> &bottoms, int l, int down_ow, int up_ow,
-               const long long cap[3], int target) {
+               const long long cap[3], int target, int only = -1) {
   const long long tile_max = p->prm.tile_cells > 0 ? p->prm.tile_cells : kTileCells;
   auto strip_level = [&](int i) {
+    if (only >= 0 && i != only) return false;
     if (l >= bottoms[i]) return false;
     const LevelInfo &L = p->lv[p->inst[i].level0 + l];
     return !(l >= 1 && (long long)L.ny * L.nx <= tile_max);  // else on the tile kernels
@@ -750,14 +751,21 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
     if (p->fp64) Runner<double>::dispatch_capacity(p, false, cap);
     else Runner<float>::dispatch_capacity(p, !any_masked, cap);
   }
+  for (int i = 0; i < p->n; ++i) p->inst[i].rz_rows = st::kRzRows;
   for (int l = 0; l < p->depth; ++l) {
     // level 0 keeps the warps-per-launch rule by default: one wave of tall strips
     // was measured slower there (4096 x 4096 x 3: 256 rows, up0 170 -> 295 us per
     // launch) than several waves of 64-row strips
     const int target = (l == 0 && target_warps == 0) ? kLevel0TargetWarps : target_warps;
     const int rb = strip_rows(p, bottoms, l, down_ow, up_ow, cap, target);
-    for (int i = 0; i < p->n; ++i)
-      if (l < bottoms[i]) p->lv[p->inst[i].level0 + l].rows_per_warp = rb;
+    for (int i = 0; i < p->n; ++i) {
+      if (l >= bottoms[i]) continue;
+      p->lv[p->inst[i].level0 + l].rows_per_warp = rb;
+      // r.z group height: level 0's height for the instance alone (the
+      // warps-per-launch rule only gives taller strips to larger launches, and
+      // its heights are powers of two, so rb is a multiple of it)
+      if (l == 0) p->inst[i].rz_rows = strip_rows(p, bottoms, 0, down_ow, up_ow, cap, target, i);
+    }
   }
   p->fine_base = (int)p->tiles.size();
   for (int i = 0; i < p->n; ++i) {
@@ -840,7 +848,7 @@ int build_plan(gd_plan p, const gd_grid_desc *grids) {
       const int rows = (l == 0 ? st::UpCta<true>::W : st::UpCta<false>::W) * F.rows_per_warp;
       if (l == 0) {  // the instance's r.z group partials (st::RzGroups)
         I.up0_begin = rz_parts;
-        rz_parts += ceil_div(F.ny, st::kRzRows) * ceil_div(F.nx, up_ow);
+        rz_parts += ceil_div(F.ny, I.rz_rows) * ceil_div(F.nx, up_ow);
         I.up0_end = rz_parts;
       }
       for (int ty = 0; ty < ceil_div(F.ny, rows); ++ty)

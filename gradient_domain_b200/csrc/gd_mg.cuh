@@ -78,7 +78,8 @@ struct InstInfo {
   long long xs_off;  // the plan's own FP64 copy of the solution (element offset, row pitch `pitch`)
   int fine_begin, fine_end;  // tile range in the fine map
   int up0_begin, up0_end;    // range of its r.z group partials (empty if bottom is level 0)
-  int zero_mean, pad;
+  int zero_mean;
+  int rz_rows;  // rows per r.z group partial: level 0's strip height for the instance alone
   // set per solve
   const double *f;
   double *x;

@@ -47,6 +47,7 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // Deterministic per-instance sum of partials [b, e) by one warp (L2 reads).
 __device__ __forceinline__ double warp_range_sum(const double *p, int b, int e) {
   double s = 0.0;
+#pragma unroll 8
   for (int k = b + (threadIdx.x & 31); k < e; k += 32) s += __ldcg(p + k);
   return warp_sum(s);
 }

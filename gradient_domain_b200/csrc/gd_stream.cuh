@@ -882,23 +882,26 @@ struct UpGeom {
   static constexpr int U = O + 2;    // rows in every circular window (even)
 };
 
-// r.z partials of the level-0 up kernel: one per kRzRows-row group and column
+// r.z partials of the level-0 up kernel: one per group of rows and column
 // strip, at a fixed place (the instance's base + group x column strips +
-// column strip), so their grouping does not depend on the strip height (strip
-// heights are multiples of kRzRows): a warp adds its lanes' products over the
-// group's rows and writes the group's warp sum when the group ends.  The last
-// CTA of the launch sums an instance's partials in index order, so an instance
-// gives the same r.z whatever strip heights its batch chose.
-constexpr int kRzRows = 8;
+// column strip).  An instance's group height (InstInfo::rz_rows, a power of
+// two) is the level-0 strip height it would get alone, and a batch's strip
+// height is a power-of-two multiple of it, so a group never spans two warps and
+// the grouping does not depend on the batch: a warp adds its lanes' products
+// over the group's rows and writes the group's warp sum when the group ends.
+// The last CTA of the launch sums an instance's partials in a fixed pattern, so
+// an instance gives the same r.z whatever strip heights its batch chose.
+constexpr int kRzRows = 8;  // the smallest group (and strip) height
 struct RzGroups {
   double *base;  // partial of group 0 of this column strip
   int stride;    // column strips of the instance
+  int rows;      // rows per group
   double acc;    // this lane's share of the open group
   __device__ __forceinline__ void add(double v) { acc += v; }
   __device__ __forceinline__ void row_done(int yo, int y_out1) {
-    if ((yo & (kRzRows - 1)) == kRzRows - 1 || yo == y_out1 - 1) {
+    if ((yo & (rows - 1)) == rows - 1 || yo == y_out1 - 1) {
       const double sum = warp_sum(acc);  // xor tree: the same sum in every lane
-      if ((threadIdx.x & 31) == 0) base[(yo / kRzRows) * stride] = sum;
+      if ((threadIdx.x & 31) == 0) base[(yo / rows) * stride] = sum;
       acc = 0.0;
     }
   }
@@ -1284,9 +1287,10 @@ __global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
   if (active) {
     fill_table(tab, L.wall);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int RB = L.rows_per_warp;  // a multiple of kRzRows
+    const int RB = L.rows_per_warp;  // level 0: a multiple of the instance's rz_rows
     const int y_out0 = (tl.ty * UpCta<LEVEL0>::W + warp) * RB;
-    RzGroups rz{a.part0 + a.inst[tl.inst].up0_begin + tl.tx, (L.nx + H::OW - 1) / H::OW, 0.0};
+    const InstInfo &II = a.inst[tl.inst];
+    RzGroups rz{a.part0 + II.up0_begin + tl.tx, (L.nx + H::OW - 1) / H::OW, II.rz_rows, 0.0};
     if (y_out0 < L.ny) {
       const int y_out1 = min(y_out0 + RB, L.ny);
       const int xl = tl.tx * H::OW - 4 * H::HL;
@@ -1321,9 +1325,14 @@ __global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
     }
   }
   if (!LEVEL0) return;
-  __threadfence();  // this CTA's group partials are visible before it takes its ticket
+  // the lane that wrote a warp's group partials makes them visible before the
+  // CTA takes its ticket (one fence per warp)
+  if ((threadIdx.x & 31) == 0) __threadfence();
   if (!last_block(a.counter + 3)) return;
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // one warp per instance (instances in parallel): each lane sums every 32nd of
+  // the instance's groups, then a fixed shuffle tree, so an instance gets the
+  // same r.z in any batch
+  const int warp = threadIdx.x >> 5, nw = UpCta<LEVEL0>::NT >> 5;
   for (int i = warp; i < a.ninst; i += nw) {
     const InstInfo &I = a.inst[i];
     if (I.up0_end <= I.up0_begin) continue;

@@ -194,27 +194,26 @@ def test_strip_height_does_not_change_the_vcycle(sweeps):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_strip_height_does_not_change_the_solve(precision):
-    """The r.z partials of the level-0 up kernel are summed per fixed 8-row group
-    and column strip, so whole solves (V-cycles and every reduction) give the same
-    bits and iteration counts whatever strip heights the plan chose."""
+def test_batch_strip_height_does_not_change_the_solve(precision):
+    """Alone, a 1500 x 1400 instance runs 8-row level-0 strips; batched with three
+    2048 x 2048 instances, 64-row strips.  Its r.z partials are summed per group of
+    rows whose height depends on the instance alone, so the solution and the
+    iteration count are the same bits either way."""
     rng = np.random.default_rng(7)
-    shapes = [(1500, 1400, "neumann"), (700, 900, "dirichlet")]
+    shapes = [(1500, 1400, "neumann")] + [(2048, 2048, "dirichlet")] * 3
     rhs = [torch.as_tensor(rng.standard_normal(s[:2])).cuda() for s in shapes]
     insts = [Instance(h, w, b, b == "neumann") for h, w, b in shapes]
-    outs = []
-    for warps in (0, 64, 1000, 1 << 20):
-        plan = PoissonPlan(insts, SolveParams(precision=precision, tolerance=1e-9,
-                                              strip_target_warps=warps, zero_start=True))
-        xs = [torch.empty_like(r) for r in rhs]
-        res = plan.solve(rhs, xs, scale=1.0)
+    params = SolveParams(precision=precision, tolerance=1e-9, zero_start=True)
+    got = []
+    for members in (insts[:1], insts):
+        plan = PoissonPlan(members, params)
+        xs = [torch.empty_like(r) for r in rhs[:len(members)]]
+        res = plan.solve(rhs[:len(members)], xs, scale=1.0)
         plan.close()
         assert all(r.converged for r in res)
-        outs.append((xs, [r.iterations for r in res]))
-    for xs, its in outs[1:]:
-        assert its == outs[0][1]
-        for a, b in zip(xs, outs[0][0]):
-            assert torch.equal(a, b)
+        got.append((xs[0], res[0].iterations))
+    assert got[0][1] == got[1][1]
+    assert torch.equal(got[0][0], got[1][0])
 
 
 @pytest.mark.parametrize("shape", [(1500, 1400), (301, 517), (130, 90)])
