@@ -73,8 +73,11 @@ typedef struct gd_params {
   int32_t check_every;    /* host poll interval of solves on direct launches         */
   int32_t use_graph;      /* from a plan's second solve on, run the whole solve as   *
                            * one CUDA graph whose while node loops on the device     */
-  int32_t strip_target_warps; /* smoother strips: warps wanted per level launch, all
-                                 instances together (0 = 1800)                      */
+  int32_t strip_target_warps; /* smoother strips: > 0: warps wanted per level launch,
+                                 all instances together (the tallest of 64/32/16/8
+                                 rows that gives them); 0: level 0 as for 1800,
+                                 coarse levels the height with the fewest waves x
+                                 rows (occupancy queried per kernel)               */
   int32_t bottom_cells;       /* largest level the one-CTA bottom takes (0 = 4096)   */
   int32_t tile_cells;         /* largest coarse level on shared-memory tiles (0 = 262144) */
   int32_t zero_start;         /* nonzero: every solve starts from x = 0 and x is only
