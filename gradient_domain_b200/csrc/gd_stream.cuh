@@ -537,7 +537,9 @@ constexpr size_t strip_smem() {
                       : UP       ? (size_t)2 * R * NT * 16 + coarse_ring_bytes<R, NT>()
                                  : (size_t)R * NT * 16;
   if (!ANY) return fast;
-  return level_smem<T, NT>() > fast ? level_smem<T, NT>() : fast;
+  // the masked form adds a ring of packed row classes (4 bytes per lane and row)
+  const size_t mask = sizeof(T) == 4 ? fast + (size_t)R * NT * 4 : 0;
+  return level_smem<T, NT>() > mask ? level_smem<T, NT>() : mask;
 }
 
 // Per-lane constants of the fast strips on rectangle levels in any position
@@ -603,14 +605,33 @@ __device__ __forceinline__ P4 mask_on(const P4 &v, unsigned on, int kind) {
             make_float2((on & 2u) ? v.o.x : 0.f, (on & 8u) ? v.o.y : 0.f)};
 }
 
+// Masked levels (MASK): the classes of a lane's four cells come packed from the
+// level's class bytes, one 32-bit word per row; diagonal inverse (NEG = false)
+// or negated diagonal (NEG = true) of the four cells as same-colour pairs, and
+// the row with its cells of class 0 (no unknown) zeroed.
+template <bool NEG>
+__device__ __forceinline__ P4 mask_diag(const ClassTable<float> &tab, unsigned c) {
+  float v[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = NEG ? -tab.d[cls(c, j)] : tab.inv[cls(c, j)];
+  return P4{make_float2(v[0], v[2]), make_float2(v[1], v[3])};
+}
+__device__ __forceinline__ P4 mask_cls(const P4 &v, unsigned c) {
+  return P4{make_float2(cls(c, 0) ? v.e.x : 0.f, cls(c, 2) ? v.e.y : 0.f),
+            make_float2(cls(c, 1) ? v.o.x : 0.f, cls(c, 3) ? v.o.y : 0.f)};
+}
+
 // Down on an FP32 strip of an unmasked level whose next level is unmasked: the
 // same cells as down_strip<float, S1, INT>, bit for bit, with ring slots and
 // window slots fixed per unrolled phase, running row offsets and the
 // arithmetic on same-colour cell pairs.  RECT = false: every row and column
 // the strip loads is an interior cell (no walls, no bounds tests); RECT = true:
 // any strip of a rectangle level (copies outside the grid are zero-filled,
-// walls take their cells' diagonals, Neumann restriction mirrors its ghosts).
-template <int S1, bool RECT>
+// walls take their cells' diagonals, Neumann restriction mirrors its ghosts);
+// MASK = true (with RECT): a masked level, every row's classes copied from its
+// class bytes through a ring of their own (the same cells as the general
+// masked strips, bit for bit).
+template <int S1, bool RECT, bool MASK = false>
 __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const LevelInfo &L,
                                                 const LevelInfo &Lc, const ClassTable<float> &tab,
                                                 int x0, bool out_lane, int y_start, int y_last,
@@ -638,24 +659,32 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
   const int xl = x0 - 4 * (int)(threadIdx.x & 31);
   const bool cols_plain = xl >= 1 && xl + 127 <= L.nx - 2;
   if constexpr (RECT) {
-    lr = lane_rect(L, tab, x0);
+    if constexpr (!MASK) lr = lane_rect(L, tab, x0);
     lane_in = x0 >= 0 && x0 < L.nx;
     full = x0 + 3 < L.nx;
     neu = L.bc == BC_NEU;
     st0 = J0 >= 0 && J0 < Lc.nx;
     st1 = J0 + 1 >= 0 && J0 + 1 < Lc.nx;
   }
+  // MASK: the class bytes (row pitch `pitch`) and their ring, after the b ring
+  const unsigned char *codes = a.codes + (MASK ? L.code_off : 0);
+  unsigned *cring = reinterpret_cast<unsigned *>(smem + (size_t)R * kSlot * 4) + threadIdx.x;
   P4 Bw[U], Uw[U];
   float2 F[U];
-  int Kw[U];  // row kinds of the window rows (RECT)
+  int Kw[U];       // row kinds of the window rows (RECT)
+  unsigned Cw[U];  // packed classes of the window rows (MASK)
 #pragma unroll
   for (int k = 0; k < U; ++k) {
-    Bw[k] = zero_p4(); Uw[k] = zero_p4(); F[k] = make_float2(0.f, 0.f); Kw[k] = 3;
+    Bw[k] = zero_p4(); Uw[k] = zero_p4(); F[k] = make_float2(0.f, 0.f); Kw[k] = 3; Cw[k] = 0u;
   }
   auto issue = [&](float *dst, int y, int gofs) {
     if constexpr (RECT) {
       const bool ok = lane_in && y >= 0 && y < L.ny;
       __pipeline_memcpy_async(dst, ok ? B + gofs : B, 16, ok ? 0 : 16);
+      if constexpr (MASK) {
+        unsigned *cdst = cring + (dst - ring) / 4;  // the same slot of the class ring
+        __pipeline_memcpy_async(cdst, ok ? codes + gofs : codes, 4, ok ? 0 : 4);
+      }
     } else {
       __pipeline_memcpy_async(dst, B + gofs, 16);
     }
@@ -684,17 +713,21 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
       gofs += pitch;
       P4 &b0 = Bw[wslot<U>(ph, 0)];
       b0 = split4(qb);
-      if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
+      if constexpr (MASK) Cw[wslot<U>(ph, 0)] = cring[(cur - ring) / 4 + ph * kSThreads];
+      else if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
       // rectangle strips: every row the step touches (y - U + 1 .. y) has no wall
       // and is in the grid (kv = 0, per-lane constants), or some row is special
       // (kv = 1, per-row kinds); one copy runs, chosen by a warp-uniform branch
-      const bool rows_plain = !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
+      // (masked levels: always the per-row classes)
+      const bool rows_plain = MASK ? false : !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
 #pragma unroll
-      for (int kv = 0; kv < (RECT ? 2 : 1); ++kv) {
+      for (int kv = MASK ? 1 : 0; kv < (RECT ? 2 : 1); ++kv) {
         if ((kv == 1) == rows_plain) continue;
         const bool kinds = kv == 1;
         auto inv_of = [&](int k) -> P4 {
-          if constexpr (RECT) return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
+          if constexpr (MASK) return mask_diag<false>(tab, Cw[wslot<U>(ph, k)]);
+          else if constexpr (RECT)
+            return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
           else return inv_i;
         };
         // first half sweep (colour 0) from a zero iterate on row y
@@ -721,11 +754,14 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
         const P4 &dnK = Uw[wslot<U>(ph, K - 1)], &bK = Bw[wslot<U>(ph, K)];
         const float left = shfl_up1(uK.o.y), right = shfl_dn1(uK.e.x);
         P4 nd{negd_i, negd_i};
-        if constexpr (RECT) nd = kinds ? rect_diag<true>(lr, tab, Kw[wslot<U>(ph, K)]) : lr.negd0;
+        if constexpr (MASK) nd = mask_diag<true>(tab, Cw[wslot<U>(ph, K)]);
+        else if constexpr (RECT) nd = kinds ? rect_diag<true>(lr, tab, Kw[wslot<U>(ph, K)]) : lr.negd0;
         P4 r;
         r.e = fma2(nd.e, uK.e, nsum2(upK.e, uK.o, make_float2(left, uK.o.x), bK.e, dnK.e));
         r.o = fma2(nd.o, uK.o, nsum2(upK.o, uK.e, make_float2(uK.e.y, right), bK.o, dnK.o));
-        if constexpr (RECT) {
+        if constexpr (MASK) {
+          r = mask_cls(r, Cw[wslot<U>(ph, K)]);
+        } else if constexpr (RECT) {
           if (kinds) r = mask_on(r, lr.on, Kw[wslot<U>(ph, K)]);
           else if (!cols_plain) r = mask_on(r, lr.on, 0);
         }
@@ -779,8 +815,15 @@ __device__ __forceinline__ void down_strip_fast(const Args<float> &a, const Leve
               }
             }
           }
-          const float2 v =
+          float2 v =
               fma2(q25, rows[3], fma2(q75, rows[2], fma2(q75, rows[1], mul2(q25, rows[0]))));
+          if constexpr (MASK) {  // coarse cells without an unknown stay zero
+            if (Lc.code_off >= 0) {
+              const unsigned char *cc = a.codes + Lc.code_off + I * Lc.pitch + J0;
+              if (st0 && !cc[0]) v.x = 0.f;
+              if (st1 && !cc[1]) v.y = 0.f;
+            }
+          }
           float *dst = Bc + I * Lc.pitch + J0;
           if (st0 && st1) {
             *reinterpret_cast<float2 *>(dst) = v;
@@ -803,9 +846,13 @@ __device__ __forceinline__ bool strip_interior(const LevelInfo &L, int y_lo, int
 }
 
 // The fast FP32 strips take unmasked levels whose next level is unmasked and
-// whose row offsets fit 32 bits.
+// whose row offsets fit 32 bits ...
 __device__ __forceinline__ bool fast_levels(const LevelInfo &L, const LevelInfo &Lc) {
   return L.code_off < 0 && Lc.code_off < 0 && (long long)(L.ny + 16) * L.pitch < (1LL << 31);
+}
+// ... and, in their masked form, masked levels.
+__device__ __forceinline__ bool mask_levels(const LevelInfo &L) {
+  return L.code_off >= 0 && (long long)(L.ny + 16) * L.pitch < (1LL << 31);
 }
 
 // Error word bit: a rectangle-only strip kernel met a level it does not handle
@@ -857,6 +904,13 @@ __global__ void __launch_bounds__(kSThreads, strip_min_ctas<T, false, kSThreads,
         down_strip_fast<S1, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0,
                                   y_out1, I_begin, I_end, smem);
       return;
+    }
+    if constexpr (ANY) {
+      if (mask_levels(L)) {
+        down_strip_fast<S1, true, true>(a, L, Lc, tab, x0, out_lane, y_start, y_last, y_out0,
+                                        y_out1, I_begin, I_end, smem);
+        return;
+      }
     }
   }
   if constexpr (ANY) {
@@ -1069,7 +1123,7 @@ __device__ __forceinline__ void up_strip(const Args<T> &a, const LevelInfo &L,
 // row Y is processed and is interpolated then.  The interpolated rows live in
 // a circular window of NC slots indexed by the coarse row's distance from the
 // strip's first one, so they rotate without moves.
-template <int S1, int S2, bool LEVEL0, bool RECT>
+template <int S1, int S2, bool LEVEL0, bool RECT, bool MASK = false>
 __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelInfo &L,
                                               const LevelInfo &Lc, const ClassTable<float> &tab,
                                               int x0, bool out_lane, int y_start, int y_out0,
@@ -1097,7 +1151,7 @@ __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelI
   const int xl = x0 - 4 * lane;
   const bool cols_plain = xl >= 1 && xl + 127 <= L.nx - 2;
   if constexpr (RECT) {
-    lr = lane_rect(L, tab, x0);
+    if constexpr (!MASK) lr = lane_rect(L, tab, x0);
     lane_in = x0 >= 0 && x0 < L.nx;
     full = x0 + 3 < L.nx;
     neu = L.bc == BC_NEU;
@@ -1152,12 +1206,19 @@ __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelI
     const float2 m = mul2(q75, v);  // interp1(near, far) on both pairs
     return P4{fma2(q25, make_float2(lft, v.x), m), fma2(q25, make_float2(v.y, rgt), m)};
   };
+  // MASK: the level's class bytes and their ring, after the coarse ring
+  const unsigned char *codes = a.codes + (MASK ? L.code_off : 0);
+  unsigned *crow = reinterpret_cast<unsigned *>(smem + (size_t)2 * R * kSlot * 4 +
+                                                coarse_ring_bytes<R, NT>()) +
+                   threadIdx.x;
   auto issue = [&](int q, int y, int gofs) {
     float *db = rb + q * kSlot, *dw = rw + q * kSlot;
     if constexpr (RECT) {
       const bool ok = lane_in && y >= 0 && y < L.ny;
       __pipeline_memcpy_async(db, ok ? B + gofs + x0 : B, 16, ok ? 0 : 16);
       __pipeline_memcpy_async(dw, ok ? Wp + gofs + x0 : Wp, 16, ok ? 0 : 16);
+      if constexpr (MASK)
+        __pipeline_memcpy_async(crow + q * NT, ok ? codes + gofs + x0 : codes, 4, ok ? 0 : 4);
     } else {
       __pipeline_memcpy_async(db, B + gofs + x0, 16);
       __pipeline_memcpy_async(dw, Wp + gofs + x0, 16);
@@ -1165,9 +1226,10 @@ __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelI
     if (!(y & 1)) cissue(q, (y >> 1) + 1);  // the coarse row interpolated at row y
   };
   P4 Bw[U], Uw[U], H[NC];
-  int Kw[U];  // row kinds of the window rows (RECT)
+  int Kw[U];       // row kinds of the window rows (RECT)
+  unsigned Cw[U];  // packed classes of the window rows (MASK)
 #pragma unroll
-  for (int k = 0; k < U; ++k) { Bw[k] = zero_p4(); Uw[k] = zero_p4(); Kw[k] = 3; }
+  for (int k = 0; k < U; ++k) { Bw[k] = zero_p4(); Uw[k] = zero_p4(); Kw[k] = 3; Cw[k] = 0u; }
   // coarse rows relative to cy0 = y_start / 2: window slot of row cy0 + k is
   // k mod NC.  Rows cy0 - 1 and cy0 come through coarse slots 1 and 3, which
   // the loop never uses (a coarse row travels with an even fine row, and even
@@ -1204,27 +1266,33 @@ __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelI
       __pipeline_commit();
       gofs += pitch;
       Bw[wslot<U>(ph, 0)] = split4(qb);
-      if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
+      if constexpr (MASK) Cw[wslot<U>(ph, 0)] = crow[(half + ph) * NT];
+      else if constexpr (RECT) Kw[wslot<U>(ph, 0)] = row_kind(L, y);
       const P4 &hn = H[c % NC];
       const P4 &hf = (ph & 1) ? H[(c + 1) % NC] : H[(c + NC - 1) % NC];
       const P4 w = split4(qw);
       // rectangle strips: per-lane constants when every row the step touches
       // (y - U + 1 .. y) has no wall and is in the grid (kv = 0), per-row kinds
       // otherwise (kv = 1); one copy runs, chosen by a warp-uniform branch
-      const bool rows_plain = !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
+      // (masked levels: always the per-row classes)
+      const bool rows_plain = MASK ? false : !RECT || (y - (U - 1) >= 1 && y <= L.ny - 2);
       P4 v;  // the output row y - O
 #pragma unroll
-      for (int kv = 0; kv < (RECT ? 2 : 1); ++kv) {
+      for (int kv = MASK ? 1 : 0; kv < (RECT ? 2 : 1); ++kv) {
         if ((kv == 1) == rows_plain) continue;
         const bool kinds = kv == 1;
         auto inv_of = [&](int k) -> P4 {
-          if constexpr (RECT) return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
+          if constexpr (MASK) return mask_diag<false>(tab, Cw[wslot<U>(ph, k)]);
+          else if constexpr (RECT)
+            return kinds ? rect_diag<false>(lr, tab, Kw[wslot<U>(ph, k)]) : lr.inv0;
           else return inv_i;
         };
         P4 &u = Uw[wslot<U>(ph, 0)];
         u.e = fma2(q25, hf.e, fma2(q75, hn.e, w.e));  // prolong1 on both pairs
         u.o = fma2(q25, hf.o, fma2(q75, hn.o, w.o));
-        if constexpr (RECT) {
+        if constexpr (MASK) {
+          u = mask_cls(u, Cw[wslot<U>(ph, 0)]);
+        } else if constexpr (RECT) {
           if (kinds) u = mask_on(u, lr.on, Kw[wslot<U>(ph, 0)]);
           else if (!cols_plain) u = mask_on(u, lr.on, 0);
         }
@@ -1239,7 +1307,9 @@ __device__ __forceinline__ void up_strip_fast(const Args<float> &a, const LevelI
                       Bw[wslot<U>(ph, g)], inv_of(g).o);
         }
         v = Uw[wslot<U>(ph, O)];
-        if constexpr (RECT) {
+        if constexpr (MASK) {
+          v = mask_cls(v, Cw[wslot<U>(ph, O)]);
+        } else if constexpr (RECT) {
           if (kinds) v = mask_on(v, lr.on, Kw[wslot<U>(ph, O)]);
           else if (!cols_plain) v = mask_on(v, lr.on, 0);
         }
@@ -1309,6 +1379,13 @@ __global__ void __launch_bounds__(UpCta<LEVEL0>::NT,
         else if (fast)
           up_strip_fast<S1, S2, LEVEL0, true>(a, L, Lc, tab, x0, out_lane, y_start, y_out0,
                                               y_out1, rz, smem);
+        if constexpr (ANY) {
+          if (!fast && mask_levels(L)) {
+            up_strip_fast<S1, S2, LEVEL0, true, true>(a, L, Lc, tab, x0, out_lane, y_start,
+                                                      y_out0, y_out1, rz, smem);
+            fast = true;
+          }
+        }
       }
       if constexpr (ANY) {
         if (fast) {
