@@ -954,10 +954,14 @@ struct RzGroups {
   __device__ __forceinline__ void add(double v) { acc += v; }
   __device__ __forceinline__ void row_done(int yo, int y_out1) {
     if ((yo & (rows - 1)) == rows - 1 || yo == y_out1 - 1) {
-      const double sum = warp_sum(acc);  // xor tree: the same sum in every lane
-      if ((threadIdx.x & 31) == 0) base[(yo / rows) * stride] = sum;
+      flush(acc, base + (yo / rows) * stride);
       acc = 0.0;
     }
+  }
+  // one copy of the flush for all unrolled phases (instruction-cache footprint)
+  static __device__ __noinline__ void flush(double acc, double *dst) {
+    const double sum = warp_sum(acc);  // xor tree: the same sum in every lane
+    if ((threadIdx.x & 31) == 0) *dst = sum;
   }
 };
 
