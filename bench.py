@@ -94,11 +94,17 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: begin the timed region once it samples
+        t0 = time.perf_counter()
+        while not self.lines and time.perf_counter() - t0 < 5.0:
+            time.sleep(0.01)
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -107,7 +113,11 @@ class ClockSampler:
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+        # at least one sample taken after the timed region began (a short region can end
+        # between two samples; the GPU is still at its load clock just after)
+        t0 = time.perf_counter()
+        while len(self.lines) <= getattr(self, "first", 0) and time.perf_counter() - t0 < 2.0:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -115,7 +125,8 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        during = self.lines[getattr(self, "first", 0):] or self.lines
+        for line in during:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
